@@ -1,0 +1,344 @@
+"""Benchmark of the lapw1 H/S setup (HAMILT + HNS [+ HORB]) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--prec fp64|split]
+                    [--impl ours|reference]
+
+One step = the full calkpt.F:153-185 setup of one k-point per GPU.  At one
+GPU the workload is the 40-atom 2x2x2 ABO3 supercell (RKmax 7, ~4950 basis
+functions, one LO per atom for l<=2, one general k).  With N GPUs each rank
+sets up its own k-point of the same cell (k-points are independent: weak
+scaling, no collective on the data path).  Prints ONE JSON line (rank 0).
+
+`value` is ms per k-point of the whole job with inputs resident in HBM
+(device timed, CUDA events on the library's stream, max over ranks).
+`e2e` is the same metric through the host C-ABI entry point lapw1gpu_setup
+(inputs from host memory, HS/HSDIAG copied back into pinned host memory).
+The reference arm (--impl reference) times the CPU restatement of the
+reference algorithm (the oracle: no Fortran compiler exists here to build
+the reference itself) on all host cores over a bounded sample of the same
+k-point and reports the extrapolated ms per k-point.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "lapw1 H+S setup ms/k-point"
+UNIT = "ms/k-point"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch, device):
+    """Measured FP64 reference: cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def baseline_def_flops(p):
+    """BASELINE's work formula F = sum_atoms (16 N^2 (lmax+1)^2 + 8 N^2 (lmax_ns+1)^2):
+    the flops of the A^H T A form the benchmark definition counts."""
+    n = p.n
+    return p.ndf * (16.0 * n * n * p.ltop ** 2 + 8.0 * n * n * (p.lnsmax + 1) ** 2)
+
+
+def problem_input_bytes(p):
+    cp = p.to_c()
+    return int(sum(a.nbytes for a in cp._keep))
+
+
+def cpu_reference(p, budget_s=12.0):
+    """Bounded CPU sample of the reference algorithm (the oracle on all host
+    cores): HAMILT over a contiguous slice of plane-wave columns, the LO
+    columns, and HNS for one atom; scaled to a full k-point by the work
+    fractions (column I of HAMILT costs ~I, each HNS atom the same)."""
+    from oracle import oracle as O
+    nv = p.nv
+    # columns [c0, nv]: work sum_{I=c0..nv} I; take the slice worth ~3%
+    frac_target = 0.03
+    c0 = int(nv * math.sqrt(1.0 - frac_target))
+    t = time.perf_counter()
+    O.hamilt_sample(p, c0, nv)
+    t_h = time.perf_counter() - t
+    frac_h = (nv * (nv + 1) / 2 - (c0 - 1) * c0 / 2) / (nv * (nv + 1) / 2)
+    t = time.perf_counter()
+    O.hns_sample(p, 1, 1)
+    t_ns = time.perf_counter() - t
+    frac_ns = 1.0 / p.ndf
+    est_s = t_h / frac_h + t_ns / frac_ns
+    sample = (f"HAMILT PW columns {c0}..{nv} of {nv} ({100 * frac_h:.1f}% of its work) + "
+              f"HNS atom 1 of {p.ndf}; extrapolated to one k-point")
+    return est_s * 1e3, sample, t_h + t_ns
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return 0
+    from hack_wein2k_b200 import synth
+    p = synth.config("c1")[0]
+    cores = os.cpu_count()
+    vals = []
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, sample, _ = cpu_reference(p)
+        if i >= args.warmup:
+            vals.append(v)
+    val = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "c1: 2x2x2 ABO3 supercell a=14.8 bohr, 40 atoms, RKmax 7, lmax 10, "
+                               "lmax_ns 4, LO l<=2, one general k", "n": p.n, "nv": p.nv, "nlo": p.nlo,
+                   "impl": "CPU restatement of HAMILT/HNS (oracle port), OpenMP all cores"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--prec", choices=["fp64", "split"], default="fp64")
+    ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from hack_wein2k_b200 import lapw1gpu, synth
+
+    rank, world, local = _env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+
+    # workload: c1 at one GPU; rank r of N takes k-point r of the same cell
+    if world == 1:
+        p = synth.config("c1")[0]
+        workload = "c1: 2x2x2 ABO3 supercell a=14.8 bohr, 40 atoms, RKmax 7, lmax 10, lmax_ns 4, LO l<=2, one general k"
+    else:
+        p = synth.config("c2", nk=max(world, 1))[rank]
+        workload = "c2 k-shard: 2x2x2 ABO3 supercell, one seeded wedge k-point per rank"
+
+    prec = lapw1gpu.PREC_SPLIT if args.prec == "split" else lapw1gpu.PREC_FP64
+    ctx = lapw1gpu.Context(local, prec=prec, slices=args.slices)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=device)
+    kp = ctx.upload(p)
+    n = p.n
+    d_hs = torch.empty((n, n, 2), dtype=torch.float64, device=device)  # column-major view: [col][row]
+    d_hd = torch.empty((n, 2), dtype=torch.float64, device=device)
+    torch.cuda.synchronize()
+
+    def step(stats=True):
+        return kp.run(d_hs.data_ptr(), n, d_hd.data_ptr(), stages=7, stats=stats)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    stage_ms = {}
+    launches = 0
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = step(stats=True)
+            for k, v in st.items():
+                stage_ms[k] = stage_ms.get(k, 0.0) + v
+            launches += int(st["kernel_launches"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = ms_step / world  # ms per k-point of the whole job (world k-points per step)
+
+    # ---- e2e through the host entry point ----
+    hs_h = torch.empty((n, n, 2), dtype=torch.float64).pin_memory()
+    hd_h = torch.empty((n, 2), dtype=torch.float64).pin_memory()
+    hs_np = hs_h.numpy().view(np.complex128).reshape(n, n).T  # Fortran-order view of [col][row]
+    hd_np = hd_h.numpy().view(np.complex128).reshape(n)
+    for _ in range(max(1, args.warmup)):
+        ctx.setup(p, hs=hs_np, hsdiag=hd_np)
+    if dist is not None:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    f0.record(stream)
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(e2e_steps):
+        ctx.setup(p, hs=hs_np, hsdiag=hd_np)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = e2e_ms / e2e_steps / world
+    h2d = problem_input_bytes(p)
+    d2h = n * n * 16 + n * 16
+
+    # ---- roofline of the dominant kernel ----
+    clocks = clk.summary()
+    avg = {k: v / args.steps for k, v in stage_ms.items()}
+    nsl2 = (p.lnsmax + 1) ** 2
+    f_sph = 8.0 * 2.0 * (2.0 * p.ndf) * p.ltop * (p.nv * (p.nv + 1) / 2.0)
+    f_hns = 8.0 * (2.0 * p.ndf * nsl2) * (n * (n + 1) / 2.0)
+    kern = {"k_spherical (K-b)": (f_sph, avg["ms_spherical"]), "HNS GEMM (K-ns)": (f_hns, avg["ms_hns"])}
+    dom = max(kern, key=lambda k: kern[k][1])
+    fl, t_ms = kern[dom]
+    peak = fp64_peak_tflops(torch, device) if args.prec == "fp64" else None
+    peak_src = "measured by bench.py: cuBLAS DGEMM 8192^3 best of 5 (no FP64 figure in MEASURED_PEAKS.json)"
+    if args.prec == "split":
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+        peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
+        peak_src = "2 x measured dense bf16 (int8 tcgen05 rate), MEASURED_PEAKS.json"
+    achieved = fl / (t_ms * 1e-3) / 1e12
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tj):
+        try:
+            traffic = json.load(open(tj)).get(dom)
+        except Exception:
+            traffic = None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample, _ = cpu_reference(p)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.prec == "fp64" else "int8-slices(f64 accum)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": workload, "n": n, "nv": p.nv, "nlo": p.nlo, "atoms": p.ndf, "lmax": p.ltop - 1,
+                   "lmax_ns": p.lnsmax, "precision": args.prec, "parallelism": f"k-shard x{world}",
+                   "l2": "HS output 0.39 GB and HNS operands 0.32 GB per k-point exceed the 126 MB L2"},
+        "kpoints_per_s": 1e3 / value,
+        "fp64_equiv_tflops": (f_sph + f_hns) / (ms_step * 1e-3) / 1e12,
+        "fp64_equiv_tflops_baseline_def": baseline_def_flops(p) / (ms_step * 1e-3) / 1e12,
+        "stage_ms": {k: v for k, v in avg.items() if k.startswith("ms_")},
+        "roofline": {"kernel": dom, "bound": "tensor" if args.prec == "split" else "fp64",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "peak_source": peak_src, "flops_per_launch": fl, "ms_per_launch": t_ms},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    kp.free()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,882 @@
+// kernels_fp64.cuh -- FP64 kernels of the lapw1 H/S setup (sm_100a).
+//
+// Data layout in HBM for one k-point (rows = HSROWS = nv + nlo, padded):
+//   al, bl     [nat][ltop][nvpad]  f64    matching coefficients (K-a)
+//   phase      [ndf][npad]         c128   exp(2 pi i K_n . r_a) of every row
+//   tab        [(2d3+1)(2d2+1)(2d1+1)] 2 x c128: (Theta(dK), WARP(dK))
+//   hns L / R  [ndf*2*nsl2][npad]  c128   HNS left (A2,B2) / right (ALM,BLM)
+//   hs         n x n c128, column-major (the caller's HS), hsdiag n c128
+#pragma once
+#include "common.cuh"
+
+struct DevProb {
+  int n, nv, nlo, nat, ndf, ltop, ldl, lnsmax, ins;
+  int nvpad, npad;
+  double vi;
+  // structure
+  const int* mult;
+  const int* atype;     // [ndf] 0-based type of atom a
+  const int* afirst;    // [nat] first atom index of type
+  const double* rmt;
+  const double* v;
+  const double* pos;    // [ndf][3]
+  const double* rotij;  // [ndf][9]
+  const double* rotloc; // [nat][9]
+  // rows
+  const int* kzz;       // [n][3]
+  const double* xk;
+  const double* yk;
+  const double* zk;
+  const double* rk;
+  // radial [nat][ldl]
+  const double* p;
+  const double* pe;
+  const double* dp;
+  const double* dpe;
+  const double* pei;
+  const double* e;
+  const int* lapw;
+  // LO
+  const int* ilo;
+  const int* loor;
+  const double* alo;
+  const double* blo;
+  const double* clo;
+  const double* elo;
+  const double* pi12lo;
+  const double* pe12lo;
+  const double* dplo;
+  // derived
+  double* al;
+  double* bl;
+  double2* phase;
+};
+
+// ---------------------------------------------------------------------
+// K-a: AL/BL (hamilt.F:160-175), one thread per (row n < nv, atom type)
+// ---------------------------------------------------------------------
+__global__ void k_albl(DevProb P, int* status) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  int jn = blockIdx.y;
+  if (n >= P.nvpad) return;
+  const int ltop = P.ltop;
+  double* al = P.al + ((size_t)jn * ltop) * P.nvpad + n;
+  double* bl = P.bl + ((size_t)jn * ltop) * P.nvpad + n;
+  if (n >= P.nv) {
+    for (int l = 0; l < ltop; l++) {
+      al[(size_t)l * P.nvpad] = 0.0;
+      bl[(size_t)l * P.nvpad] = 0.0;
+    }
+    return;
+  }
+  double fj[L1G_MAXL + 2], dfj[L1G_MAXL + 2];
+  double rkn = P.rk[n], r = P.rmt[jn];
+  int st = dev_sphbes(ltop - 1, r * rkn, fj);
+  if (st) atomicOr(status, st);
+  dev_dvbes1(fj, dfj, rkn, r, ltop);
+  const double* U = P.p + jn * P.ldl;
+  const double* UP = P.pe + jn * P.ldl;
+  const double* DU = P.dp + jn * P.ldl;
+  const double* DUP = P.dpe + jn * P.ldl;
+  const int* LAPW = P.lapw + jn * P.ldl;
+  for (int l = 0; l < ltop; l++) {
+    double a, b;
+    if (LAPW[l]) {
+      a = rkn * dfj[l] * UP[l] - fj[l] * DUP[l];
+      b = fj[l] * DU[l] - rkn * dfj[l] * U[l];
+    } else {
+      a = fj[l] / U[l] / (r * r);
+      b = 0.0;
+    }
+    al[(size_t)l * P.nvpad] = a;
+    bl[(size_t)l * P.nvpad] = b;
+  }
+}
+
+// structure-factor phases of every row for every atom (hns.F:171-174)
+__global__ void k_phase(DevProb P) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  int a = blockIdx.y;
+  if (n >= P.npad) return;
+  double2 v = cmk(0.0, 0.0);
+  if (n < P.n) {
+    const double* r = P.pos + 3 * a;
+    const int* k = P.kzz + 3 * n;
+    double s = r[0] * (double)k[0] + r[1] * (double)k[1] + r[2] * (double)k[2];
+    v = cexp2pi(s);
+  }
+  P.phase[(size_t)a * P.npad + n] = v;
+}
+
+// ---------------------------------------------------------------------
+// K-c table: Theta(dK) and WARP(dK) on the integer box of row differences.
+//   INS == 0: Theta(dK != 0) = sum_type 3 V PHASE BESR  (hamilt.F:297-326)
+//             Theta(0)       = sum_type (1/NAT - V MULT) (hamilt.F:328-329)
+//   INS != 0: USTPHX (ustphx.F:31-52); no warp term (hamilt.F:349-365)
+// ---------------------------------------------------------------------
+struct TabDesc {
+  int d1, d2, d3;       // half extents
+  int w1, w2, w3;       // WARP half extents
+  double bk[9];         // Cartesian dK = bk * dKZZ  (bk row-major [3][3])
+};
+
+__global__ void k_table(DevProb P, TabDesc T, const double2* warp, double2* tab) {
+  int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1, nz = 2 * T.d3 + 1;
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nx * ny * nz) return;
+  int ix = idx % nx, iy = (idx / nx) % ny, iz = idx / (nx * ny);
+  int d[3] = {ix - T.d1, iy - T.d2, iz - T.d3};
+  double g0 = T.bk[0] * d[0] + T.bk[1] * d[1] + T.bk[2] * d[2];
+  double g1 = T.bk[3] * d[0] + T.bk[4] * d[1] + T.bk[5] * d[2];
+  double g2 = T.bk[6] * d[0] + T.bk[7] * d[1] + T.bk[8] * d[2];
+  double slen = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+  bool zero = (d[0] == 0 && d[1] == 0 && d[2] == 0);
+  double2 th = cmk(0.0, 0.0);
+  if (P.ins == 0) {
+    for (int jn = 0; jn < P.nat; jn++) {
+      if (zero) {
+        th.x = th.x + 1.0 / (double)P.nat - P.v[jn] * (double)P.mult[jn];
+      } else {
+        double2 ph = cmk(0.0, 0.0);
+        int a0 = P.afirst[jn];
+        for (int q = 0; q < P.mult[jn]; q++) {
+          const double* r = P.pos + 3 * (a0 + q);
+          ph = cadd(ph, cexp2pi(r[0] * d[0] + r[1] * d[1] + r[2] * d[2]));
+        }
+        double h = slen * P.rmt[jn];
+        double sn, cs;
+        sincos(h, &sn, &cs);
+        double besr = (h * cs - sn) * (1.0 / (h * h * h));
+        double v3 = 3.0 * P.v[jn];
+        th = cadd(th, cscale(cscale(ph, v3), besr));
+      }
+    }
+  } else {
+    if (slen > 1.0e-10) {
+      double2 u = cmk(0.0, 0.0);
+      for (int jn = 0; jn < P.nat; jn++) {
+        double2 ph = cmk(0.0, 0.0);
+        int a0 = P.afirst[jn];
+        for (int q = 0; q < P.mult[jn]; q++) {
+          const double* r = P.pos + 3 * (a0 + q);
+          ph = cadd(ph, cexp2pi(r[0] * d[0] + r[1] * d[1] + r[2] * d[2]));
+        }
+        double qq = slen * P.rmt[jn];
+        double sn, cs;
+        sincos(qq, &sn, &cs);
+        double besr = (qq * cs - sn) / (qq * qq * qq);
+        u = cadd(u, cscale(cscale(ph, P.v[jn]), besr));
+      }
+      th = cscale(u, 3.0);
+    } else {
+      double u = 0.0;
+      for (int jn = 0; jn < P.nat; jn++) u = u + P.v[jn] * (double)P.mult[jn];
+      th = cmk(1.0 - u, 0.0);
+    }
+  }
+  double2 w = cmk(0.0, 0.0);
+  if (P.ins == 0 && abs(d[0]) <= T.w1 && abs(d[1]) <= T.w2 && abs(d[2]) <= T.w3) {
+    size_t wi = ((size_t)(d[2] + T.w3) * (2 * T.w2 + 1) + (size_t)(d[1] + T.w2)) * (2 * T.w1 + 1) +
+                (size_t)(d[0] + T.w1);
+    w = warp[wi];
+  }
+  tab[2 * (size_t)idx] = th;
+  tab[2 * (size_t)idx + 1] = w;
+}
+
+// ---------------------------------------------------------------------
+// K-b + K-c: PW x PW block of H and S (hamilt.F:188-466 + ZSWAP).
+//
+// The reference's per-pair sum over atoms and l,
+//   S_JI += sum_a VIF_a PHASE_a(J,I) sum_l (2l+1) P_l(x_JI) s_l(I,J)
+// is regrouped as sum_l (2l+1) P_l(x_JI) G_l(J,I) with
+//   G_l(J,I) = sum_{a,r} X_l[(a,r),J] * Y_l[(a,r),I]
+//   X_l[(a,0/1),J] = phi_a(J) * {AL, BL}(J,l,type a)
+//   YS [(a,0/1),I] = conj(phi_a(I)) VIF {AL, CHN*BL}(I)
+//   YH [(a,0/1),I] = conj(phi_a(I)) VIF {(E+R^2 U DU) AL + R^2 UP DU BL,
+//                                        (1+R^2 U DUP) AL + (E CHN + R^2 UP DUP) BL}(I)
+// (the non-symmetric 2x2 block of hamilt.F:386-424, surface terms included),
+// i.e. one complex GEMM with K = 2*NDF per l and a per-pair Legendre epilogue
+// that keeps the reference's recursion and its UTOP branch (hamilt.F:250-281).
+// ---------------------------------------------------------------------
+#define SPH_TJ 64
+#define SPH_TI 32
+#define SPH_KT 8
+#define SPH_THREADS 256
+#define SPH_DYN_SMEM (24 * SPH_THREADS * 8)
+
+struct SphCoef {  // per (type, l)
+  double vif, chn, mAA, mAB, mBA, mBB;
+};
+
+__global__ void k_sph_coef(DevProb P, SphCoef* coef) {
+  int l = threadIdx.x, jn = blockIdx.x;
+  if (l >= P.ltop) return;
+  const double pi = 3.141592653589793238462643;
+  double r = P.rmt[jn];
+  double r2 = r * r;
+  int o = jn * P.ldl + l;
+  double U = P.p[o], UP = P.pe[o], DU = P.dp[o], DUP = P.dpe[o], CHN = P.pei[o], E = P.e[o];
+  SphCoef c;
+  c.vif = 4.0 * pi * P.vi * (r2 * r2);
+  c.chn = P.lapw[o] ? CHN : 0.0;
+  c.mAA = E + r2 * (U * DU);
+  c.mAB = r2 * (UP * DU);
+  c.mBA = 1.0 + r2 * (U * DUP);
+  c.mBB = E * CHN + r2 * (UP * DUP);
+  coef[jn * P.ltop + l] = c;
+}
+
+__global__ void __launch_bounds__(SPH_THREADS, 1)
+    k_spherical(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef,
+                const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs,
+                int ld, double2* __restrict__ hsdiag) {
+  __shared__ double2 sX[2 * SPH_KT][SPH_TJ];
+  __shared__ double2 sYH[2 * SPH_KT][SPH_TI];
+  __shared__ double2 sYS[2 * SPH_KT][SPH_TI];
+  // Legendre recursion state of the 8 pairs each thread owns (48 KB dynamic)
+  extern __shared__ double sLeg[];
+  double* sLx = sLeg;
+  double* sLp1 = sLeg + 8 * SPH_THREADS;
+  double* sLp2 = sLeg + 16 * SPH_THREADS;
+
+  const int tid = threadIdx.x;
+  const int tj = tid & 15, ti = tid >> 4;
+  const int2 t = tiles[blockIdx.x];
+  const int i0 = t.x * SPH_TI, j0 = t.y * SPH_TJ;
+  const int nv = P.nv, ltop = P.ltop, ndf = P.ndf;
+
+  // Legendre argument per owned pair (hamilt.F:250-256)
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+      int J = j0 + tj * 4 + u, I = i0 + ti * 2 + v;
+      double x = 0.0;
+      if (J < nv && I < nv) {
+        x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
+        double den = P.rk[I] * P.rk[J];
+        if (den > 1.0e-8) x = x / den;
+      }
+      int q = (u * 2 + v) * SPH_THREADS + tid;
+      sLx[q] = x;
+      sLp1[q] = 0.0;
+      sLp2[q] = 0.0;
+    }
+
+  double2 aH[4][2], aS[4][2];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) aH[u][v] = aS[u][v] = cmk(0.0, 0.0);
+
+  for (int l = 0; l < ltop; l++) {
+    double2 gH[4][2], gS[4][2];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 2; v++) gH[u][v] = gS[u][v] = cmk(0.0, 0.0);
+
+    for (int a0 = 0; a0 < ndf; a0 += SPH_KT) {
+      __syncthreads();
+      // operand tiles
+      for (int idx = tid; idx < SPH_KT * (SPH_TJ + SPH_TI); idx += SPH_THREADS) {
+        if (idx < SPH_KT * SPH_TJ) {
+          int ka = idx / SPH_TJ, jj = idx % SPH_TJ;
+          int a = a0 + ka, J = j0 + jj;
+          double2 x0 = cmk(0.0, 0.0), x1 = cmk(0.0, 0.0);
+          if (a < ndf && J < nv) {
+            int jn = P.atype[a];
+            double2 ph = P.phase[(size_t)a * P.npad + J];
+            size_t o = ((size_t)jn * ltop + l) * P.nvpad + J;
+            double alv = P.al[o], blv = P.bl[o];
+            x0 = cscale(ph, alv);
+            x1 = cscale(ph, blv);
+          }
+          sX[2 * ka][jj] = x0;
+          sX[2 * ka + 1][jj] = x1;
+        } else {
+          int id2 = idx - SPH_KT * SPH_TJ;
+          int ka = id2 / SPH_TI, ii = id2 % SPH_TI;
+          int a = a0 + ka, I = i0 + ii;
+          double2 h0 = cmk(0.0, 0.0), h1 = h0, s0 = h0, s1 = h0;
+          if (a < ndf && I < nv) {
+            int jn = P.atype[a];
+            double2 ph = cconj(P.phase[(size_t)a * P.npad + I]);
+            size_t o = ((size_t)jn * ltop + l) * P.nvpad + I;
+            double alv = P.al[o], blv = P.bl[o];
+            SphCoef c = coef[jn * ltop + l];
+            double2 pv = cscale(ph, c.vif);
+            s0 = cscale(pv, alv);
+            s1 = cscale(pv, c.chn * blv);
+            h0 = cscale(pv, c.mAA * alv + c.mAB * blv);
+            h1 = cscale(pv, c.mBA * alv + c.mBB * blv);
+          }
+          sYS[2 * ka][ii] = s0;
+          sYS[2 * ka + 1][ii] = s1;
+          sYH[2 * ka][ii] = h0;
+          sYH[2 * ka + 1][ii] = h1;
+        }
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int k = 0; k < 2 * SPH_KT; k++) {
+        double2 xv[4], yh[2], ys[2];
+#pragma unroll
+        for (int u = 0; u < 4; u++) xv[u] = sX[k][tj * 4 + u];
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+          yh[v] = sYH[k][ti * 2 + v];
+          ys[v] = sYS[k][ti * 2 + v];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            gH[u][v].x = fma(xv[u].x, yh[v].x, gH[u][v].x);
+            gH[u][v].x = fma(-xv[u].y, yh[v].y, gH[u][v].x);
+            gH[u][v].y = fma(xv[u].x, yh[v].y, gH[u][v].y);
+            gH[u][v].y = fma(xv[u].y, yh[v].x, gH[u][v].y);
+            gS[u][v].x = fma(xv[u].x, ys[v].x, gS[u][v].x);
+            gS[u][v].x = fma(-xv[u].y, ys[v].y, gS[u][v].x);
+            gS[u][v].y = fma(xv[u].x, ys[v].y, gS[u][v].y);
+            gS[u][v].y = fma(xv[u].y, ys[v].x, gS[u][v].y);
+          }
+      }
+    }
+    // Legendre epilogue for this l
+    const double dll1 = (double)(2 * l + 1);
+    const double xl = (l >= 2) ? (double)(l - 1) / (double)l : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        int q = (u * 2 + v) * SPH_THREADS + tid;
+        double x = sLx[q], pm1 = sLp1[q], pm2 = sLp2[q], pl;
+        if (l == 0)
+          pl = 1.0;
+        else if (l == 1)
+          pl = x;
+        else if (fabs(x) < 0.9999999) {
+          double pplx = x * pm1;
+          double pply = pplx - pm2;
+          pl = pplx + xl * pply;
+        } else
+          pl = x * pm1;
+        sLp2[q] = pm1;
+        sLp1[q] = pl;
+        double w = dll1 * pl;
+        aH[u][v].x = fma(w, gH[u][v].x, aH[u][v].x);
+        aH[u][v].y = fma(w, gH[u][v].y, aH[u][v].y);
+        aS[u][v].x = fma(w, gS[u][v].x, aS[u][v].x);
+        aS[u][v].y = fma(w, gS[u][v].y, aS[u][v].y);
+      }
+  }
+  // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
+  const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
+#pragma unroll
+  for (int v = 0; v < 2; v++) {
+    int I = i0 + ti * 2 + v;
+    if (I >= nv) continue;
+    const int k1 = P.kzz[3 * I], k2 = P.kzz[3 * I + 1], k3 = P.kzz[3 * I + 2];
+    const double xi = P.xk[I], yi = P.yk[I], zi = P.zk[I];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      int J = j0 + tj * 4 + u;
+      if (J > I) continue;
+      double x2 = P.xk[J] * xi + P.yk[J] * yi + P.zk[J] * zi;
+      double2 th, wp;
+      if (J == I) {
+        size_t c0 = ((size_t)T.d3 * ny + T.d2) * nx + T.d1;
+        th = tab[2 * c0];
+        wp = tab[2 * c0 + 1];
+      } else {
+        int d1 = P.kzz[3 * J] - k1 + T.d1, d2 = P.kzz[3 * J + 1] - k2 + T.d2, d3 = P.kzz[3 * J + 2] - k3 + T.d3;
+        size_t c = ((size_t)d3 * ny + d2) * nx + d1;
+        th = tab[2 * c];
+        wp = tab[2 * c + 1];
+      }
+      double2 s = cadd(th, aS[u][v]);
+      double2 h = cadd(cadd(cscale(th, x2), wp), aH[u][v]);
+      if (J == I) {
+        hs[(size_t)I * ld + I] = h;
+        hsdiag[I] = s;
+      } else {
+        hs[(size_t)I * ld + J] = s;   // S upper: HS(J,I)
+        hs[(size_t)J * ld + I] = h;   // H lower: HS(I,J)
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// K-b': local-orbital columns (hamilt.F:475-818).  One block row per LO
+// column, threads over rows J <= I.
+// ---------------------------------------------------------------------
+struct LoCol {
+  int jn, l, jlo, jeqo, mo1, nnlo, a0;  // a0: first atom of the type
+  double clr, cli;                       // i^l
+};
+
+__global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restrict__ hs, int ld,
+                     double2* __restrict__ hsdiag) {
+  const LoCol c = cols[blockIdx.y];
+  const int nv = P.nv;
+  const int I = nv + c.nnlo - 1;  // 0-based row/column of this LO
+  int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J > I) return;
+  const int jn = c.jn, l = c.l, jlo = c.jlo, jeqo = c.jeqo, mo1 = c.mo1, mult = P.mult[jn];
+  const double pi = 3.141592653589793238462643;
+  const double r = P.rmt[jn], r2 = r * r;
+  const double pi4r2v = 4.0 * pi * sqrt(P.vi) * r * r;
+  const int o = jn * P.ldl + l;
+  const double U = P.p[o], UP = P.pe[o], DU = P.dp[o], DUP = P.dpe[o], CHN = P.pei[o], E = P.e[o];
+  const int lo4 = jn * (L1G_LOMAX + 1) + l;
+#define LOV(arr, jj) P.arr[(jn * L1G_NLOAT + (jj)-1) * (L1G_LOMAX + 1) + l]
+  const double ALO = LOV(alo, jlo), BLO = LOV(blo, jlo), CLO = LOV(clo, jlo), ELO = LOV(elo, jlo);
+  const double PI12 = P.pi12lo[lo4], PE12 = P.pe12lo[lo4], DPL = P.dplo[lo4];
+  const double c1r = ALO + PI12 * CLO;
+  const double c2r = BLO * CHN + PE12 * CLO;
+  const double c11r = ALO * E + 0.5 * (BLO + CLO * PI12 * (ELO + E));
+  const double c12r = BLO * CHN * E + 0.5 * (ALO + CLO * PI12 + CLO * PE12 * (ELO + E));
+  const double c3r = CLO + PE12 * BLO + ALO * PI12;
+  const double c13r = CLO * ELO + 0.5 * (BLO * PI12 + (ELO + E) * (ALO * PI12 + PE12 * BLO));
+  const double akinlor = 0.5 * r2 * (ALO * DU + BLO * DUP + CLO * DPL);
+  const double clr = c.clr, cli = c.cli;
+
+  // LO-LO row ranges (hamilt.F:677-680), 1-based NNLO arithmetic
+  bool inlo[L1G_NLOAT + 1];
+  int Jf = J + 1;  // 1-based row
+  bool any_lo = false;
+  for (int jlop = 1; jlop <= jlo; jlop++) {
+    int jbeg = nv + c.nnlo - (mo1 + l) - (2 * l + 1) * (jeqo - 1) - (jlo - jlop) * (2 * l + 1) * mult;
+    int jend = nv + c.nnlo - (jlo - jlop) * (mo1 + l + 1) - (jlo - jlop) * (jeqo - 1) * (2 * l + 1);
+    inlo[jlop] = (Jf >= jbeg && Jf <= jend);
+    any_lo |= inlo[jlop];
+  }
+  double2 S = cmk(0.0, 0.0), H = cmk(0.0, 0.0);
+  if (J < nv || any_lo) {
+    double alj = 0.0, blj = 0.0;
+    if (J < nv) {
+      size_t oo = ((size_t)jn * P.ltop + l) * P.nvpad + J;
+      alj = P.al[oo];
+      blj = P.bl[oo];
+    }
+    for (int jeq = 0; jeq < mult; jeq++) {
+      const int a = c.a0 + jeq;
+      const double* ra = P.pos + 3 * a;
+      double s = ra[0] * (double)(P.kzz[3 * I] - P.kzz[3 * J]) + ra[1] * (double)(P.kzz[3 * I + 1] - P.kzz[3 * J + 1]) +
+                 ra[2] * (double)(P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
+      const double2 ph = cconj(cexp2pi(s));
+      double2 yi[16], yj[16];
+      dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yi);
+      dev_ylm_row<3>(P.xk[J], P.yk[J], P.zk[J], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yj);
+      for (int mo2 = -l; mo2 <= l; mo2++) {
+        const int lm = l * (l + 1) + mo2;
+        const double clylnr = clr * yi[lm].x + cli * yi[lm].y;
+        const double clylni = cli * yi[lm].x - clr * yi[lm].y;
+        const double c1rup = c1r * clylnr * pi4r2v, c1iup = c1r * clylni * pi4r2v;
+        const double c2rup = c2r * clylnr * pi4r2v, c2iup = c2r * clylni * pi4r2v;
+        const double c3rup = c3r * clylnr * pi4r2v, c3iup = c3r * clylni * pi4r2v;
+        const double c11rup = c11r * clylnr * pi4r2v, c11iup = c11r * clylni * pi4r2v;
+        const double c12rup = c12r * clylnr * pi4r2v, c12iup = c12r * clylni * pi4r2v;
+        const double c13rup = c13r * clylnr * pi4r2v, c13iup = c13r * clylni * pi4r2v;
+        const double akinlorup = akinlor * clylnr * pi4r2v, akinloiup = akinlor * clylni * pi4r2v;
+        const double clylr = clr * yj[lm].x + cli * yj[lm].y;
+        const double clyli = cli * yj[lm].x - clr * yj[lm].y;
+        if (J < nv) {
+          const double c6r = clylr * alj * pi4r2v, c6i = clyli * alj * pi4r2v;
+          const double c7r = clylr * blj * pi4r2v, c7i = clyli * blj * pi4r2v;
+          double cabr = c6r * c1rup + c7r * c2rup + c6i * c1iup + c7i * c2iup;
+          double cabi = -c6i * c1rup - c7i * c2rup + c6r * c1iup + c7r * c2iup;
+          S = cadd(S, cmk(cabr * ph.x - cabi * ph.y, cabr * ph.y + cabi * ph.x));
+          cabr = c6r * c11rup + c7r * c12rup + c6i * c11iup + c7i * c12iup;
+          cabi = -c6i * c11rup - c7i * c12rup + c6r * c11iup + c7r * c12iup;
+          const double ua = c6r * U + c7r * UP, ub = c6i * U + c7i * UP;
+          const double akinbr = ua * akinlorup + ub * akinloiup;
+          const double akinbi = ua * akinloiup - ub * akinlorup;
+          H = cadd(H, cmk(cabr * ph.x - cabi * ph.y, cabr * ph.y + cabi * ph.x));
+          H = cadd(H, cmk(akinbr * ph.x - akinbi * ph.y, akinbr * ph.y + akinbi * ph.x));
+        } else {
+          for (int jlop = 1; jlop <= jlo; jlop++) {
+            if (!inlo[jlop]) continue;
+            const double alop = LOV(alo, jlop), blop = LOV(blo, jlop), clop = LOV(clo, jlop);
+            const double c6r = clylr * alop * pi4r2v, c6i = clyli * alop * pi4r2v;
+            const double c7r = clylr * blop * pi4r2v, c7i = clyli * blop * pi4r2v;
+            const double c8r = clylr * clop * pi4r2v, c8i = clyli * clop * pi4r2v;
+            double cr = c6r * c1rup + c6i * c1iup + c7r * c2rup + c7i * c2iup + c8r * c3rup + c8i * c3iup;
+            double ci = -c6i * c1rup + c6r * c1iup - c7i * c2rup + c7r * c2iup - c8i * c3rup + c8r * c3iup;
+            S = cadd(S, cmk(cr * ph.x - ci * ph.y, cr * ph.y + ci * ph.x));
+            cr = c6r * c11rup + c6i * c11iup + c7r * c12rup + c7i * c12iup + c8r * c13rup + c8i * c13iup;
+            ci = -c6i * c11rup + c6r * c11iup - c7i * c12rup + c7r * c12iup - c8i * c13rup + c8r * c13iup;
+            H = cadd(H, cmk(cr * ph.x - ci * ph.y, cr * ph.y + ci * ph.x));
+          }
+        }
+      }
+    }
+  }
+#undef LOV
+  if (J == I) {
+    hs[(size_t)I * ld + I] = H;
+    hsdiag[I] = S;
+  } else {
+    hs[(size_t)I * ld + J] = S;
+    hs[(size_t)J * ld + I] = H;
+  }
+}
+
+// ---------------------------------------------------------------------
+// K-ns operands (hns.F:165-437) for one atom a: right operand R = {ALM, BLM}
+// and left operand L = {A2, B2} in [k][row] layout, plus CLM / C2 of the LO
+// rows.  k = (a*2 + r)*nsl2 + lm.
+// ---------------------------------------------------------------------
+struct LoRange {
+  int jn, l, jlo, i1, i2;  // rows nv+i1..nv+i2 (1-based LO indices)
+};
+
+__global__ void k_hns_ops(DevProb P, const double2* __restrict__ tns, const LoRange* __restrict__ lor, int nlor,
+                          double2* __restrict__ Lop, double2* __restrict__ Rop, double2* __restrict__ Clo,
+                          double2* __restrict__ C2lo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
+  const int a = blockIdx.y;                              // atom
+  const int nsl = P.lnsmax + 1, nsl2 = nsl * nsl;
+  if (i >= P.npad) return;
+  const size_t Kst = (size_t)P.npad;
+  double2* RA = Rop + ((size_t)(a * 2 + 0) * nsl2) * Kst + i;
+  double2* RB = Rop + ((size_t)(a * 2 + 1) * nsl2) * Kst + i;
+  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2) * Kst + i;
+  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2) * Kst + i;
+  if (i >= P.n) {
+    for (int lm = 0; lm < nsl2; lm++) RA[lm * Kst] = RB[lm * Kst] = LA[lm * Kst] = LB[lm * Kst] = cmk(0.0, 0.0);
+    return;
+  }
+  const int jn = P.atype[a];
+  const double pi = 3.141592653589793238462643;
+  const double rhoatm = 4.0 * pi * sqrt(P.vi) * P.rmt[jn] * P.rmt[jn];
+  const double2 ph = P.phase[(size_t)a * P.npad + i];
+  double2 y[25];
+  dev_ylm_row<4>(P.xk[i], P.yk[i], P.zk[i], P.rotij + 9 * a, P.rotloc + 9 * jn, nsl - 1, y);
+  double2 alm[25], blm[25], clm[25];
+  // LO identity of this row for this atom type
+  int myl = -1, myjlo = 0;
+  if (i >= P.nv) {
+    int li = i - P.nv + 1;
+    for (int q = 0; q < nlor; q++)
+      if (lor[q].jn == jn && li >= lor[q].i1 && li <= lor[q].i2) {
+        myl = lor[q].l;
+        myjlo = lor[q].jlo;
+      }
+  }
+  double2 cil = cmk(1.0, 0.0);
+  int lm = 0;
+  for (int l0 = 0; l0 < nsl; l0++) {
+    for (int m0 = -l0; m0 <= l0; m0++, lm++) {
+      double2 tt = cmul(cmul(cil, ph), cconj(y[lm]));
+      double almr = rhoatm * tt.x, almi = rhoatm * tt.y;
+      if (i < P.nv) {
+        size_t o = ((size_t)jn * P.ltop + l0) * P.nvpad + i;
+        double alv = P.al[o], blv = P.bl[o];
+        blm[lm] = cmk(blv * almr, blv * almi);
+        alm[lm] = cmk(alv * almr, alv * almi);
+        clm[lm] = cmk(0.0, 0.0);
+      } else if (l0 == myl) {
+        int oo = (jn * L1G_NLOAT + myjlo - 1) * (L1G_LOMAX + 1) + l0;
+        blm[lm] = cmk(P.blo[oo] * almr, P.blo[oo] * almi);
+        clm[lm] = cmk(P.clo[oo] * almr, P.clo[oo] * almi);
+        alm[lm] = cmk(P.alo[oo] * almr, P.alo[oo] * almi);
+      } else {
+        alm[lm] = blm[lm] = clm[lm] = cmk(0.0, 0.0);
+      }
+    }
+    cil = cmk(-cil.y, cil.x);
+  }
+  // A2/B2/C2 = T (x) conj(ALM/BLM/CLM) summed over (lp,mp) (hns.F:387-433)
+  const double2* T = tns + (size_t)jn * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  for (int la = 0; la < nsl2; la++) {
+    double a2r = 0, a2i = 0, b2r = 0, b2i = 0, c2r = 0, c2i = 0;
+    for (int b = 0; b < nsl2; b++) {
+#define TT(blk) __ldg(&T[((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b])
+      const double2 tuu = TT(0), tdu = TT(1), tuu21 = TT(2), tud = TT(3), tdd = TT(4), tud21 = TT(5),
+                    tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
+#undef TT
+      const double2 A = alm[b], B = blm[b], Cc = clm[b];
+      double t;
+      t = tuu.x * A.x;
+      t = t + tuu.y * A.y;
+      t = t + tdu.x * B.x;
+      t = t + tdu.y * B.y;
+      t = t + tuu21.x * Cc.x;
+      t = t + tuu21.y * Cc.y;
+      a2r = a2r + t;
+      t = tuu.y * A.x;
+      t = t - tuu.x * A.y;
+      t = t - tdu.x * B.y;
+      t = t + tdu.y * B.x;
+      t = t - tuu21.x * Cc.y;
+      t = t + tuu21.y * Cc.x;
+      a2i = a2i + t;
+      t = tud.x * A.x;
+      t = t + tud.y * A.y;
+      t = t + tdd.x * B.x;
+      t = t + tdd.y * B.y;
+      t = t + tud21.x * Cc.x;
+      t = t + tud21.y * Cc.y;
+      b2r = b2r + t;
+      t = tud.y * A.x;
+      t = t - tud.x * A.y;
+      t = t - tdd.x * B.y;
+      t = t + tdd.y * B.x;
+      t = t - tud21.x * Cc.y;
+      t = t + tud21.y * Cc.x;
+      b2i = b2i + t;
+      t = tuu12.x * A.x;
+      t = t + tuu12.y * A.y;
+      t = t + tdu12.x * B.x;
+      t = t + tdu12.y * B.y;
+      t = t + tuu22.x * Cc.x;
+      t = t + tuu22.y * Cc.y;
+      c2r = c2r + t;
+      t = tuu12.y * A.x;
+      t = t - tuu12.x * A.y;
+      t = t - tdu12.x * B.y;
+      t = t + tdu12.y * B.x;
+      t = t - tuu22.x * Cc.y;
+      t = t + tuu22.y * Cc.x;
+      c2i = c2i + t;
+    }
+    RA[la * Kst] = alm[la];
+    RB[la * Kst] = blm[la];
+    LA[la * Kst] = cmk(a2r, a2i);
+    LB[la * Kst] = cmk(b2r, b2i);
+    if (i >= P.nv) {
+      size_t oc = ((size_t)a * nsl2 + la) * (size_t)(P.nlo > 0 ? P.nlo : 1) + (i - P.nv);
+      Clo[oc] = clm[la];
+      C2lo[oc] = cmk(c2r, c2i);
+    }
+  }
+}
+
+// HS(i,j) += sum_k Lop[k][i] * Rop[k][j] on the lower triangle i >= j
+// (zher2m.f:69-80, 'L','N','T').  64x64 tiles, 4x4 complex per thread.
+#define HNS_T 64
+#define HNS_KT 16
+__global__ void __launch_bounds__(256, 2)
+    k_hns_gemm(int n, int npad, int K, const int2* __restrict__ tiles, const double2* __restrict__ Lop,
+               const double2* __restrict__ Rop, double2* __restrict__ hs, int ld) {
+  __shared__ double2 sL[HNS_KT][HNS_T];
+  __shared__ double2 sR[HNS_KT][HNS_T];
+  const int tid = threadIdx.x, ti = tid & 15, tj = tid >> 4;
+  const int2 t = tiles[blockIdx.x];
+  const int i0 = t.x * HNS_T, j0 = t.y * HNS_T;
+  double2 acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) acc[u][v] = cmk(0.0, 0.0);
+  for (int k0 = 0; k0 < K; k0 += HNS_KT) {
+    __syncthreads();
+    for (int idx = tid; idx < HNS_KT * HNS_T; idx += 256) {
+      int kk = idx / HNS_T, r = idx % HNS_T;
+      int k = k0 + kk;
+      double2 lv = cmk(0.0, 0.0), rv = cmk(0.0, 0.0);
+      if (k < K) {
+        lv = Lop[(size_t)k * npad + i0 + r];
+        rv = Rop[(size_t)k * npad + j0 + r];
+      }
+      sL[kk][r] = lv;
+      sR[kk][r] = rv;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < HNS_KT; kk++) {
+      double2 lv[4], rv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) lv[u] = sL[kk][ti * 4 + u];
+#pragma unroll
+      for (int v = 0; v < 4; v++) rv[v] = sR[kk][tj * 4 + v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          acc[u][v].x = fma(lv[u].x, rv[v].x, acc[u][v].x);
+          acc[u][v].x = fma(-lv[u].y, rv[v].y, acc[u][v].x);
+          acc[u][v].y = fma(lv[u].x, rv[v].y, acc[u][v].y);
+          acc[u][v].y = fma(lv[u].y, rv[v].x, acc[u][v].y);
+        }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    int j = j0 + tj * 4 + v;
+    if (j >= n) continue;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      int i = i0 + ti * 4 + u;
+      if (i >= n || i < j) continue;
+      double2* dst = hs + (size_t)j * ld + i;
+      *dst = cadd(*dst, acc[u][v]);
+    }
+  }
+}
+
+// LO block of HNS: HS(i,j) += sum C2[k][i] CLM[k][j], nv <= j <= i < n
+__global__ void k_hns_lo(int nv, int nlo, int K, const double2* __restrict__ C2lo, const double2* __restrict__ Clo,
+                         double2* __restrict__ hs, int ld) {
+  int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  int cj = blockIdx.y;
+  if (ci >= nlo || ci < cj) return;
+  double2 s = cmk(0.0, 0.0);
+  for (int k = 0; k < K; k++) {
+    double2 a = C2lo[(size_t)k * nlo + ci], b = Clo[(size_t)k * nlo + cj];
+    s = cadd(s, cmul(a, b));
+  }
+  double2* dst = hs + (size_t)(nv + cj) * ld + (nv + ci);
+  *dst = cadd(*dst, s);
+}
+
+// ---------------------------------------------------------------------
+// K-orb: HORB (horb.F:98-297) for one (U-atom a, l = lvor)
+// ---------------------------------------------------------------------
+__global__ void k_horb_rows(DevProb P, int a, int lvor, const double2* __restrict__ pot /*[7][7] pot(m2,m1)*/,
+                            const LoRange* __restrict__ lor, int nlor, double2* __restrict__ alm,
+                            double2* __restrict__ blm, double2* __restrict__ clm) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const int jn = P.atype[a];
+  const double pi = 3.141592653589793238462643;
+  const double rhoatm = 4.0 * pi * sqrt(P.vi) * P.rmt[jn] * P.rmt[jn];
+  const double* r = P.pos + 3 * a;
+  double arg = (r[0] * P.kzz[3 * i] + r[1] * P.kzz[3 * i + 1] + r[2] * P.kzz[3 * i + 2]);
+  double2 ph = cexp2pi(arg);
+  double2 y[16];
+  dev_ylm_row<3>(P.xk[i], P.yk[i], P.zk[i], P.rotij + 9 * a, P.rotloc + 9 * jn, lvor, y);
+  double2 cil = cmk(1.0, 0.0);
+  for (int q = 0; q < lvor; q++) cil = cmk(-cil.y, cil.x);
+  int myjlo = 0;
+  if (i >= P.nv) {
+    int li = i - P.nv + 1;
+    for (int q = 0; q < nlor; q++)
+      if (lor[q].jn == jn && lor[q].l == lvor && li >= lor[q].i1 && li <= lor[q].i2) myjlo = lor[q].jlo;
+  }
+  for (int m = -3; m <= 3; m++) {
+    double2 A = cmk(0, 0), B = A, Cc = A;
+    if (m >= -lvor && m <= lvor) {
+      int lm = lvor * (lvor + 1) + m;
+      double2 t1 = cmul(cmul(cscale(cil, rhoatm), ph), cconj(y[lm]));
+      if (i < P.nv) {
+        size_t o = ((size_t)jn * P.ltop + lvor) * P.nvpad + i;
+        A = cscale(t1, P.al[o]);
+        B = cscale(t1, P.bl[o]);
+      } else if (myjlo > 0) {
+        int oo = (jn * L1G_NLOAT + myjlo - 1) * (L1G_LOMAX + 1) + lvor;
+        B = cscale(t1, P.blo[oo]);
+        Cc = cscale(t1, P.clo[oo]);
+        A = cscale(t1, P.alo[oo]);
+      }
+    }
+    alm[(size_t)i * 7 + m + 3] = A;
+    blm[(size_t)i * 7 + m + 3] = B;
+    clm[(size_t)i * 7 + m + 3] = Cc;
+  }
+}
+
+__global__ void k_horb_pairs(DevProb P, int a, int lvor, const double2* __restrict__ pot, const LoRange* __restrict__ lor,
+                             int nlor, const double2* __restrict__ alm, const double2* __restrict__ blm,
+                             const double2* __restrict__ clm, double2* __restrict__ hs, int ld) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (i >= P.n || i < j) return;
+  const int jn = P.atype[a], nv = P.nv;
+  const int o = jn * P.ldl + lvor;
+  const double peil = P.pei[o];
+  const double pi12 = lvor <= L1G_LOMAX ? P.pi12lo[jn * (L1G_LOMAX + 1) + lvor] : 0.0;
+  const double pe12 = lvor <= L1G_LOMAX ? P.pe12lo[jn * (L1G_LOMAX + 1) + lvor] : 0.0;
+#define POT(m1, m0) pot[((m1) + 3) * 7 + (m0) + 3]
+#define AL7(mm, r) alm[(size_t)(r)*7 + (mm) + 3]
+#define BL7(mm, r) blm[(size_t)(r)*7 + (mm) + 3]
+#define CL7(mm, r) clm[(size_t)(r)*7 + (mm) + 3]
+  double2 add = cmk(0.0, 0.0);
+  bool hit = false;
+  if (i < nv && j < nv) {
+    double2 t4 = cmk(0, 0), t5 = cmk(0, 0);
+    for (int m0 = -lvor; m0 <= lvor; m0++) {
+      double2 t1 = cmk(0, 0), t2 = cmk(0, 0);
+      for (int m1 = -lvor; m1 <= lvor; m1++) {
+        t1 = cadd(t1, cmul(POT(m1, m0), AL7(m1, j)));
+        t2 = cadd(t2, cmul(POT(m1, m0), BL7(m1, j)));
+      }
+      t2 = cscale(t2, peil);
+      t4 = cadd(t4, cmul(t1, cconj(AL7(m0, i))));
+      t5 = cadd(t5, cmul(t2, cconj(BL7(m0, i))));
+    }
+    add = cadd(t4, t5);
+    hit = true;
+  } else if (i >= nv && lvor <= L1G_LOMAX) {
+    int li = i - nv + 1, lj = j - nv + 1;
+    int jlo_i = 0, i22 = 0, jlo_j = 0;
+    for (int q = 0; q < nlor; q++) {
+      if (lor[q].jn == jn && lor[q].l == lvor && li >= lor[q].i1 && li <= lor[q].i2) jlo_i = lor[q].jlo;
+      if (j >= nv && lor[q].jn == jn && lor[q].l == lvor && lj >= lor[q].i1 && lj <= lor[q].i2) {
+        jlo_j = lor[q].jlo;
+        i22 = lor[q].i2;
+      }
+    }
+    if (jlo_i > 0 && j < nv) {  // <APW||LO>
+      double2 t4 = cmk(0, 0), t5 = t4, t6 = t4, t7 = t4;
+      for (int m0 = -lvor; m0 <= lvor; m0++) {
+        double2 t1 = cmk(0, 0), t2 = cmk(0, 0);
+        for (int m1 = -lvor; m1 <= lvor; m1++) {
+          t1 = cadd(t1, cmul(AL7(m1, j), POT(m1, m0)));
+          t2 = cadd(t2, cmul(BL7(m1, j), POT(m1, m0)));
+        }
+        t4 = cadd(t4, cmul(t1, cconj(AL7(m0, i))));
+        t5 = cadd(t5, cmul(t2, cconj(BL7(m0, i))));
+        t6 = cadd(t6, cmul(t1, cconj(CL7(m0, i))));
+        t7 = cadd(t7, cmul(t2, cconj(CL7(m0, i))));
+      }
+      add = cadd(cadd(cadd(t4, cscale(t5, peil)), cscale(t6, pi12)), cscale(t7, pe12));
+      hit = true;
+    } else if (jlo_i > 0 && jlo_j > 0 && jlo_j <= jlo_i && lj <= i22) {  // <LO||LO>
+      double2 t4 = cmk(0, 0), t5 = t4, t6 = t4, t7 = t4;
+      for (int m0 = -lvor; m0 <= lvor; m0++) {
+        double2 t1 = cmk(0, 0), t2 = t1, t3 = t1;
+        for (int m1 = -lvor; m1 <= lvor; m1++) {
+          t1 = cadd(t1, cmul(POT(m1, m0), AL7(m1, j)));
+          t2 = cadd(t2, cmul(POT(m1, m0), BL7(m1, j)));
+          t3 = cadd(t3, cmul(POT(m1, m0), CL7(m1, j)));
+        }
+        t4 = cadd(cadd(t4, cmul(t1, cconj(AL7(m0, i)))), cmul(cconj(CL7(m0, i)), t3));
+        t5 = cadd(t5, cmul(cconj(BL7(m0, i)), t2));
+        t6 = cadd(cadd(t6, cmul(cconj(CL7(m0, i)), t1)), cmul(cconj(AL7(m0, i)), t3));
+        t7 = cadd(cadd(t7, cmul(cconj(BL7(m0, i)), t3)), cmul(cconj(CL7(m0, i)), t2));
+      }
+      add = cadd(cadd(cadd(cscale(t5, peil), cscale(t6, pi12)), cscale(t7, pe12)), t4);
+      hit = true;
+    }
+  }
+#undef POT
+#undef AL7
+#undef BL7
+#undef CL7
+  if (hit) {
+    double2* dst = hs + (size_t)j * ld + i;
+    *dst = cadd(*dst, add);
+  }
+}
+
+// non-finite scan of the n x n block and hsdiag
+__global__ void k_check_finite(int n, const double2* __restrict__ hs, int ld, const double2* __restrict__ hsdiag,
+                               int* status) {
+  size_t tot = (size_t)n * n;
+  bool bad = false;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    size_t j = q / n, i = q % n;
+    double2 v = hs[j * ld + i];
+    if (!isfinite(v.x) || !isfinite(v.y)) bad = true;
+    if (j == 0) {
+      double2 d = hsdiag[i];
+      if (!isfinite(d.x) || !isfinite(d.y)) bad = true;
+    }
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, L1G_STATUS_NONFINITE);
+}

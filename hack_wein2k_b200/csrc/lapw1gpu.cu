@@ -1,0 +1,754 @@
+// lapw1gpu.cu -- C ABI of the B200 lapw1 H/S setup (include/lapw1gpu.h).
+//
+// Host side: context (stream, events, grow-only device buffers), upload of
+// one k-point's inputs, and the stage sequence of calkpt.F:153-185:
+//   HAMILT  -> k_albl, k_phase, k_table, k_sph_coef, k_spherical, k_lo
+//   ZSWAP   -> folded into the HAMILT writes (diag(HS) = H, HSDIAG = S)
+//   HNS     -> k_hns_ops, k_hns_gemm (FP64) or the split-precision tcgen05
+//              path, k_hns_lo
+//   HORB    -> k_horb_rows, k_horb_pairs per U-atom and l
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels_fp64.cuh"
+
+#define L1G_VERSION "lapw1gpu 0.1 (sm_100a)"
+
+namespace {
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct lapw1gpu_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[12] = {};
+  int* d_status = nullptr;
+  int last_status = 0;
+  int prec = LAPW1GPU_PREC_FP64;
+  int slices = 6;
+  bool sph_attr = false;
+  std::map<std::string, DevBuf> bufs;
+
+  // grow-only scratch buffer; returns nullptr on allocation failure
+  void* buf(const char* name, size_t bytes) {
+    DevBuf& b = bufs[name];
+    if (bytes == 0) bytes = 16;
+    if (b.bytes < bytes) {
+      if (b.ptr) cudaFree(b.ptr);
+      b.ptr = nullptr;
+      b.bytes = 0;
+      if (cudaMalloc(&b.ptr, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+      b.bytes = bytes;
+    }
+    return b.ptr;
+  }
+};
+
+#include "split_tc.cuh"
+
+struct lapw1gpu_kpoint {
+  lapw1gpu_context* ctx = nullptr;
+  // host copies of sizes and small tables
+  int n = 0, nv = 0, nlo = 0, nat = 0, ndf = 0, ltop = 0, ldl = 0, lnsmax = 0, ins = 0, nohns = 0;
+  int nvpad = 0, npad = 0;
+  double vi = 0.0;
+  TabDesc tab{};
+  std::vector<LoCol> locols;
+  std::vector<LoRange> loranges;
+  std::vector<int> mult, atype, afirst;
+  // HORB description
+  struct OrbItem {
+    int a, lvor, iat;
+  };
+  std::vector<OrbItem> orbs;
+  std::vector<double2> pots;  // [norb][49] pot(m1,m0) arrays
+  // device inputs (one arena)
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  bool owns_arena = true;
+  DevProb P{};
+  const double2* d_warp = nullptr;
+  const double2* d_tns = nullptr;
+  const LoCol* d_locols = nullptr;
+  const LoRange* d_loranges = nullptr;
+  const double2* d_pots = nullptr;
+};
+
+namespace {
+
+#define CK(x)                                 \
+  do {                                        \
+    cudaError_t _e = (x);                     \
+    if (_e != cudaSuccess) {                  \
+      cudaGetLastError();                     \
+      return LAPW1GPU_ERR_CUDA;               \
+    }                                         \
+  } while (0)
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// validation of the caller's problem (the checks the reference makes by
+// array bounds and STOPs: param.inc limits, sizes consistent)
+int validate(const lapw1gpu_problem* p) {
+  if (!p) return LAPW1GPU_ERR_ARG;
+  if (p->nv < 1 || p->nlo < 0 || p->n != p->nv + p->nlo || p->nat < 1 || p->ndf < p->nat) return LAPW1GPU_ERR_ARG;
+  if (p->ltop < 3 || p->ltop > L1G_MAXL || p->ldl < p->ltop) return LAPW1GPU_ERR_RANGE;
+  if (p->lnsmax < 0 || p->lnsmax > 4 || p->lnsmax + 1 > p->ltop) return LAPW1GPU_ERR_RANGE;
+  if (!p->mult || !p->rmt || !p->v || !p->pos || !p->rotij || !p->rotloc || !p->kzz || !p->xk || !p->yk ||
+      !p->zk || !p->rk || !p->p || !p->pe || !p->dp || !p->dpe || !p->pei || !p->e || !p->lapw || !p->ilo ||
+      !p->loor || !p->alo || !p->blo || !p->clo || !p->elo || !p->pi12lo || !p->pe12lo || !p->dplo)
+    return LAPW1GPU_ERR_ARG;
+  if (p->ins == 0 && !p->warp) return LAPW1GPU_ERR_ARG;
+  if (!p->nohns && !p->tns) return LAPW1GPU_ERR_ARG;
+  int ndf = 0;
+  for (int a = 0; a < p->nat; a++) {
+    if (p->mult[a] < 1) return LAPW1GPU_ERR_ARG;
+    ndf += p->mult[a];
+  }
+  if (ndf != p->ndf) return LAPW1GPU_ERR_ARG;
+  long nlo = 0;
+  for (int a = 0; a < p->nat; a++)
+    for (int l = 0; l <= L1G_LOMAX; l++) {
+      int il = p->ilo[a * (L1G_LOMAX + 1) + l];
+      if (il < 0 || il > L1G_NLOAT) return LAPW1GPU_ERR_RANGE;
+      nlo += (long)(2 * l + 1) * p->mult[a] * il;
+    }
+  if (nlo != p->nlo) return LAPW1GPU_ERR_ARG;
+  if (p->natorb < 0) return LAPW1GPU_ERR_ARG;
+  if (p->natorb > 0 && (!p->iatom || !p->nlorb || !p->lorb || !p->vorb)) return LAPW1GPU_ERR_ARG;
+  for (int i = 0; i < p->natorb; i++) {
+    if (p->iatom[i] < 1 || p->iatom[i] > p->nat) return LAPW1GPU_ERR_ARG;
+    if (i > 0 && p->iatom[i] <= p->iatom[i - 1]) return LAPW1GPU_ERR_ARG;  // horb.F:100 walks them in order
+    if (p->nlorb[i] < 0 || p->nlorb[i] > 3) return LAPW1GPU_ERR_RANGE;
+    for (int q = 0; q < p->nlorb[i]; q++)
+      if (p->lorb[i * 3 + q] < 0 || p->lorb[i * 3 + q] > 3 || p->lorb[i * 3 + q] >= p->ltop) return LAPW1GPU_ERR_RANGE;
+  }
+  return LAPW1GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lapw1gpu_version(void) { return L1G_VERSION; }
+
+int lapw1gpu_init(int device, lapw1gpu_context** out) {
+  if (!out) return LAPW1GPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return LAPW1GPU_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return LAPW1GPU_ERR_NODEVICE;
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return LAPW1GPU_ERR_NODEVICE;  // built for sm_100a only
+  CK(cudaSetDevice(device));
+  lapw1gpu_context* c = new lapw1gpu_context();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return LAPW1GPU_ERR_CUDA;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return LAPW1GPU_ERR_NOMEM;
+  }
+  cudaMemset(c->d_status, 0, sizeof(int));
+  *out = c;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_finalize(lapw1gpu_context* c) {
+  if (!c) return LAPW1GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->bufs)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  if (c->d_status) cudaFree(c->d_status);
+  for (auto& e : c->ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_set_precision(lapw1gpu_context* c, int prec, int slices) {
+  if (!c) return LAPW1GPU_ERR_ARG;
+  if (prec != LAPW1GPU_PREC_FP64 && prec != LAPW1GPU_PREC_SPLIT) return LAPW1GPU_ERR_ARG;
+  if (prec == LAPW1GPU_PREC_SPLIT && (slices < 2 || slices > L1G_MAX_SLICES)) return LAPW1GPU_ERR_RANGE;
+  c->prec = prec;
+  if (prec == LAPW1GPU_PREC_SPLIT) c->slices = slices;
+  return LAPW1GPU_OK;
+}
+
+void* lapw1gpu_stream(lapw1gpu_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int lapw1gpu_last_status(lapw1gpu_context* c) { return c ? c->last_status : 0; }
+
+}  // extern "C"
+
+static int kpoint_upload_impl(lapw1gpu_context* ctx, const lapw1gpu_problem* p, lapw1gpu_kpoint** out,
+                              bool borrow) {
+  if (!ctx || !out) return LAPW1GPU_ERR_ARG;
+  *out = nullptr;
+  int rc = validate(p);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  lapw1gpu_kpoint* k = new lapw1gpu_kpoint();
+  k->ctx = ctx;
+  k->n = p->n;
+  k->nv = p->nv;
+  k->nlo = p->nlo;
+  k->nat = p->nat;
+  k->ndf = p->ndf;
+  k->ltop = p->ltop;
+  k->ldl = p->ldl;
+  k->lnsmax = p->lnsmax;
+  k->ins = p->ins;
+  k->nohns = p->nohns;
+  k->vi = p->vi;
+  k->nvpad = round_up(p->nv, 64);
+  k->npad = round_up(p->n, 64);
+  k->mult.assign(p->mult, p->mult + p->nat);
+  k->afirst.resize(p->nat);
+  k->atype.resize(p->ndf);
+  for (int a = 0, q = 0; a < p->nat; a++) {
+    k->afirst[a] = q;
+    for (int e = 0; e < p->mult[a]; e++) k->atype[q++] = a;
+  }
+  // difference-vector box of the PW rows and the WARP extents
+  int kmin[3] = {1 << 30, 1 << 30, 1 << 30}, kmax[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+  for (int i = 0; i < p->nv; i++)
+    for (int c = 0; c < 3; c++) {
+      kmin[c] = std::min(kmin[c], p->kzz[3 * i + c]);
+      kmax[c] = std::max(kmax[c], p->kzz[3 * i + c]);
+    }
+  k->tab.d1 = kmax[0] - kmin[0];
+  k->tab.d2 = kmax[1] - kmin[1];
+  k->tab.d3 = kmax[2] - kmin[2];
+  k->tab.w1 = p->warp1;
+  k->tab.w2 = p->warp2;
+  k->tab.w3 = p->warp3;
+  for (int q = 0; q < 9; q++) k->tab.bk[q] = p->bkzz[q];
+  // LO columns in the order of hamilt.F:495-791 and LOHNS ranges
+  {
+    int nnlo = 0;
+    for (int jn = 0; jn < p->nat; jn++) {
+      double clr = 1.0, cli = 0.0;
+      for (int l = 0; l <= L1G_LOMAX; l++) {
+        int nil = p->ilo[jn * (L1G_LOMAX + 1) + l];
+        for (int jlo = 1; jlo <= nil; jlo++) {
+          LoRange r;
+          r.jn = jn;
+          r.l = l;
+          r.jlo = jlo;
+          r.i1 = nnlo + 1;
+          for (int jeqo = 1; jeqo <= p->mult[jn]; jeqo++)
+            for (int mo1 = -l; mo1 <= l; mo1++) {
+              nnlo++;
+              LoCol cc;
+              cc.jn = jn;
+              cc.l = l;
+              cc.jlo = jlo;
+              cc.jeqo = jeqo;
+              cc.mo1 = mo1;
+              cc.nnlo = nnlo;
+              cc.a0 = k->afirst[jn];
+              cc.clr = clr;
+              cc.cli = cli;
+              k->locols.push_back(cc);
+            }
+          r.i2 = nnlo;
+          k->loranges.push_back(r);
+        }
+        double t = clr;
+        clr = -cli;
+        cli = t;
+      }
+    }
+  }
+  // HORB items in the reference's order (horb.F:98-113): atom type, then
+  // equivalent atom, then l; pot(m2,m1) = vorb(iat,lvor,m1,m2)
+  for (int i = 0; i < p->natorb; i++) {
+    int jn = p->iatom[i] - 1;
+    int pot0 = (int)(k->pots.size() / 49);
+    for (int q = 0; q < p->nlorb[i]; q++) {
+      int lv = p->lorb[i * 3 + q];
+      std::vector<double2> pot(49, make_double2(0, 0));
+      for (int m1 = -lv; m1 <= lv; m1++)
+        for (int m2 = -lv; m2 <= lv; m2++) {
+          size_t o = (((size_t)i * 4 + lv) * 7 + (m1 + 3)) * 7 + (m2 + 3);
+          pot[(m2 + 3) * 7 + (m1 + 3)] = make_double2(p->vorb[2 * o], p->vorb[2 * o + 1]);
+        }
+      k->pots.insert(k->pots.end(), pot.begin(), pot.end());
+    }
+    for (int e = 0; e < p->mult[jn]; e++)
+      for (int q = 0; q < p->nlorb[i]; q++) {
+        lapw1gpu_kpoint::OrbItem it{k->afirst[jn] + e, p->lorb[i * 3 + q], pot0 + q};
+        k->orbs.push_back(it);
+      }
+  }
+  // one arena for all device inputs
+  struct Seg {
+    const void* src;
+    size_t bytes;
+    size_t off;
+  };
+  std::vector<Seg> segs;
+  size_t off = 0;
+  auto add = [&](const void* src, size_t bytes) -> size_t {
+    size_t o = off;
+    segs.push_back({src, bytes, o});
+    off += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const int nat = p->nat, ndf = p->ndf, n = p->n, ldl = p->ldl;
+  const int L4 = L1G_LOMAX + 1;
+  size_t o_mult = add(p->mult, sizeof(int) * nat);
+  size_t o_atype = add(k->atype.data(), sizeof(int) * ndf);
+  size_t o_afirst = add(k->afirst.data(), sizeof(int) * nat);
+  size_t o_rmt = add(p->rmt, sizeof(double) * nat);
+  size_t o_v = add(p->v, sizeof(double) * nat);
+  size_t o_pos = add(p->pos, sizeof(double) * 3 * ndf);
+  size_t o_rotij = add(p->rotij, sizeof(double) * 9 * ndf);
+  size_t o_rotloc = add(p->rotloc, sizeof(double) * 9 * nat);
+  size_t o_kzz = add(p->kzz, sizeof(int) * 3 * n);
+  size_t o_xk = add(p->xk, sizeof(double) * n);
+  size_t o_yk = add(p->yk, sizeof(double) * n);
+  size_t o_zk = add(p->zk, sizeof(double) * n);
+  size_t o_rk = add(p->rk, sizeof(double) * n);
+  size_t o_p = add(p->p, sizeof(double) * nat * ldl);
+  size_t o_pe = add(p->pe, sizeof(double) * nat * ldl);
+  size_t o_dp = add(p->dp, sizeof(double) * nat * ldl);
+  size_t o_dpe = add(p->dpe, sizeof(double) * nat * ldl);
+  size_t o_pei = add(p->pei, sizeof(double) * nat * ldl);
+  size_t o_e = add(p->e, sizeof(double) * nat * ldl);
+  size_t o_lapw = add(p->lapw, sizeof(int) * nat * ldl);
+  size_t o_ilo = add(p->ilo, sizeof(int) * nat * L4);
+  size_t o_loor = add(p->loor, sizeof(int) * nat * L4);
+  size_t o_alo = add(p->alo, sizeof(double) * nat * L1G_NLOAT * L4);
+  size_t o_blo = add(p->blo, sizeof(double) * nat * L1G_NLOAT * L4);
+  size_t o_clo = add(p->clo, sizeof(double) * nat * L1G_NLOAT * L4);
+  size_t o_elo = add(p->elo, sizeof(double) * nat * L1G_NLOAT * L4);
+  size_t o_pi12 = add(p->pi12lo, sizeof(double) * nat * L4);
+  size_t o_pe12 = add(p->pe12lo, sizeof(double) * nat * L4);
+  size_t o_dplo = add(p->dplo, sizeof(double) * nat * L4);
+  size_t nwarp = (size_t)(2 * p->warp1 + 1) * (2 * p->warp2 + 1) * (2 * p->warp3 + 1);
+  size_t o_warp = add(p->ins == 0 ? (const void*)p->warp : nullptr, p->ins == 0 ? sizeof(double2) * nwarp : 16);
+  size_t ntns = (size_t)nat * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  size_t o_tns = add(p->nohns ? nullptr : (const void*)p->tns, p->nohns ? 16 : sizeof(double2) * ntns);
+  size_t o_locol = add(k->locols.data(), sizeof(LoCol) * std::max<size_t>(1, k->locols.size()));
+  size_t o_lor = add(k->loranges.data(), sizeof(LoRange) * std::max<size_t>(1, k->loranges.size()));
+  size_t o_pots = add(k->pots.data(), sizeof(double2) * std::max<size_t>(1, k->pots.size()));
+  if (borrow) {
+    // one-shot host entry point: reuse the context's grow-only arena
+    k->arena = ctx->buf("arena", off);
+    k->owns_arena = false;
+    if (!k->arena) {
+      delete k;
+      return LAPW1GPU_ERR_NOMEM;
+    }
+  } else if (cudaMalloc(&k->arena, off) != cudaSuccess) {
+    cudaGetLastError();
+    delete k;
+    return LAPW1GPU_ERR_NOMEM;
+  }
+  k->arena_bytes = off;
+  char* base = (char*)k->arena;
+  int crc = LAPW1GPU_OK;
+  for (auto& s : segs)
+    if (s.src && s.bytes && crc == LAPW1GPU_OK)
+      if (cudaMemcpyAsync(base + s.off, s.src, s.bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        crc = LAPW1GPU_ERR_CUDA;
+  if (crc == LAPW1GPU_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) crc = LAPW1GPU_ERR_CUDA;
+  if (crc != LAPW1GPU_OK) {
+    cudaGetLastError();
+    if (k->owns_arena) cudaFree(k->arena);
+    delete k;
+    return crc;
+  }
+  DevProb& P = k->P;
+  P.n = n;
+  P.nv = p->nv;
+  P.nlo = p->nlo;
+  P.nat = nat;
+  P.ndf = ndf;
+  P.ltop = p->ltop;
+  P.ldl = ldl;
+  P.lnsmax = p->lnsmax;
+  P.ins = p->ins;
+  P.nvpad = k->nvpad;
+  P.npad = k->npad;
+  P.vi = p->vi;
+#define SEGP(T, o) reinterpret_cast<T>(base + (o))
+  P.mult = SEGP(const int*, o_mult);
+  P.atype = SEGP(const int*, o_atype);
+  P.afirst = SEGP(const int*, o_afirst);
+  P.rmt = SEGP(const double*, o_rmt);
+  P.v = SEGP(const double*, o_v);
+  P.pos = SEGP(const double*, o_pos);
+  P.rotij = SEGP(const double*, o_rotij);
+  P.rotloc = SEGP(const double*, o_rotloc);
+  P.kzz = SEGP(const int*, o_kzz);
+  P.xk = SEGP(const double*, o_xk);
+  P.yk = SEGP(const double*, o_yk);
+  P.zk = SEGP(const double*, o_zk);
+  P.rk = SEGP(const double*, o_rk);
+  P.p = SEGP(const double*, o_p);
+  P.pe = SEGP(const double*, o_pe);
+  P.dp = SEGP(const double*, o_dp);
+  P.dpe = SEGP(const double*, o_dpe);
+  P.pei = SEGP(const double*, o_pei);
+  P.e = SEGP(const double*, o_e);
+  P.lapw = SEGP(const int*, o_lapw);
+  P.ilo = SEGP(const int*, o_ilo);
+  P.loor = SEGP(const int*, o_loor);
+  P.alo = SEGP(const double*, o_alo);
+  P.blo = SEGP(const double*, o_blo);
+  P.clo = SEGP(const double*, o_clo);
+  P.elo = SEGP(const double*, o_elo);
+  P.pi12lo = SEGP(const double*, o_pi12);
+  P.pe12lo = SEGP(const double*, o_pe12);
+  P.dplo = SEGP(const double*, o_dplo);
+  k->d_warp = SEGP(const double2*, o_warp);
+  k->d_tns = SEGP(const double2*, o_tns);
+  k->d_locols = SEGP(const LoCol*, o_locol);
+  k->d_loranges = SEGP(const LoRange*, o_lor);
+  k->d_pots = SEGP(const double2*, o_pots);
+#undef SEGP
+  *out = k;
+  return LAPW1GPU_OK;
+}
+
+extern "C" {
+
+int lapw1gpu_kpoint_upload(lapw1gpu_context* ctx, const lapw1gpu_problem* p, lapw1gpu_kpoint** out) {
+  return kpoint_upload_impl(ctx, p, out, false);
+}
+
+int lapw1gpu_kpoint_free(lapw1gpu_kpoint* k) {
+  if (!k) return LAPW1GPU_ERR_ARG;
+  if (k->arena && k->owns_arena) {
+    cudaSetDevice(k->ctx->device);
+    cudaStreamSynchronize(k->ctx->stream);
+    cudaFree(k->arena);
+  }
+  delete k;
+  return LAPW1GPU_OK;
+}
+
+// tile lists (device) for the triangle kernels, cached per shape in the context
+static const int2* tiles_sph(lapw1gpu_context* c, int nv, int* count) {
+  int nbi = (nv + SPH_TI - 1) / SPH_TI;
+  std::vector<int2> t;
+  for (int bi = 0; bi < nbi; bi++) {
+    int bjmax = (bi * SPH_TI + SPH_TI - 1) / SPH_TJ;
+    for (int bj = 0; bj <= bjmax; bj++) t.push_back(make_int2(bi, bj));
+  }
+  *count = (int)t.size();
+  int2* d = (int2*)c->buf("tiles_sph", sizeof(int2) * t.size());
+  if (!d) return nullptr;
+  if (cudaMemcpyAsync(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return nullptr;
+  return d;
+}
+
+static const int2* tiles_tri(lapw1gpu_context* c, const char* name, int n, int T, int* count) {
+  int nb = (n + T - 1) / T;
+  std::vector<int2> t;
+  for (int bi = 0; bi < nb; bi++)
+    for (int bj = 0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
+  *count = (int)t.size();
+  int2* d = (int2*)c->buf(name, sizeof(int2) * t.size());
+  if (!d) return nullptr;
+  if (cudaMemcpyAsync(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return nullptr;
+  return d;
+}
+
+// algorithmic FP64-equivalent flops of the contractions (see DESIGN.md roofline)
+static double alg_flops(const lapw1gpu_kpoint* k) {
+  double nv = k->nv, n = k->n;
+  double sph = 8.0 * 2.0 * (2.0 * k->ndf) * k->ltop * (nv * (nv + 1) / 2.0);  // H and S, lower triangle
+  int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
+  double hns = k->nohns ? 0.0 : 8.0 * (2.0 * k->ndf * nsl2) * (n * (n + 1) / 2.0);
+  return sph + hns;
+}
+
+int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, double* d_hs_, int ldhs,
+                        double* d_hsdiag_, lapw1gpu_stats* st) {
+  if (!c || !k || !d_hs_ || !d_hsdiag_ || ldhs < k->n || k->ctx != c) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  double2* d_hs = reinterpret_cast<double2*>(d_hs_);
+  double2* d_hsdiag = reinterpret_cast<double2*>(d_hsdiag_);
+  cudaStream_t s = c->stream;
+  DevProb P = k->P;
+  const int n = k->n, nv = k->nv, ltop = k->ltop, ndf = k->ndf, nat = k->nat;
+  P.al = (double*)c->buf("al", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.bl = (double*)c->buf("bl", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.phase = (double2*)c->buf("phase", sizeof(double2) * (size_t)ndf * k->npad);
+  if (!P.al || !P.bl || !P.phase) return LAPW1GPU_ERR_NOMEM;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  if (st) CK(cudaEventRecord(c->ev[0], s));
+  int nl = 0;  // kernels launched by this run
+
+  // ---- K-a: matching coefficients and phases (always needed) ----
+  nl++;
+  k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
+  nl++;
+  k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
+  CK(cudaGetLastError());
+  if (st) CK(cudaEventRecord(c->ev[1], s));
+
+  if (stages & 1) {
+    // ---- K-c table + K-b spherical ----
+    size_t ntab = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
+    double2* tab = (double2*)c->buf("tab", sizeof(double2) * 2 * ntab);
+    SphCoef* coef = (SphCoef*)c->buf("coef", sizeof(SphCoef) * nat * ltop);
+    if (!tab || !coef) return LAPW1GPU_ERR_NOMEM;
+    nl++;
+    k_table<<<(unsigned)((ntab + 127) / 128), 128, 0, s>>>(P, k->tab, k->d_warp, tab);
+    nl++;
+    k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
+    int ntiles = 0;
+    const int2* tl = tiles_sph(c, nv, &ntiles);
+    if (!tl) return LAPW1GPU_ERR_NOMEM;
+    if (!c->sph_attr) {  // function attributes are per device: once per context
+      CK(cudaFuncSetAttribute(k_spherical, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
+      c->sph_attr = true;
+    }
+    nl++;
+    k_spherical<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, tab, k->tab, d_hs, ldhs, d_hsdiag);
+    CK(cudaGetLastError());
+    if (st) CK(cudaEventRecord(c->ev[2], s));
+    // ---- K-b': local-orbital columns ----
+    if (k->nlo > 0) nl++;
+    if (k->nlo > 0) k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag);
+    CK(cudaGetLastError());
+    if (st) CK(cudaEventRecord(c->ev[3], s));
+  } else if (st) {
+    CK(cudaEventRecord(c->ev[2], s));
+    CK(cudaEventRecord(c->ev[3], s));
+  }
+
+  if ((stages & 2) && !k->nohns) {
+    // ---- K-ns ----
+    const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
+    const int K = ndf * 2 * nsl2;
+    double2* Lop = (double2*)c->buf("hnsL", sizeof(double2) * (size_t)K * k->npad);
+    double2* Rop = (double2*)c->buf("hnsR", sizeof(double2) * (size_t)K * k->npad);
+    size_t nloc = (size_t)ndf * nsl2 * std::max(1, k->nlo);
+    double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
+    double2* C2lo = (double2*)c->buf("hnsC2lo", sizeof(double2) * nloc);
+    if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
+    nl++;
+    k_hns_ops<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P, k->d_tns, k->d_loranges,
+                                                               (int)k->loranges.size(), Lop, Rop, Clo, C2lo);
+    CK(cudaGetLastError());
+    int rc = LAPW1GPU_OK;
+    if (c->prec == LAPW1GPU_PREC_SPLIT)
+      rc = split_hns_gemm(c, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices, s, &nl);
+    else {
+      int ntiles = 0;
+      const int2* tl = tiles_tri(c, "tiles_hns", n, HNS_T, &ntiles);
+      if (!tl) return LAPW1GPU_ERR_NOMEM;
+      nl++;
+      k_hns_gemm<<<ntiles, 256, 0, s>>>(n, k->npad, K, tl, Lop, Rop, d_hs, ldhs);
+    }
+    if (rc) return rc;
+    if (k->nlo > 0)
+      nl++;
+      k_hns_lo<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);
+    CK(cudaGetLastError());
+  }
+  if (st) CK(cudaEventRecord(c->ev[4], s));
+
+  if ((stages & 4) && !k->orbs.empty()) {
+    double2* alm = (double2*)c->buf("orb_alm", sizeof(double2) * 7 * (size_t)n);
+    double2* blm = (double2*)c->buf("orb_blm", sizeof(double2) * 7 * (size_t)n);
+    double2* clm = (double2*)c->buf("orb_clm", sizeof(double2) * 7 * (size_t)n);
+    if (!alm || !blm || !clm) return LAPW1GPU_ERR_NOMEM;
+    for (auto& it : k->orbs) {
+      const double2* pot = k->d_pots + (size_t)it.iat * 49;
+      nl++;
+      k_horb_rows<<<(n + 127) / 128, 128, 0, s>>>(P, it.a, it.lvor, pot, k->d_loranges, (int)k->loranges.size(), alm,
+                                                  blm, clm);
+      nl++;
+      k_horb_pairs<<<dim3((n + 127) / 128, n), 128, 0, s>>>(P, it.a, it.lvor, pot, k->d_loranges,
+                                                           (int)k->loranges.size(), alm, blm, clm, d_hs, ldhs);
+    }
+    CK(cudaGetLastError());
+  }
+  if (st) CK(cudaEventRecord(c->ev[5], s));
+  nl++;
+  k_check_finite<<<296, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
+  CK(cudaGetLastError());
+  if (st) {
+    CK(cudaEventRecord(c->ev[6], s));
+    int hstat = 0;
+    CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c->last_status = hstat;
+    float t[6];
+    for (int q = 0; q < 6; q++) cudaEventElapsedTime(&t[q], c->ev[q], c->ev[q + 1]);
+    memset(st, 0, sizeof(*st));
+    st->ms_albl = t[0];
+    st->ms_spherical = t[1];
+    st->ms_lo = t[2];
+    st->ms_hns = t[3];
+    st->ms_horb = t[4];
+    float tot;
+    cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]);
+    st->ms_total = tot;
+    st->flops_fp64_equiv = alg_flops(k);
+    st->kernel_launches = nl;
+    if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+    if (hstat) return LAPW1GPU_ERR_RANGE;
+  }
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs, int ldhs,
+                          double* hsdiag, lapw1gpu_stats* st) {
+  if (!c || !p || !hs || !hsdiag || ldhs < p->n) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  cudaEvent_t e0 = c->ev[7], e1 = c->ev[8], e2 = c->ev[9], e3 = c->ev[10];
+  cudaEventRecord(e0, c->stream);
+  lapw1gpu_kpoint* k = nullptr;
+  int rc = kpoint_upload_impl(c, p, &k, true);
+  if (rc) return rc;
+  const int n = p->n;
+  double2* d_hs = (double2*)c->buf("hs", sizeof(double2) * (size_t)n * n);
+  double2* d_hd = (double2*)c->buf("hsdiag", sizeof(double2) * (size_t)n);
+  if (!d_hs || !d_hd) {
+    lapw1gpu_kpoint_free(k);
+    return LAPW1GPU_ERR_NOMEM;
+  }
+  // stages that only add (HNS/HORB alone) start from the caller's HS
+  if (!(stages & 1)) {
+    cudaMemcpy2DAsync(d_hs, sizeof(double2) * n, hs, sizeof(double2) * ldhs, sizeof(double2) * n, n,
+                      cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d_hd, hsdiag, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream);
+  }
+  cudaEventRecord(e1, c->stream);
+  lapw1gpu_stats st2;
+  rc = lapw1gpu_kpoint_run(c, k, stages, (double*)d_hs, n, (double*)d_hd, &st2);
+  cudaEventRecord(e2, c->stream);
+  if (rc == LAPW1GPU_OK) {
+    if (cudaMemcpy2DAsync(hs, sizeof(double2) * ldhs, d_hs, sizeof(double2) * n, sizeof(double2) * n, n,
+                          cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaMemcpyAsync(hsdiag, d_hd, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      rc = LAPW1GPU_ERR_CUDA;
+  }
+  cudaEventRecord(e3, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+  if (st) {
+    *st = st2;
+    float a, b;
+    cudaEventElapsedTime(&a, e0, e1);
+    cudaEventElapsedTime(&b, e2, e3);
+    st->ms_h2d = a;
+    st->ms_d2h = b;
+  }
+  lapw1gpu_kpoint_free(k);
+  return rc;
+}
+
+// hns.F:317-380 sums over LMSORT's grouping of the gaunt list
+// (lmsort.f:246-421): entries sorted by (l0,m0,l',m',LM) with a stable
+// insertion sort; a repeated tuple keeps the first gaunt factor only.
+int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx, const int* lqind, const int* lqns,
+                            const double* gfac, const double* vns1, const double* vns2, const double* vns3,
+                            const double* vnslo1, const double* vnslo2, const double* vnslo3, const int* loor,
+                            double* tns) {
+  if (nat < 1 || lnsmax < 0 || lnsmax > 4 || ngau < 0 || lmmx < 1 || !lqind || !lqns || !gfac || !vns1 || !vns2 ||
+      !vns3 || !vnslo1 || !vnslo2 || !vnslo3 || !loor || !tns)
+    return LAPW1GPU_ERR_ARG;
+  const int K = L1G_NSL2, NS = LAPW1GPU_NSLMAX, NL = L1G_LOMAX + 1;
+  memset(tns, 0, sizeof(double) * 2 * (size_t)nat * LAPW1GPU_NTNS * K * K);
+  struct Ent {
+    int l0, m0, lp, mp, lmx;
+    double gr, gi;
+  };
+  std::vector<Ent> e;
+  for (int ja = 0; ja < nat; ja++) {
+    const int nq = lqind[ja];
+    if (nq < 0 || nq > ngau) return LAPW1GPU_ERR_RANGE;
+    e.clear();
+    for (int i = 0; i < nq; i++) {
+      const int* q = lqns + ((size_t)ja * ngau + i) * 6;
+      Ent x{q[2] - 1, q[5], q[0] - 1, q[4], q[3], gfac[((size_t)ja * ngau + i) * 2],
+            gfac[((size_t)ja * ngau + i) * 2 + 1]};
+      auto before = [](const Ent& a, const Ent& b) {
+        if (a.l0 != b.l0) return a.l0 < b.l0;
+        if (a.m0 != b.m0) return a.m0 < b.m0;
+        if (a.lp != b.lp) return a.lp < b.lp;
+        if (a.mp != b.mp) return a.mp < b.mp;
+        return a.lmx < b.lmx;
+      };
+      auto it = std::upper_bound(e.begin(), e.end(), x, before);  // stable: after equal keys
+      e.insert(it, x);
+    }
+    double* T = tns + (size_t)ja * LAPW1GPU_NTNS * K * K * 2;
+    for (size_t i = 0; i < e.size(); i++) {
+      const Ent& x = e[i];
+      if (i > 0) {
+        const Ent& y = e[i - 1];
+        if (x.l0 == y.l0 && x.m0 == y.m0 && x.lp == y.lp && x.mp == y.mp && x.lmx == y.lmx) continue;
+      }
+      const int lmx = x.lmx - 1;
+      if (x.l0 < 0 || x.lp < 0 || x.l0 > lnsmax || x.lp > lnsmax || lmx < 0 || lmx >= lmmx) continue;
+      if (abs(x.m0) > x.l0 || abs(x.mp) > x.lp) return LAPW1GPU_ERR_ARG;
+      const int a = x.l0 * (x.l0 + 1) + x.m0, b = x.lp * (x.lp + 1) + x.mp;
+      auto v3 = [&](const double* arr, int i1, int i3) { return arr[(((size_t)ja * NS + i3) * lmmx + lmx) * NS + i1]; };
+      auto vlo = [&](const double* arr, int i1, int i3) { return arr[(((size_t)ja * NS + i3) * lmmx + lmx) * NL + i1]; };
+      auto addt = [&](int blk, double val) {
+        T[(((size_t)blk * K + a) * K + b) * 2] += x.gr * val;
+        T[(((size_t)blk * K + a) * K + b) * 2 + 1] += x.gi * val;
+      };
+      addt(0, v3(vns1, x.lp, x.l0));  // TUU  VNS1(LP,LMX,L0)
+      addt(1, v3(vns3, x.l0, x.lp));  // TDU  VNS3(L0,LMX,LP)
+      addt(3, v3(vns3, x.lp, x.l0));  // TUD  VNS3(LP,LMX,L0)
+      addt(4, v3(vns2, x.lp, x.l0));  // TDD  VNS2(LP,LMX,L0)
+      bool loorl0 = false;
+      if (x.l0 <= L1G_LOMAX) {
+        loorl0 = loor[ja * NL + x.l0] != 0;
+        if (loorl0) {
+          addt(6, vlo(vnslo1, x.l0, x.lp));  // TUU12 VNS1LO(L0+1,LMX,LP+1)
+          addt(7, vlo(vnslo2, x.l0, x.lp));  // TDU12 VNS2LO(L0+1,LMX,LP+1)
+        }
+      }
+      if (x.lp <= L1G_LOMAX && loor[ja * NL + x.lp]) {
+        if (loorl0) addt(8, vlo(vnslo3, x.lp, x.l0));  // TUU22 VNS3LO(LP+1,LMX,L0+1)
+        addt(2, vlo(vnslo1, x.lp, x.l0));              // TUU21 VNS1LO(LP+1,LMX,L0+1)
+        addt(5, vlo(vnslo2, x.lp, x.l0));              // TUD21 VNS2LO(LP+1,LMX,L0+1)
+      }
+    }
+  }
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_setup(lapw1gpu_context* c, const lapw1gpu_problem* p, double* hs, int ldhs, double* hsdiag,
+                   lapw1gpu_stats* st) {
+  return lapw1gpu_setup_stages(c, p, 7, hs, ldhs, hsdiag, st);
+}
+
+}  // extern "C"

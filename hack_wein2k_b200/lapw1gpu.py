@@ -1,0 +1,190 @@
+"""ctypes binding of liblapw1gpu.so (the C ABI of include/lapw1gpu.h).
+
+This is the Python side of the drop-in boundary: the same entry points a
+Fortran caller binds with ISO_C_BINDING.  The library must be present:
+there is no CPU fallback, and every call fails loudly if the CUDA
+extension is missing or the device is unusable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .problem import CProblem, CStats, Problem
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblapw1gpu.so")
+
+PREC_FP64 = 0
+PREC_SPLIT = 1
+
+STATUS = {
+    0: "ok", 1: "bad argument", 2: "device out of memory", 3: "CUDA error",
+    4: "non-finite matrix element", 5: "device wait timed out", 6: "no sm_100 device",
+    7: "size beyond a documented limit",
+}
+
+# every symbol include/lapw1gpu.h declares
+EXPORTS = [
+    "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
+    "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
+    "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
+]
+
+_lib = None
+
+
+class Lapw1GpuError(RuntimeError):
+    def __init__(self, where: str, code: int):
+        super().__init__(f"{where}: {STATUS.get(code, 'error')} (status {code})")
+        self.code = code
+
+
+def load(path: Optional[str] = None):
+    """Load the library (built by hack_wein2k_b200.build); raise if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m hack_wein2k_b200.build`")
+    lib = C.CDLL(path)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    lib.lapw1gpu_init.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.lapw1gpu_finalize.argtypes = [vp]
+    lib.lapw1gpu_set_precision.argtypes = [vp, C.c_int, C.c_int]
+    lib.lapw1gpu_kpoint_upload.argtypes = [vp, C.POINTER(CProblem), C.POINTER(vp)]
+    lib.lapw1gpu_kpoint_free.argtypes = [vp]
+    lib.lapw1gpu_kpoint_run.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(CStats)]
+    lib.lapw1gpu_setup.argtypes = [vp, C.POINTER(CProblem), dp, C.c_int, dp, C.POINTER(CStats)]
+    lib.lapw1gpu_setup_stages.argtypes = [vp, C.POINTER(CProblem), C.c_int, dp, C.c_int, dp,
+                                          C.POINTER(CStats)]
+    lib.lapw1gpu_stream.argtypes = [vp]
+    lib.lapw1gpu_stream.restype = vp
+    lib.lapw1gpu_last_status.argtypes = [vp]
+    lib.lapw1gpu_version.restype = C.c_char_p
+    lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
+                                            dp, dp, dp, ip, dp]
+    _lib = lib
+    return lib
+
+
+def _check(where: str, rc: int):
+    if rc != 0:
+        raise Lapw1GpuError(where, rc)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class KPoint:
+    """One k-point's inputs resident on the device (lapw1gpu_kpoint)."""
+
+    def __init__(self, ctx: "Context", prob: Problem):
+        self.ctx, self.prob = ctx, prob
+        self._cp = prob.to_c()
+        h = C.c_void_p()
+        _check("lapw1gpu_kpoint_upload", ctx.lib.lapw1gpu_kpoint_upload(ctx.h, C.byref(self._cp), C.byref(h)))
+        self.h = h
+
+    def run(self, d_hs_ptr: int, ldhs: int, d_hsdiag_ptr: int, stages: int = 7, stats: bool = False):
+        st = CStats() if stats else None
+        rc = self.ctx.lib.lapw1gpu_kpoint_run(self.ctx.h, self.h, stages, C.c_void_p(d_hs_ptr), ldhs,
+                                              C.c_void_p(d_hsdiag_ptr), C.byref(st) if st is not None else None)
+        _check("lapw1gpu_kpoint_run", rc)
+        return st.as_dict() if st is not None else None
+
+    def free(self):
+        if self.h:
+            self.ctx.lib.lapw1gpu_kpoint_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Context:
+    """A lapw1gpu context on one CUDA device."""
+
+    def __init__(self, device: int = 0, prec: int = PREC_FP64, slices: int = 6):
+        self.lib = load()
+        h = C.c_void_p()
+        _check("lapw1gpu_init", self.lib.lapw1gpu_init(device, C.byref(h)))
+        self.h = h
+        self.device = device
+        self.set_precision(prec, slices)
+
+    def set_precision(self, prec: int, slices: int = 6):
+        _check("lapw1gpu_set_precision", self.lib.lapw1gpu_set_precision(self.h, prec, slices))
+        self.prec, self.slices = prec, slices
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self.lib.lapw1gpu_stream(self.h) or 0)
+
+    def last_status(self) -> int:
+        return int(self.lib.lapw1gpu_last_status(self.h))
+
+    def setup(self, prob: Problem, stages: int = 7, hs: Optional[np.ndarray] = None,
+              hsdiag: Optional[np.ndarray] = None, stats: bool = False):
+        """calkpt.F:153-185 on host buffers.  Returns (HS, HSDIAG[, stats]);
+        HS is n x n complex128 in Fortran order (the reference's HS)."""
+        n = prob.n
+        if hs is None:
+            hs = np.zeros((n, n), dtype=np.complex128, order="F")
+        if hsdiag is None:
+            hsdiag = np.zeros(n, dtype=np.complex128)
+        assert hs.flags.f_contiguous and hs.dtype == np.complex128 and hs.shape[0] >= n
+        cp = prob.to_c()
+        st = CStats()
+        rc = self.lib.lapw1gpu_setup_stages(self.h, C.byref(cp), stages,
+                                            _dp(hs.reshape(-1, order="F").view(np.float64)), hs.shape[0],
+                                            _dp(hsdiag.view(np.float64)), C.byref(st))
+        _check("lapw1gpu_setup", rc)
+        if stats:
+            return hs, hsdiag, st.as_dict()
+        return hs, hsdiag
+
+    def upload(self, prob: Problem) -> KPoint:
+        return KPoint(self, prob)
+
+    def close(self):
+        if self.h:
+            self.lib.lapw1gpu_finalize(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def version() -> str:
+    return load().lapw1gpu_version().decode()
+
+
+def tns_from_gaunt(nat, lnsmax, lqind, lqns, gfac, vns1, vns2, vns3, vnslo1, vnslo2, vnslo3, loor):
+    """Product-side gaunt-list -> T-block builder (lapw1gpu_tns_from_gaunt)."""
+    lib = load()
+    lqns = np.ascontiguousarray(lqns, dtype=np.int32)
+    ngau = lqns.shape[1]
+    lmmx = np.asarray(vns1).shape[2]
+    out = np.zeros((nat, 9, 25, 25), dtype=np.complex128)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (vns1, vns2, vns3, vnslo1, vnslo2, vnslo3)]
+    g = np.ascontiguousarray(gfac, dtype=np.complex128)
+    li = np.ascontiguousarray(lqind, dtype=np.int32)
+    lo = np.ascontiguousarray(loor, dtype=np.int32)
+    rc = lib.lapw1gpu_tns_from_gaunt(nat, lnsmax, ngau, lmmx, li.ctypes.data_as(C.POINTER(C.c_int)),
+                                     lqns.ctypes.data_as(C.POINTER(C.c_int)), _dp(g.view(np.float64)),
+                                     *[_dp(a) for a in arrs], lo.ctypes.data_as(C.POINTER(C.c_int)),
+                                     _dp(out.view(np.float64)))
+    _check("lapw1gpu_tns_from_gaunt", rc)
+    return out

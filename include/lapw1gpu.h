@@ -1,0 +1,225 @@
+/*
+ * lapw1gpu.h -- C ABI of the B200 lapw1 Hamiltonian/overlap setup.
+ *
+ * The library replaces the matrix-setup segment of WIEN2k lapw1's CALKPT
+ * (SRC_lapw1/calkpt.F:153-185):
+ *
+ *     CALL HAMILT(NT,NAT,NV,P,PE,DP,DPE,MULT,RMT,POS,V,VI,PEI,E,INS)
+ *     CALL ZSWAP(HSROWS,HS,HSROWS+1,HSDIAG,1)
+ *     if(.not.nohns) CALL HNS(NV,NAT,LNSMAX+1,POS,VI,RMT,MULT,LQIND,LQNS,
+ *                             GFAC,ROTLOC,ROTIJ,VNS1,VNS2,VNS3)
+ *     if(Nmod.ne.0)  CALL HORB(NV,NAT,LNSMAX+1,POS,VI,RMT,MULT,LQIND,LQNS,
+ *                             PEI,ROTLOC,ROTIJ,HS)
+ *
+ * and leaves HS / HSDIAG in exactly the state that sequence leaves them
+ * (complex build, sequential path):
+ *   - HS(i,j), i>j   : conj-stored spherical H (hamilt.F:463) plus the HNS
+ *                      'T'-transposed updates (hns.F:449-467) and HORB terms
+ *   - HS(i,i)        : diagonal of H (after the ZSWAP, calkpt.F:164) plus
+ *                      HNS/HORB diagonal terms
+ *   - HS(i,j), i<j   : overlap S (hamilt.F:464)
+ *   - HSDIAG(i)      : diagonal of S
+ *
+ * Every array is a plain host pointer.  Complex numbers are interleaved
+ * (re, im) doubles, the layout of Fortran COMPLEX*16.  Array layouts are the
+ * Fortran ones of the reference's modules, written here as C index order
+ * (last C index fastest == first Fortran index).  Every entry point returns
+ * a status code (LAPW1GPU_OK == 0) and never exits the process; the Fortran
+ * shim maps a non-zero status to OUTERR + STOP (the reference's error path,
+ * SRC_lapw1/outerr.f).
+ */
+#ifndef LAPW1GPU_H
+#define LAPW1GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAPW1GPU_LOMAX 3   /* param.inc LOMAX: highest l carrying local orbitals */
+#define LAPW1GPU_NLOAT 3   /* param.inc nloat: local orbitals per (l, atom) */
+#define LAPW1GPU_NSLMAX 5  /* param.inc NSLMAX: lmax_ns + 1 upper bound */
+#define LAPW1GPU_NSL2 25   /* NSLMAX*NSLMAX: (l,m) pairs of the non-spherical block */
+#define LAPW1GPU_NTNS 9    /* T blocks per atom type: see lapw1gpu_problem.tns */
+
+/* status codes */
+enum {
+  LAPW1GPU_OK = 0,
+  LAPW1GPU_ERR_ARG = 1,        /* inconsistent sizes or a NULL required array */
+  LAPW1GPU_ERR_NOMEM = 2,      /* device allocation failed */
+  LAPW1GPU_ERR_CUDA = 3,       /* a CUDA runtime call failed */
+  LAPW1GPU_ERR_NONFINITE = 4,  /* a kernel met a non-finite intermediate */
+  LAPW1GPU_ERR_TIMEOUT = 5,    /* a bounded device wait ran out */
+  LAPW1GPU_ERR_NODEVICE = 6,   /* no usable sm_100 device */
+  LAPW1GPU_ERR_RANGE = 7       /* a size exceeds a documented limit */
+};
+
+/* arithmetic of the muffin-tin contractions */
+enum {
+  LAPW1GPU_PREC_FP64 = 0,      /* every product in FP64 (the comparator path) */
+  LAPW1GPU_PREC_SPLIT = 1      /* Ozaki int8 slices on tcgen05, exact int32 accumulation */
+};
+
+/*
+ * One k-point's setup problem.  Field names follow the reference's module
+ * variables; the comment gives the reference array each field carries.
+ */
+typedef struct lapw1gpu_problem {
+  /* ---- sizes ---- */
+  int n;        /* HSROWS = NV + NLO                     (modules.F:441-535) */
+  int nv;       /* NV: plane waves                        (coors.f:165)        */
+  int nlo;      /* NLO: local-orbital rows                (atpar.f:187-199)    */
+  int nat;      /* NAT: inequivalent atoms                                     */
+  int ndf;      /* NDF: all atoms, sum of MULT                                 */
+  int ltop;     /* NT = lmax+1, 3 <= ltop <= ldl          (inilpw.f:346-350)   */
+  int ldl;      /* leading dimension of the per-l arrays (LMAX=13 in lapw1)    */
+  int lnsmax;   /* LNSMAX, 0..4: HNS uses (lnsmax+1)^2 (l,m) pairs             */
+  int ins;      /* INS: 0 = warped interstitial (WARPIN), else USTPHX only     */
+  int nohns;    /* 1 skips HNS (lapw1 -nohns, calkpt.F:169)                    */
+  double vi;    /* VI = 1/unit-cell volume                                     */
+  double bkzz[9]; /* row-major 3x3 B with Cartesian (k+G) = k + B.KZZ: the
+                     matrix COORS builds XK/YK/ZK with (coors.f:47-55,81-83):
+                     diag(PIA) for ORTHO lattices, BR2 otherwise            */
+
+  /* ---- structure ---- */
+  const int* mult;      /* MULT(NAT)                     [nat]            */
+  const double* rmt;    /* RMT(NAT)                      [nat]            */
+  const double* v;      /* V(NAT) = 4 pi VI RMT^3 / 3    [nat]            */
+  const double* pos;    /* POS(3,NDF), fractional        [ndf][3]         */
+  const double* rotij;  /* ROTIJ(3,3,NDF)                [ndf][3][3]      */
+  const double* rotloc; /* ROTLOC(3,3,NAT)               [nat][3][3]      */
+
+  /* ---- basis (COORS + LOPW output, fixes the row order) ---- */
+  const int* kzz;       /* KZZ(3,HSROWS)                 [n][3]           */
+  const double* xk;     /* XK(HSROWS): Cartesian k+G     [n]              */
+  const double* yk;     /* YK(HSROWS)                    [n]              */
+  const double* zk;     /* ZK(HSROWS)                    [n]              */
+  const double* rk;     /* RK(HSROWS) = |k+G|            [n]              */
+
+  /* ---- radial parameters (ATPAR output), [nat][ldl] = X(0:LMAX-1,NAT) ---- */
+  const double* p;      /* U(R)      (HAMILT arg U   = P)    */
+  const double* pe;     /* Udot(R)   (HAMILT arg UP  = PE)   */
+  const double* dp;     /* U'(R)     (HAMILT arg DU  = DP)   */
+  const double* dpe;    /* Udot'(R)  (HAMILT arg DUP = DPE)  */
+  const double* pei;    /* |Udot|^2  (HAMILT arg CHN = PEI)  */
+  const double* e;      /* E_l       (HAMILT arg E)          */
+  const int* lapw;      /* LAPW(0:LMAX-1,NAT): 1 LAPW, 0 APW  [nat][ldl] */
+
+  /* ---- local orbitals (modules loabc / lolog) ---- */
+  const int* ilo;       /* ILO(0:LOMAX,NAT)                 [nat][4]        */
+  const int* loor;      /* LOOR(0:LOMAX,NAT): 1 = LAPW-type LO [nat][4]     */
+  const double* alo;    /* ALO(0:LOMAX,NLOAT,NAT)            [nat][3][4]    */
+  const double* blo;    /* BLO(0:LOMAX,NLOAT,NAT)            [nat][3][4]    */
+  const double* clo;    /* CLO(0:LOMAX,NLOAT,NAT)            [nat][3][4]    */
+  const double* elo;    /* ELO(0:LOMAX,NLOAT,NAT)            [nat][3][4]    */
+  const double* pi12lo; /* PI12LO(0:LOMAX,NAT)               [nat][4]       */
+  const double* pe12lo; /* PE12LO(0:LOMAX,NAT)               [nat][4]       */
+  const double* dplo;   /* DPLO(0:LOMAX,NAT)                 [nat][4]       */
+
+  /* ---- interstitial warped potential (module out, SETWAR output) ---- */
+  int warp1, warp2, warp3;  /* WARP1..3: half extents                       */
+  const double* warp;       /* WARP(-W1:W1,-W2:W2,-W3:W3), complex
+                               [2w3+1][2w2+1][2w1+1][2]                      */
+
+  /* ---- non-spherical muffin-tin matrix elements (HNS) ----
+   * tns[a][b][l0m0][lpmp] complex, a = atom type, lm = l*(l+1)+m.  These are
+   * the sums that hns.F:317-380 forms from GNT x VNS before its loop 30:
+   *   b=0 TUU   b=1 TDU   b=2 TUU21   (row block A2, hns.F:387-401)
+   *   b=3 TUD   b=4 TDD   b=5 TUD21   (row block B2, hns.F:403-417)
+   *   b=6 TUU12 b=7 TDU12 b=8 TUU22   (row block C2, hns.F:419-433)
+   * lapw1gpu_tns_from_gaunt() builds them from the reference's GFAC/LQNS/VNS. */
+  const double* tns;    /* [nat][9][25][25][2] */
+
+  /* ---- orbital potential (HORB, module orb) ---- */
+  int natorb;           /* NATORB; 0 skips HORB (calkpt.F:176)         */
+  const int* iatom;     /* IATOM(NATORB): atom type of each U-atom     */
+  const int* nlorb;     /* NLORB(NATORB)                               */
+  const int* lorb;      /* LORB(3,NATORB)            [natorb][3]       */
+  const double* vorb;   /* VORB(iat,l,m1,m2) complex [natorb][4][7][7][2],
+                           index [iat][l][m1+3][m2+3]                  */
+} lapw1gpu_problem;
+
+/* timings of one setup, milliseconds of device time (CUDA events) */
+typedef struct lapw1gpu_stats {
+  double ms_total;      /* whole setup on the device                  */
+  double ms_albl;       /* K-a: matching coefficients + operand build  */
+  double ms_spherical;  /* K-b + K-c: PW x PW spherical + interstitial */
+  double ms_lo;         /* K-b': local-orbital columns                 */
+  double ms_hns;        /* K-ns: non-spherical contraction             */
+  double ms_horb;       /* K-orb                                       */
+  double ms_h2d;        /* host->device copies (host entry points)     */
+  double ms_d2h;        /* device->host copy of HS/HSDIAG              */
+  double flops_fp64_equiv; /* algorithmic FP64 flops of K-b + K-ns     */
+  double kernel_launches;  /* kernels this library launched in the run */
+} lapw1gpu_stats;
+
+typedef struct lapw1gpu_context lapw1gpu_context;
+
+/* Context on one CUDA device: stream, events, cached device buffers.
+ * Replaces nothing in the reference (lapw1 has no device); one context per
+ * host thread and device. */
+int lapw1gpu_init(int device, lapw1gpu_context** ctx);
+int lapw1gpu_finalize(lapw1gpu_context* ctx);
+/* select the muffin-tin contraction arithmetic (LAPW1GPU_PREC_*) */
+int lapw1gpu_set_precision(lapw1gpu_context* ctx, int prec, int slices);
+
+/* One k-point's inputs resident in device memory (uploaded once; the
+ * benchmark's resident-input path and the k-point batch driver use it). */
+typedef struct lapw1gpu_kpoint lapw1gpu_kpoint;
+int lapw1gpu_kpoint_upload(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
+                           lapw1gpu_kpoint** kp);
+int lapw1gpu_kpoint_free(lapw1gpu_kpoint* kp);
+/* Run the selected stages on a resident k-point into device memory:
+ * d_hs is n x n complex column-major with leading dimension ldhs, d_hsdiag
+ * n complex.  Stage bits: 1 HAMILT (+ZSWAP), 2 HNS, 4 HORB; 7 = all of
+ * calkpt.F:153-185.  Asynchronous on the context's stream unless st != NULL
+ * (then it synchronises and fills the timings). */
+int lapw1gpu_kpoint_run(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp, int stages,
+                        double* d_hs, int ldhs, double* d_hsdiag,
+                        lapw1gpu_stats* st);
+
+/* Full drop-in for calkpt.F:153-185 (HAMILT, ZSWAP, HNS, HORB) with host
+ * buffers: hs is HS(HSROWS,HSROWS) complex, column-major with leading
+ * dimension ldhs >= n; hsdiag is HSDIAG(HSROWS).  The library writes every
+ * element of the n x n block (INIT_MATRICES zeroing is not needed).
+ * Synchronous: returns when hs/hsdiag hold the result. */
+int lapw1gpu_setup(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
+                   double* hs, int ldhs, double* hsdiag, lapw1gpu_stats* st);
+
+/* lapw1gpu_setup restricted to the given stages (parity tests of each
+ * reference routine). */
+int lapw1gpu_setup_stages(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
+                          int stages, double* hs, int ldhs, double* hsdiag,
+                          lapw1gpu_stats* st);
+
+/* the context's CUDA stream (cudaStream_t), for callers that order their
+ * own work after an asynchronous lapw1gpu_kpoint_run */
+void* lapw1gpu_stream(lapw1gpu_context* ctx);
+
+/* device status word of the last run (L1G_STATUS_* bits), 0 if clean */
+int lapw1gpu_last_status(lapw1gpu_context* ctx);
+
+/* Build the nine HNS T blocks from the reference's gaunt lists: the sums of
+ * hns.F:317-380 over LMSORT's grouping (lmsort.f:246-421: entries sorted by
+ * (l0,m0,l',m',LM), a repeated tuple keeping its first gaunt factor).
+ *   lqind[nat]                       LQIND(NAT)
+ *   lqns  [nat][ngau][6]             LQNS(6,NGAU,NAT)
+ *   gfac  complex [nat][ngau]        GFAC(NGAU,NAT)
+ *   vns1/2/3 [nat][5][lmmx][5]       VNS1(0:NSLMAX-1,LMMX,0:NSLMAX-1,NAT)
+ *   vnslo1/2/3 [nat][5][lmmx][4]     VNS1LO(LOMAX+1,LMMX,NSLMAX,NAT)
+ *   loor  [nat][4]                   LOOR(0:LOMAX,NAT)
+ * Output tns as in lapw1gpu_problem.tns.  Host-only, no device needed. */
+int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx,
+                            const int* lqind, const int* lqns,
+                            const double* gfac, const double* vns1,
+                            const double* vns2, const double* vns3,
+                            const double* vnslo1, const double* vnslo2,
+                            const double* vnslo3, const int* loor,
+                            double* tns);
+
+/* version string of the library */
+const char* lapw1gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LAPW1GPU_H */
