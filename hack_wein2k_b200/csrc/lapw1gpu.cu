@@ -574,9 +574,10 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
       k_hns_gemm<<<ntiles, 256, 0, s>>>(n, k->npad, K, tl, Lop, Rop, d_hs, ldhs);
     }
     if (rc) return rc;
-    if (k->nlo > 0)
+    if (k->nlo > 0) {
       nl++;
       k_hns_lo<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);
+    }
     CK(cudaGetLastError());
   }
   if (st) CK(cudaEventRecord(c->ev[4], s));

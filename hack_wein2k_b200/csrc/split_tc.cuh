@@ -1,9 +1,432 @@
-// split_tc.cuh -- split-precision (Ozaki int8 slices, tcgen05) contractions.
+// split_tc.cuh -- split-precision HNS contraction on the 5th-generation
+// tensor cores (tcgen05, kind::i8), sm_100a.
+//
+// The HNS update of the lower triangle (hns.F:449-467, zher2m.f:69-80),
+//   HS(i,j) += sum_k L(i,k) R(j,k),  i >= j,   K = 2*NDF*(lnsmax+1)^2 complex,
+// is computed as an Ozaki-style sum of exact integer products:
+//   * every row of L (and of R) gets a power-of-two scale 2^e, e = ilogb(max)+1,
+//     so the scaled row lies in (-1, 1);
+//   * the scaled row is cut into S int8 slices, l = sum_p a_p 2^(-6-7(p-1)),
+//     |a_p| <= 64 (first slice 6 bits + sign, then 7 bits each); the cut is
+//     exact in FP64 (power-of-two scalings and Sterbenz subtractions);
+//   * slice products a_p b_q with p+q-2 = d < S are accumulated EXACTLY in one
+//     int32 TMEM accumulator per level d (|sum| <= 64*64*2K < 2^31);
+//   * the epilogue combines the levels in FP64, sum_d c_d 2^(-7d), scales by
+//     2^(e_i + f_j - 12) and adds into HS.
+// The dropped products (p+q-2 >= S) bound the error by ~(S+1) 2^(-7S) of
+// max|L_i| max|R_j| K per element: S=7 is FP64-class (2^-49).
+//
+// Complex arithmetic as one real GEMM with K' = 2K (a Kcp-padded real half
+// and imaginary half per row): A row i = [Re L_i | Im L_i],
+// B rows 2j = [Re R_j | -Im R_j] (-> Re C), 2j+1 = [Im R_j | Re R_j] (-> Im C),
+// so the accumulator columns alternate Re/Im of consecutive j.
+//
+// Kernel shape: one CTA per (128-row, N/2-column) tile of the triangle,
+// M=128, N = 512/S rounded down to 16 (all S levels fit the 512 TMEM
+// columns), 64-byte K blocks with 64B-swizzled TMA tiles of all S slices
+// in one 3-D box, 2-3 pipeline stages.  Thread 0 issues TMA and MMA; all
+// four warps run the epilogue.  Every mbarrier wait is bounded (about one
+// second of clock64); a timeout sets a status bit, skips the writes,
+// drains the copies in flight (bounded) and frees TMEM before returning.
 #pragma once
-#define L1G_MAX_SLICES 8
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
-static int split_hns_gemm(lapw1gpu_context* c, int n, int npad, int K, const double2* Lop, const double2* Rop,
+#define L1G_MAX_SLICES 8
+#define L1G_STATUS_TIMEOUT 8
+
+namespace split {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait (~1 s of SM clock); false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// K-major operand tile, 64-byte swizzle: rows of 64 B, 8-row groups 512 B apart
+__device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;     // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;              // descriptor version (sm100)
+  d |= (uint64_t)4 << 61;              // SWIZZLE_64B
+  return d;
+}
+// instruction descriptor: D s32, A s8, B s8, both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+template <int S>
+struct Cfg {
+  static constexpr int N = ((512 / S) / 16) * 16 > 128 ? 128 : ((512 / S) / 16) * 16;  // real columns
+  static constexpr int JT = N / 2;                                                     // complex columns
+  static constexpr int A_BYTES = S * 128 * 64;
+  static constexpr int B_BYTES = S * N * 64;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int STAGES = (3 * STAGE + 1024 <= 220 * 1024) ? 3 : 2;
+  static constexpr int SMEM = STAGES * STAGE + 1024;
+};
+
+// FP64 -> int8 slices.  X: [Kc][npad] complex (k-major planes, the HNS
+// operand layout).  Out: [S][rows][Kp] int8 with Kp = 2*Kcp; for the left
+// operand (isB = 0) rows = npad, row i = [Re | Im]; for the right operand
+// rows = 2*npad, row 2j = [Re | -Im], row 2j+1 = [Im | Re].  ex[row of X] =
+// the power-of-two exponent.  One block of 256 threads per 32 rows.
+__global__ void __launch_bounds__(256) k_slice(const double2* __restrict__ X, int Kc, int Kcp, int npad, int np_out,
+                                               int S, int isB, int8_t* __restrict__ out, int* __restrict__ ex) {
+  __shared__ double2 tile[64][33];
+  __shared__ double red[8][32];
+  __shared__ int rexp[32];
+  const int r0 = blockIdx.x * 32;
+  const int tid = threadIdx.x;
+  const int Kp = 2 * Kcp;
+  // rows of one slice plane in the output (the tensor map's row extent)
+  const size_t rows = isB ? 2 * (size_t)np_out : (size_t)np_out;
+  {
+    const int row = tid & 31, part = tid >> 5;
+    double m = 0.0;
+    for (int k = part; k < Kc; k += 8) {
+      double2 v = X[(size_t)k * npad + r0 + row];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+    red[part][row] = m;
+    __syncthreads();
+    if (tid < 32) {
+      double mm = 0.0;
+      for (int q = 0; q < 8; q++) mm = fmax(mm, red[q][tid]);
+      int e = (mm > 0.0) ? ilogb(mm) + 1 : 0;
+      rexp[tid] = e;
+      ex[r0 + tid] = e;
+    }
+    __syncthreads();
+  }
+  const int rr = tid >> 3;       // row within the block
+  const int kq = (tid & 7) * 8;  // 8 consecutive k
+  const int e = rexp[rr];
+  for (int k0 = 0; k0 < Kcp; k0 += 64) {
+    for (int q = tid; q < 64 * 32; q += 256) {
+      int kk = q >> 5, r = q & 31;
+      int k = k0 + kk;
+      tile[kk][r] = (k < Kc) ? X[(size_t)k * npad + r0 + r] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
+#pragma unroll
+    for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      double2 v = tile[kq + t][rr];
+      double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
+#pragma unroll
+      for (int p = 0; p < L1G_MAX_SLICES; p++) {
+        if (p < S) {
+          double ar = rint(tr), ai = rint(ti);
+          tr = (tr - ar) * 128.0;
+          ti = (ti - ai) * 128.0;
+          pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
+          pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
+        }
+      }
+    }
+    const int col = k0 + kq;
+    const size_t row = (size_t)(r0 + rr);
+#pragma unroll
+    for (int p = 0; p < L1G_MAX_SLICES; p++) {
+      if (p >= S) break;
+      int8_t* base = out + (size_t)p * rows * Kp;
+      if (!isB) {
+        *(uint64_t*)(base + row * Kp + col) = pre[p];
+        *(uint64_t*)(base + row * Kp + Kcp + col) = pim[p];
+      } else {
+        // negate 8 packed int8 lanes: -x per byte (values within [-64, 64])
+        uint64_t nim = 0;
+#pragma unroll
+        for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
+        *(uint64_t*)(base + (2 * row) * Kp + col) = pre[p];
+        *(uint64_t*)(base + (2 * row) * Kp + Kcp + col) = nim;
+        *(uint64_t*)(base + (2 * row + 1) * Kp + col) = pim[p];
+        *(uint64_t*)(base + (2 * row + 1) * Kp + Kcp + col) = pre[p];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(128, 1)
+    k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const int2* __restrict__ tiles, int nkb, int n, const int* __restrict__ exA,
+                 const int* __restrict__ exB, double2* __restrict__ hs, int ld, int* __restrict__ status) {
+  using C = Cfg<S>;
+  constexpr int N = C::N, STAGES = C::STAGES;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t full[STAGES], empty[STAGES], accbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 t = tiles[blockIdx.x];
+  const int i0 = t.x * 128, j0 = t.y * C::JT;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&accbar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (tid == 0) {
+    constexpr uint32_t idesc = idesc_i8(128, N);
+    int issued = 0;  // k blocks whose TMA was issued
+    bool ok = true;
+    auto load = [&](int kb) {
+      const int st = kb % STAGES;
+      uint8_t* a = smem + st * C::STAGE;
+      uint8_t* b = a + C::A_BYTES;
+      mbar_expect_tx(&full[st], C::STAGE);
+      tma_load_3d(a, &tmA, &full[st], kb * 64, i0, 0);
+      tma_load_3d(b, &tmB, &full[st], kb * 64, 2 * j0, 0);
+    };
+    for (int kb = 0; kb < STAGES - 1 && kb < nkb; kb++) load(issued++);
+    for (int kb = 0; kb < nkb && ok; kb++) {
+      const int st = kb % STAGES;
+      if (!mbar_wait(&full[st], (kb / STAGES) & 1)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(smem + st * C::STAGE);
+      const uint32_t b0 = a0 + C::A_BYTES;
+#pragma unroll
+      for (int p = 0; p < S; p++)
+#pragma unroll
+        for (int q = 0; q < S - p; q++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
+            const uint64_t bd = desc_sw64(b0 + q * N * 64 + h * 32);
+            const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
+            const uint32_t d = tmem + (uint32_t)((p + q) * N);
+            asm volatile(
+                "{\n\t.reg .pred pa;\n\t"
+                "setp.ne.b32 pa, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
+          }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&empty[st]))
+                   : "memory");
+      const int nk = kb + STAGES - 1;
+      if (nk < nkb) {
+        const int rs = nk % STAGES;
+        if (nk >= STAGES && !mbar_wait(&empty[rs], ((nk - STAGES) / STAGES) & 1)) {
+          ok = false;
+          break;
+        }
+        load(nk);
+        issued = nk + 1;
+      }
+    }
+    if (!ok) {
+      atomicOr(status, L1G_STATUS_TIMEOUT);
+      abort_flag = 1;
+      // drain the copies that can still be in flight (the last STAGES
+      // issued) before the CTA may exit; every wait is bounded
+      for (int kb = issued - STAGES > 0 ? issued - STAGES : 0; kb < issued; kb++) {
+        const int st = kb % STAGES;
+        mbar_wait(&full[st], (kb / STAGES) & 1);
+      }
+    }
+    // arrives once every MMA issued so far has completed, so TMEM is
+    // quiescent when the epilogue (or the abort path) proceeds
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(&accbar))
+                 : "memory");
+  }
+  __syncwarp();
+  // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i0+32w..
+  const bool acc_ok = mbar_wait(&accbar, 0);
+  tc_fence_after();
+  if (!acc_ok && lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
+  __syncthreads();
+  if (acc_ok && !abort_flag) {
+    const int i = i0 + warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const double sa = (i < n) ? ldexp(1.0, exA[i] - 12) : 0.0;
+#pragma unroll 1
+    for (int c = 0; c < N / 16; c++) {
+      double v[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = 0.0;
+      double w = 1.0;
+#pragma unroll
+      for (int d = 0; d < S; d++) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+            "[%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(trow + (uint32_t)(d * N + c * 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 16; q++) v[q] = fma((double)(int)r[q], w, v[q]);
+        w *= 0.0078125;  // 2^-7
+      }
+      if (i < n) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int j = j0 + c * 8 + q;
+          if (j < n && j <= i) {
+            const double sc = sa * ldexp(1.0, exB[j]);
+            double2* dst = hs + (size_t)j * ld + i;
+            double2 o = *dst;
+            o.x = fma(v[2 * q], sc, o.x);
+            o.y = fma(v[2 * q + 1], sc, o.y);
+            *dst = o;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+}  // namespace split
+
+// ---------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 l1g_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t rows, uint64_t S, uint32_t box_rows) {
+  auto enc = l1g_encode_fn();
+  if (!enc) return LAPW1GPU_ERR_CUDA;
+  cuuint64_t dims[3] = {kp, rows, S};
+  cuuint64_t strides[2] = {kp, kp * rows};
+  cuuint32_t box[3] = {64, box_rows, (cuuint32_t)S};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+template <int S>
+static int split_gemm_launch(lapw1gpu_context* c, int n, int npad, int Kc, const double2* Lop, const double2* Rop,
+                             double2* hs, int ld, cudaStream_t s, int* nlaunch) {
+  using Cf = split::Cfg<S>;
+  const int Kcp = (Kc + 63) / 64 * 64;
+  const int Kp = 2 * Kcp;
+  const int np = (npad + 127) / 128 * 128;  // slice rows padded to the 128-row tile
+  int8_t* A = (int8_t*)c->buf("splitA", (size_t)S * np * Kp);
+  int8_t* B = (int8_t*)c->buf("splitB", (size_t)S * 2 * np * Kp);
+  int* exA = (int*)c->buf("splitExA", sizeof(int) * np);
+  int* exB = (int*)c->buf("splitExB", sizeof(int) * np);
+  if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
+  // rows in [npad, np) and the K padding stay zero
+  if (cudaMemsetAsync(A, 0, (size_t)S * np * Kp, s) != cudaSuccess ||
+      cudaMemsetAsync(B, 0, (size_t)S * 2 * np * Kp, s) != cudaSuccess ||
+      cudaMemsetAsync(exA, 0, sizeof(int) * np, s) != cudaSuccess ||
+      cudaMemsetAsync(exB, 0, sizeof(int) * np, s) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  // slice the real rows; the row count of X is npad (a multiple of 64, so of 32)
+  split::k_slice<<<npad / 32, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, S, 0, A, exA);
+  split::k_slice<<<npad / 32, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, S, 1, B, exB);
+  *nlaunch += 2;
+  CUtensorMap ta, tb;
+  if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
+    return LAPW1GPU_ERR_CUDA;
+  std::vector<int2> t;
+  const int nbi = (n + 127) / 128, nbj = (n + Cf::JT - 1) / Cf::JT;
+  for (int bi = 0; bi < nbi; bi++)
+    for (int bj = 0; bj < nbj; bj++)
+      if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
+  int2* dt = (int2*)c->buf("tiles_split", sizeof(int2) * t.size());
+  if (!dt) return LAPW1GPU_ERR_NOMEM;
+  if (cudaMemcpyAsync(dt, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  if (cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM) !=
+      cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  split::k_split_gemm<S><<<(unsigned)t.size(), 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, exA, exB, hs, ld,
+                                                                   c->d_status);
+  *nlaunch += 1;
+  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+static int split_hns_gemm(lapw1gpu_context* c, int n, int npad, int Kc, const double2* Lop, const double2* Rop,
                           double2* hs, int ld, int slices, cudaStream_t s, int* nlaunch) {
-  (void)c; (void)n; (void)npad; (void)K; (void)Lop; (void)Rop; (void)hs; (void)ld; (void)slices; (void)s; (void)nlaunch;
-  return LAPW1GPU_ERR_RANGE;
+  switch (slices) {
+    case 2: return split_gemm_launch<2>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 3: return split_gemm_launch<3>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 4: return split_gemm_launch<4>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 5: return split_gemm_launch<5>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 6: return split_gemm_launch<6>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 7: return split_gemm_launch<7>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 8: return split_gemm_launch<8>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    default: return LAPW1GPU_ERR_RANGE;
+  }
 }

@@ -1,0 +1,79 @@
+"""Split-precision path (Ozaki int8 slices on tcgen05) against the FP64 oracle.
+
+The HNS contraction runs as exact int32 products of S int8 slices per
+operand; the per-matrix relative error of H therefore falls as ~2^(-7S)
+(S is the slice count).  Tolerances per S are written below; S is also
+checked through the generalized eigenvalues (SECLR4's problem), against
+the north-star bound of 1e-6 Ry for the split path.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from hack_wein2k_b200 import lapw1gpu, synth
+from hack_wein2k_b200.problem import hermitian_from_packed
+from oracle import oracle as O
+from tests.conftest import gpu_available
+from tests.helpers import rel_errors
+
+# relative max-norm error bound of H per slice count (S is exact: TOL_S = 1e-12)
+TOL_H = {4: 2e-7, 5: 2e-9, 6: 2e-11, 7: 1e-12, 8: 1e-12}
+
+
+@pytest.fixture(scope="module")
+def sctx():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    c = lapw1gpu.Context(0, prec=lapw1gpu.PREC_SPLIT, slices=7)
+    yield c
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slices", [4, 5, 6, 7, 8])
+@pytest.mark.parametrize("kind", ["lo", "apw", "multilo"])
+def test_split_small(sctx, kind, slices):
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
+    p = synth.small_case(kind)
+    hs, hsd = sctx.setup(p)
+    hs_o, hsd_o = O.setup(p)
+    err = rel_errors(hs, hsd, hs_o, hsd_o)
+    assert err["S"] <= 1e-12, err           # S does not go through HNS
+    assert err["H"] <= TOL_H[slices], err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slices", [5, 7])
+def test_split_c1(sctx, slices):
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
+    p = synth.config("c1")[0]
+    hs, hsd = sctx.setup(p)
+    hs_o, hsd_o = O.setup(p)
+    err = rel_errors(hs, hsd, hs_o, hsd_o)
+    assert err["S"] <= 1e-12 and err["H"] <= TOL_H[slices], err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slices", [4, 5])
+def test_split_eigenvalues(sctx, slices):
+    """Generalized eigenvalues of the split-path H,S within 1e-6 Ry of the
+    FP64 oracle's (fewest slices meeting the bound)."""
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
+    p = synth.small_case("lo", rkmax=6.0)
+    hs, hsd = sctx.setup(p)
+    hs_o, hsd_o = O.setup(p)
+    w = sl.eigh(*hermitian_from_packed(hs, hsd), eigvals_only=True)
+    wo = sl.eigh(*hermitian_from_packed(hs_o, hsd_o), eigvals_only=True)
+    assert np.max(np.abs(w - wo)) <= 1e-6, np.max(np.abs(w - wo))
+
+
+@pytest.mark.gpu
+def test_split_matches_fp64_gpu_path(sctx):
+    """S=8 split and the FP64 GPU path agree to FP64 rounding on c0."""
+    p = synth.config("c0")[0]
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, 8)
+    a = sctx.setup(p)
+    sctx.set_precision(lapw1gpu.PREC_FP64)
+    b = sctx.setup(p)
+    err = rel_errors(a[0], a[1], b[0], b[1])
+    assert err["H"] <= 1e-12 and err["S"] == 0.0, err
