@@ -456,21 +456,6 @@ int lapw1gpu_kpoint_free(lapw1gpu_kpoint* k) {
 }
 
 // tile lists (device) for the triangle kernels, cached per shape in the context
-static const int2* tiles_sph(lapw1gpu_context* c, int nv, int* count) {
-  int nbi = (nv + SPH_TI - 1) / SPH_TI;
-  std::vector<int2> t;
-  for (int bi = 0; bi < nbi; bi++) {
-    int bjmax = (bi * SPH_TI + SPH_TI - 1) / SPH_TJ;
-    for (int bj = 0; bj <= bjmax; bj++) t.push_back(make_int2(bi, bj));
-  }
-  *count = (int)t.size();
-  int2* d = (int2*)c->buf("tiles_sph", sizeof(int2) * t.size());
-  if (!d) return nullptr;
-  if (cudaMemcpyAsync(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-    return nullptr;
-  return d;
-}
-
 static const int2* tiles_tri(lapw1gpu_context* c, const char* name, int n, int T, int* count) {
   int nb = (n + T - 1) / T;
   std::vector<int2> t;
@@ -487,7 +472,9 @@ static const int2* tiles_tri(lapw1gpu_context* c, const char* name, int n, int T
 // algorithmic FP64-equivalent flops of the contractions (see DESIGN.md roofline)
 static double alg_flops(const lapw1gpu_kpoint* k) {
   double nv = k->nv, n = k->n;
-  double sph = 8.0 * 2.0 * (2.0 * k->ndf) * k->ltop * (nv * (nv + 1) / 2.0);  // H and S, lower triangle
+  // spherical: per pair and atom type 6 FMA per l, 4 FMA per equivalent
+  // atom's phase product, 4 FMA to add PHASE * t into S and H
+  double sph = 2.0 * (6.0 * k->ltop * k->nat + 4.0 * k->ndf + 4.0 * k->nat) * (nv * (nv + 1) / 2.0);
   int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
   double hns = k->nohns ? 0.0 : 8.0 * (2.0 * k->ndf * nsl2) * (n * (n + 1) / 2.0);
   return sph + hns;
@@ -529,7 +516,7 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     nl++;
     k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
     int ntiles = 0;
-    const int2* tl = tiles_sph(c, nv, &ntiles);
+    const int2* tl = tiles_tri(c, "tiles_sph", nv, SPH_T, &ntiles);
     if (!tl) return LAPW1GPU_ERR_NOMEM;
     if (!c->sph_attr) {  // function attributes are per device: once per context
       CK(cudaFuncSetAttribute(k_spherical, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
@@ -753,3 +740,170 @@ int lapw1gpu_setup(lapw1gpu_context* c, const lapw1gpu_problem* p, double* hs, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------
+// HNS without device allocation.
+//
+// Some callers cannot let this library allocate device memory: a Fortran
+// lapw1 whose device memory is already reserved by the eigen-solver library
+// it hands HS to, or a host framework whose caching allocator owns the GPU,
+// where a cudaMalloc here could fail for lack of memory or fragment their
+// pool (and cudaFree synchronises the device under their stream work).
+// This entry point computes the same HNS update as the HNS stage of
+// lapw1gpu_setup_stages, with all of its intermediate buffers (the uploaded
+// inputs, AL/BL, phases, the HNS operands, tile list, status word) carved
+// from one file-scope device array of L1G_NOALLOC_BYTES.  Every GPU that
+// loads the library holds that array until the process exits.
+// ---------------------------------------------------------------------
+#define L1G_NOALLOC_BYTES (64ull << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[L1G_NOALLOC_BYTES];
+#define L1G_NOALLOC_MAXDEV 64
+static void* g_noalloc_addr[L1G_NOALLOC_MAXDEV];  // device address of the array, per device
+
+// bookkeeping tables of one problem, built on the device (one thread):
+// atom type / first atom per type, the LOHNS ranges, the triangle tiles
+__global__ void k_noalloc_tables(int nat, const int* __restrict__ mult, const int* __restrict__ ilo, int ntri,
+                                 int* atype, int* afirst, LoRange* lor, int2* tiles) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int a = 0, q = 0; a < nat; a++) {
+    afirst[a] = q;
+    for (int e = 0; e < mult[a]; e++) atype[q++] = a;
+  }
+  int nr = 0;
+  for (int jn = 0, nnlo = 0; jn < nat; jn++)
+    for (int l = 0; l <= L1G_LOMAX; l++)
+      for (int jlo = 1; jlo <= ilo[jn * (L1G_LOMAX + 1) + l]; jlo++) {
+        LoRange r{jn, l, jlo, nnlo + 1, nnlo + (2 * l + 1) * mult[jn]};
+        nnlo = r.i2;
+        lor[nr++] = r;
+      }
+  for (int bi = 0, t = 0; bi < ntri; bi++)
+    for (int bj = 0; bj <= bi; bj++) tiles[t++] = make_int2(bi, bj);
+}
+
+extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, int ldhs, void* stream) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (!d_hs_ || ldhs < p->n) return LAPW1GPU_ERR_ARG;
+  if (p->nohns) return LAPW1GPU_OK;  // calkpt.F:169: nothing to add
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= L1G_NOALLOC_MAXDEV) return LAPW1GPU_ERR_RANGE;
+  // first call on this device: the array's device address (host code only
+  // sees a host-side stand-in under its name)
+  if (!g_noalloc_addr[dev]) {
+    void* a = nullptr;
+    CK(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+    g_noalloc_addr[dev] = a;
+  }
+  char* base = (char*)g_noalloc_addr[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  double2* d_hs = reinterpret_cast<double2*>(d_hs_);
+
+  // sizes of this problem (tables themselves are built on the device)
+  const int n = p->n, nv = p->nv, nat = p->nat, ndf = p->ndf, ltop = p->ltop, ldl = p->ldl;
+  const int nvpad = round_up(nv, 64), npad = round_up(n, 64);
+  const int nsl2 = (p->lnsmax + 1) * (p->lnsmax + 1);
+  const int K = ndf * 2 * nsl2;
+  const int L4 = L1G_LOMAX + 1;
+  int nlor = 0;
+  for (int jn = 0; jn < nat; jn++)
+    for (int l = 0; l <= L1G_LOMAX; l++) nlor += p->ilo[jn * L4 + l];
+  const int ntri = (n + HNS_T - 1) / HNS_T;
+  const int ntiles = ntri * (ntri + 1) / 2;
+
+  // carve the array: inputs first, then the intermediates; the input copies
+  // are issued as the regions are taken (no host-side bookkeeping storage)
+  size_t off = 0;
+  bool fits = true;
+  auto take = [&](size_t bytes) -> char* {
+    size_t o = off;
+    off += (bytes + 255) / 256 * 256;
+    if (off > L1G_NOALLOC_BYTES) fits = false;
+    return base + o;
+  };
+  // first pass only sizes the layout; the copies run once it is known to fit
+  struct Pending {
+    char* dst;
+    const void* src;
+    size_t bytes;
+  } pend[40];
+  int npend = 0;
+  auto in = [&](const void* src, size_t bytes) -> char* {
+    char* d = take(bytes);
+    pend[npend++] = {d, src, bytes};
+    return d;
+  };
+  DevProb P{};
+  P.n = n;
+  P.nv = nv;
+  P.nlo = p->nlo;
+  P.nat = nat;
+  P.ndf = ndf;
+  P.ltop = ltop;
+  P.ldl = ldl;
+  P.lnsmax = p->lnsmax;
+  P.ins = p->ins;
+  P.nvpad = nvpad;
+  P.npad = npad;
+  P.vi = p->vi;
+  P.mult = (const int*)in(p->mult, sizeof(int) * nat);
+  int* d_atype = (int*)take(sizeof(int) * ndf);
+  int* d_afirst = (int*)take(sizeof(int) * nat);
+  P.atype = d_atype;
+  P.afirst = d_afirst;
+  P.rmt = (const double*)in(p->rmt, sizeof(double) * nat);
+  P.v = (const double*)in(p->v, sizeof(double) * nat);
+  P.pos = (const double*)in(p->pos, sizeof(double) * 3 * ndf);
+  P.rotij = (const double*)in(p->rotij, sizeof(double) * 9 * ndf);
+  P.rotloc = (const double*)in(p->rotloc, sizeof(double) * 9 * nat);
+  P.kzz = (const int*)in(p->kzz, sizeof(int) * 3 * n);
+  P.xk = (const double*)in(p->xk, sizeof(double) * n);
+  P.yk = (const double*)in(p->yk, sizeof(double) * n);
+  P.zk = (const double*)in(p->zk, sizeof(double) * n);
+  P.rk = (const double*)in(p->rk, sizeof(double) * n);
+  P.p = (const double*)in(p->p, sizeof(double) * nat * ldl);
+  P.pe = (const double*)in(p->pe, sizeof(double) * nat * ldl);
+  P.dp = (const double*)in(p->dp, sizeof(double) * nat * ldl);
+  P.dpe = (const double*)in(p->dpe, sizeof(double) * nat * ldl);
+  P.pei = (const double*)in(p->pei, sizeof(double) * nat * ldl);
+  P.e = (const double*)in(p->e, sizeof(double) * nat * ldl);
+  P.lapw = (const int*)in(p->lapw, sizeof(int) * nat * ldl);
+  P.ilo = (const int*)in(p->ilo, sizeof(int) * nat * L4);
+  P.loor = (const int*)in(p->loor, sizeof(int) * nat * L4);
+  P.alo = (const double*)in(p->alo, sizeof(double) * nat * L1G_NLOAT * L4);
+  P.blo = (const double*)in(p->blo, sizeof(double) * nat * L1G_NLOAT * L4);
+  P.clo = (const double*)in(p->clo, sizeof(double) * nat * L1G_NLOAT * L4);
+  P.elo = (const double*)in(p->elo, sizeof(double) * nat * L1G_NLOAT * L4);
+  P.pi12lo = (const double*)in(p->pi12lo, sizeof(double) * nat * L4);
+  P.pe12lo = (const double*)in(p->pe12lo, sizeof(double) * nat * L4);
+  P.dplo = (const double*)in(p->dplo, sizeof(double) * nat * L4);
+  const double2* d_tns = (const double2*)in(p->tns, sizeof(double2) * nat * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2);
+  LoRange* d_lor = (LoRange*)take(sizeof(LoRange) * (nlor > 0 ? nlor : 1));
+  int2* d_tiles = (int2*)take(sizeof(int2) * ntiles);
+  P.al = (double*)take(sizeof(double) * (size_t)nat * ltop * nvpad);
+  P.bl = (double*)take(sizeof(double) * (size_t)nat * ltop * nvpad);
+  P.phase = (double2*)take(sizeof(double2) * (size_t)ndf * npad);
+  double2* Lop = (double2*)take(sizeof(double2) * (size_t)K * npad);
+  double2* Rop = (double2*)take(sizeof(double2) * (size_t)K * npad);
+  const size_t nloc = (size_t)ndf * nsl2 * std::max(1, p->nlo);
+  double2* Clo = (double2*)take(sizeof(double2) * nloc);
+  double2* C2lo = (double2*)take(sizeof(double2) * nloc);
+  int* d_status = (int*)take(sizeof(int));
+  if (!fits) return LAPW1GPU_ERR_RANGE;  // beyond L1G_NOALLOC_BYTES
+
+  for (int q = 0; q < npend; q++)
+    if (pend[q].src && pend[q].bytes)
+      CK(cudaMemcpyAsync(pend[q].dst, pend[q].src, pend[q].bytes, cudaMemcpyHostToDevice, s));
+  // the array keeps the previous call's contents: the status word must start at 0
+  CK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
+  k_noalloc_tables<<<1, 32, 0, s>>>(nat, P.mult, P.ilo, ntri, d_atype, d_afirst, d_lor, d_tiles);
+  k_albl<<<dim3((nvpad + 127) / 128, nat), 128, 0, s>>>(P, d_status);
+  k_phase<<<dim3((npad + 127) / 128, ndf), 128, 0, s>>>(P);
+  k_hns_ops<<<dim3((npad + 127) / 128, ndf), 128, 0, s>>>(P, d_tns, d_lor, nlor, Lop, Rop, Clo, C2lo);
+  k_hns_gemm<<<(unsigned)ntiles, 256, 0, s>>>(n, npad, K, d_tiles, Lop, Rop, d_hs, ldhs);
+  if (p->nlo > 0)
+    k_hns_lo<<<dim3((p->nlo + 127) / 128, p->nlo), 128, 0, s>>>(nv, p->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);
+  CK(cudaGetLastError());
+  return LAPW1GPU_OK;
+}

@@ -32,6 +32,7 @@ EXPORTS = [
     "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
+    "lapw1gpu_hns_noalloc",
 ]
 
 _lib = None
@@ -68,6 +69,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_version.restype = C.c_char_p
     lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
                                             dp, dp, dp, ip, dp]
+    lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p]
     _lib = lib
     return lib
 
@@ -169,6 +171,14 @@ class Context:
 
 def version() -> str:
     return load().lapw1gpu_version().decode()
+
+
+def hns_noalloc(prob: Problem, d_hs_ptr: int, ldhs: int, stream: int = 0) -> None:
+    """lapw1gpu_hns_noalloc: add the HNS update into a caller-owned device
+    HS without any allocation by the library (see include/lapw1gpu.h)."""
+    cp = prob.to_c()
+    _check("lapw1gpu_hns_noalloc",
+           load().lapw1gpu_hns_noalloc(C.byref(cp), C.c_void_p(d_hs_ptr), ldhs, C.c_void_p(stream)))
 
 
 def tns_from_gaunt(nat, lnsmax, lqind, lqns, gfac, vns1, vns2, vns3, vnslo1, vnslo2, vnslo3, loor):

@@ -216,6 +216,23 @@ int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx,
                             const double* vnslo3, const int* loor,
                             double* tns);
 
+/* HNS stage without any allocation.  No counterpart in the reference: it
+ * exists for callers that cannot let this library allocate device memory,
+ * such as a lapw1 whose device memory is already reserved by the eigen-solver
+ * library that HS is handed to, or a host framework whose caching allocator
+ * owns the GPU (a cudaMalloc here could fail or fragment their pool, and
+ * cudaFree synchronises the device).  It adds the HNS update (hns.F:150-467,
+ * the same result as stage 2 of lapw1gpu_setup_stages) into d_hs, a device
+ * n x n complex column-major HS with leading dimension ldhs, on `stream`
+ * (a cudaStream_t, NULL for the default stream), asynchronously.  All of its
+ * intermediate buffers live in one 64 MiB device array inside the library
+ * (held by every GPU that loads the library until the process exits);
+ * problems needing more return LAPW1GPU_ERR_RANGE.  The first call on a
+ * device looks up that array's device address: make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race. */
+int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs, int ldhs,
+                         void* stream);
+
 /* version string of the library */
 const char* lapw1gpu_version(void);
 
