@@ -187,23 +187,28 @@ __global__ void k_table(DevProb P, TabDesc T, const double2* warp, double2* tab)
 // ---------------------------------------------------------------------
 // K-b + K-c: PW x PW block of H and S (hamilt.F:188-466 + ZSWAP).
 //
-// The reference's per-pair sum over atoms and l,
-//   S_JI += sum_a VIF_a PHASE_a(J,I) sum_l (2l+1) P_l(x_JI) s_l(I,J)
-// is regrouped as sum_l (2l+1) P_l(x_JI) G_l(J,I) with
-//   G_l(J,I) = sum_{a,r} X_l[(a,r),J] * Y_l[(a,r),I]
-//   X_l[(a,0/1),J] = phi_a(J) * {AL, BL}(J,l,type a)
-//   YS [(a,0/1),I] = conj(phi_a(I)) VIF {AL, CHN*BL}(I)
-//   YH [(a,0/1),I] = conj(phi_a(I)) VIF {(E+R^2 U DU) AL + R^2 UP DU BL,
-//                                        (1+R^2 U DUP) AL + (E CHN + R^2 UP DUP) BL}(I)
-// (the non-symmetric 2x2 block of hamilt.F:386-424, surface terms included),
-// i.e. one complex GEMM with K = 2*NDF per l and a per-pair Legendre epilogue
-// that keeps the reference's recursion and its UTOP branch (hamilt.F:250-281).
+// Per pair (J <= I), the reference accumulates, atom type by atom type,
+//   t_S = sum_l (2l+1) P_l(x_JI) [AL_J AL_I + CHN BL_J BL_I]
+//   t_H = sum_l (2l+1) P_l(x_JI) [AL_J hA_I + BL_J hB_I]
+// with hA/hB the non-symmetric 2x2 block of hamilt.F:386-424 (surface
+// kinetic terms included) applied on the column side, and adds
+// VIF * PHASE * t to S and H, PHASE = sum_eq exp(2 pi i (K_J - K_I) r_eq).
+// This kernel keeps that loop order: the Legendre weights w_l = (2l+1) P_l
+// of each pair are computed once with the reference's recursion (UTOP
+// branch included, hamilt.F:250-281) and held in registers; per atom type
+// the J-side {AL, BL} and the I-side VIF {AL, CHN BL, hA, hB} are staged in
+// shared memory; PHASE is formed as sum_eq phi_a(J) conj(phi_a(I)) from the
+// per-row phases.  That is 6 FMA per (pair, type, l) plus the phase
+// products, instead of 16 for the same sum as a GEMM over explicit (l, r).
+// Thread (tj, ti) owns rows J = j0 + tj + 16u and columns I = i0 + ti + 16v
+// (u, v in {0,1}), so shared-memory reads are conflict-free.
 // ---------------------------------------------------------------------
-#define SPH_TJ 64
-#define SPH_TI 32
-#define SPH_KT 8
+#define SPH_T 32
+#define SPH_TC 8
 #define SPH_THREADS 256
-#define SPH_DYN_SMEM (24 * SPH_THREADS * 8)
+#define SPH_LMAX 13
+// dynamic shared memory: per staged type 2 J-side and 4 I-side values per (l, row)
+#define SPH_DYN_SMEM (SPH_TC * 6 * SPH_LMAX * SPH_T * 8)
 
 struct SphCoef {  // per (type, l)
   double vif, chn, mAA, mAB, mBA, mBB;
@@ -229,181 +234,175 @@ __global__ void k_sph_coef(DevProb P, SphCoef* coef) {
 
 __global__ void __launch_bounds__(SPH_THREADS, 1)
     k_spherical(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef,
-                const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs,
-                int ld, double2* __restrict__ hsdiag) {
-  __shared__ double2 sX[2 * SPH_KT][SPH_TJ];
-  __shared__ double2 sYH[2 * SPH_KT][SPH_TI];
-  __shared__ double2 sYS[2 * SPH_KT][SPH_TI];
-  // Legendre recursion state of the 8 pairs each thread owns (48 KB dynamic)
-  extern __shared__ double sLeg[];
-  double* sLx = sLeg;
-  double* sLp1 = sLeg + 8 * SPH_THREADS;
-  double* sLp2 = sLeg + 16 * SPH_THREADS;
-
+                const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs, int ld,
+                double2* __restrict__ hsdiag) {
+  extern __shared__ double sm[];
+  // staged operands: J side [tc][l][2][32], I side [tc][l][4][32]
+  double* sJ = sm;
+  double* sI = sm + SPH_TC * SPH_LMAX * 2 * SPH_T;
   const int tid = threadIdx.x;
   const int tj = tid & 15, ti = tid >> 4;
   const int2 t = tiles[blockIdx.x];
-  const int i0 = t.x * SPH_TI, j0 = t.y * SPH_TJ;
-  const int nv = P.nv, ltop = P.ltop, ndf = P.ndf;
+  const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
+  const int nv = P.nv, ltop = P.ltop, nat = P.nat;
 
-  // Legendre argument per owned pair (hamilt.F:250-256)
+  // Legendre weights (2l+1) P_l(x_JI) of the four owned pairs
+  double w[4][SPH_LMAX];
 #pragma unroll
-  for (int u = 0; u < 4; u++)
+  for (int u = 0; u < 2; u++)
 #pragma unroll
     for (int v = 0; v < 2; v++) {
-      int J = j0 + tj * 4 + u, I = i0 + ti * 2 + v;
+      const int q = u * 2 + v;
+      const int J = j0 + tj + 16 * u, I = i0 + ti + 16 * v;
       double x = 0.0;
       if (J < nv && I < nv) {
         x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
         double den = P.rk[I] * P.rk[J];
         if (den > 1.0e-8) x = x / den;
       }
-      int q = (u * 2 + v) * SPH_THREADS + tid;
-      sLx[q] = x;
-      sLp1[q] = 0.0;
-      sLp2[q] = 0.0;
+      const bool top = !(fabs(x) < 0.9999999);
+      double pm2 = 1.0, pm1 = x;
+      w[q][0] = 1.0;
+      w[q][1] = 3.0 * x;
+#pragma unroll
+      for (int l = 2; l < SPH_LMAX; l++) {
+        double pl;
+        if (!top) {
+          const double pplx = x * pm1;
+          const double pply = pplx - pm2;
+          pl = pplx + ((double)(l - 1) / (double)l) * pply;
+        } else {
+          pl = x * pm1;
+        }
+        pm2 = pm1;
+        pm1 = pl;
+        w[q][l] = (double)(2 * l + 1) * pl;
+      }
     }
 
-  double2 aH[4][2], aS[4][2];
+  double2 aS[4], aH[4];
 #pragma unroll
-  for (int u = 0; u < 4; u++)
-#pragma unroll
-    for (int v = 0; v < 2; v++) aH[u][v] = aS[u][v] = cmk(0.0, 0.0);
+  for (int q = 0; q < 4; q++) aS[q] = aH[q] = cmk(0.0, 0.0);
 
-  for (int l = 0; l < ltop; l++) {
-    double2 gH[4][2], gS[4][2];
-#pragma unroll
-    for (int u = 0; u < 4; u++)
-#pragma unroll
-      for (int v = 0; v < 2; v++) gH[u][v] = gS[u][v] = cmk(0.0, 0.0);
-
-    for (int a0 = 0; a0 < ndf; a0 += SPH_KT) {
-      __syncthreads();
-      // operand tiles
-      for (int idx = tid; idx < SPH_KT * (SPH_TJ + SPH_TI); idx += SPH_THREADS) {
-        if (idx < SPH_KT * SPH_TJ) {
-          int ka = idx / SPH_TJ, jj = idx % SPH_TJ;
-          int a = a0 + ka, J = j0 + jj;
-          double2 x0 = cmk(0.0, 0.0), x1 = cmk(0.0, 0.0);
-          if (a < ndf && J < nv) {
-            int jn = P.atype[a];
-            double2 ph = P.phase[(size_t)a * P.npad + J];
-            size_t o = ((size_t)jn * ltop + l) * P.nvpad + J;
-            double alv = P.al[o], blv = P.bl[o];
-            x0 = cscale(ph, alv);
-            x1 = cscale(ph, blv);
-          }
-          sX[2 * ka][jj] = x0;
-          sX[2 * ka + 1][jj] = x1;
-        } else {
-          int id2 = idx - SPH_KT * SPH_TJ;
-          int ka = id2 / SPH_TI, ii = id2 % SPH_TI;
-          int a = a0 + ka, I = i0 + ii;
-          double2 h0 = cmk(0.0, 0.0), h1 = h0, s0 = h0, s1 = h0;
-          if (a < ndf && I < nv) {
-            int jn = P.atype[a];
-            double2 ph = cconj(P.phase[(size_t)a * P.npad + I]);
-            size_t o = ((size_t)jn * ltop + l) * P.nvpad + I;
-            double alv = P.al[o], blv = P.bl[o];
-            SphCoef c = coef[jn * ltop + l];
-            double2 pv = cscale(ph, c.vif);
-            s0 = cscale(pv, alv);
-            s1 = cscale(pv, c.chn * blv);
-            h0 = cscale(pv, c.mAA * alv + c.mAB * blv);
-            h1 = cscale(pv, c.mBA * alv + c.mBB * blv);
-          }
-          sYS[2 * ka][ii] = s0;
-          sYS[2 * ka + 1][ii] = s1;
-          sYH[2 * ka][ii] = h0;
-          sYH[2 * ka + 1][ii] = h1;
-        }
+  for (int t0 = 0; t0 < nat; t0 += SPH_TC) {
+    const int ntc = min(SPH_TC, nat - t0);
+    __syncthreads();
+    // stage AL/BL (J side) and VIF-scaled {AL, CHN BL, hA, hB} (I side)
+    for (int idx = tid; idx < ntc * ltop * SPH_T; idx += SPH_THREADS) {
+      const int r = idx % SPH_T, l = (idx / SPH_T) % ltop, tc = idx / (SPH_T * ltop);
+      const int jn = t0 + tc;
+      const size_t ob = ((size_t)jn * ltop + l) * P.nvpad;
+      const int J = j0 + r, I = i0 + r;
+      double aj = 0.0, bj = 0.0, ai = 0.0, bi = 0.0;
+      if (J < nv) {
+        aj = P.al[ob + J];
+        bj = P.bl[ob + J];
       }
-      __syncthreads();
-#pragma unroll 4
-      for (int k = 0; k < 2 * SPH_KT; k++) {
-        double2 xv[4], yh[2], ys[2];
+      if (I < nv) {
+        ai = P.al[ob + I];
+        bi = P.bl[ob + I];
+      }
+      const SphCoef c = coef[jn * ltop + l];
+      double* dj = sJ + ((size_t)(tc * SPH_LMAX + l) * 2) * SPH_T + r;
+      dj[0] = aj;
+      dj[SPH_T] = bj;
+      double* di = sI + ((size_t)(tc * SPH_LMAX + l) * 4) * SPH_T + r;
+      di[0] = c.vif * ai;
+      di[SPH_T] = c.vif * (c.chn * bi);
+      di[2 * SPH_T] = c.vif * (c.mAA * ai + c.mAB * bi);
+      di[3 * SPH_T] = c.vif * (c.mBA * ai + c.mBB * bi);
+    }
+    __syncthreads();
+    for (int tc = 0; tc < ntc; tc++) {
+      const int jn = t0 + tc;
+      double tS[4], tH[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) xv[u] = sX[k][tj * 4 + u];
+      for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
 #pragma unroll
-        for (int v = 0; v < 2; v++) {
-          yh[v] = sYH[k][ti * 2 + v];
-          ys[v] = sYS[k][ti * 2 + v];
-        }
+      for (int l = 0; l < SPH_LMAX; l++) {
+        if (l < ltop) {
+          const double* dj = sJ + ((size_t)(tc * SPH_LMAX + l) * 2) * SPH_T;
+          const double* di = sI + ((size_t)(tc * SPH_LMAX + l) * 4) * SPH_T;
+          double aJ[2], bJ[2], s0[2], s1[2], h0[2], h1[2];
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+          for (int u = 0; u < 2; u++) {
+            aJ[u] = dj[tj + 16 * u];
+            bJ[u] = dj[SPH_T + tj + 16 * u];
+          }
 #pragma unroll
           for (int v = 0; v < 2; v++) {
-            gH[u][v].x = fma(xv[u].x, yh[v].x, gH[u][v].x);
-            gH[u][v].x = fma(-xv[u].y, yh[v].y, gH[u][v].x);
-            gH[u][v].y = fma(xv[u].x, yh[v].y, gH[u][v].y);
-            gH[u][v].y = fma(xv[u].y, yh[v].x, gH[u][v].y);
-            gS[u][v].x = fma(xv[u].x, ys[v].x, gS[u][v].x);
-            gS[u][v].x = fma(-xv[u].y, ys[v].y, gS[u][v].x);
-            gS[u][v].y = fma(xv[u].x, ys[v].y, gS[u][v].y);
-            gS[u][v].y = fma(xv[u].y, ys[v].x, gS[u][v].y);
+            s0[v] = di[ti + 16 * v];
+            s1[v] = di[SPH_T + ti + 16 * v];
+            h0[v] = di[2 * SPH_T + ti + 16 * v];
+            h1[v] = di[3 * SPH_T + ti + 16 * v];
+          }
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+              const int q = u * 2 + v;
+              const double s = fma(bJ[u], s1[v], aJ[u] * s0[v]);
+              const double h = fma(bJ[u], h1[v], aJ[u] * h0[v]);
+              tS[q] = fma(w[q][l], s, tS[q]);
+              tH[q] = fma(w[q][l], h, tH[q]);
+            }
+        }
+      }
+      // PHASE = sum over the equivalent atoms of this type
+      double2 ph[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) ph[q] = cmk(0.0, 0.0);
+      const int a0 = P.afirst[jn], me = P.mult[jn];
+      for (int e = 0; e < me; e++) {
+        const double2* pa = P.phase + (size_t)(a0 + e) * P.npad;
+        double2 fj[2], fi[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) fj[u] = pa[min(j0 + tj + 16 * u, P.npad - 1)];
+#pragma unroll
+        for (int v = 0; v < 2; v++) fi[v] = pa[min(i0 + ti + 16 * v, P.npad - 1)];
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            const int q = u * 2 + v;
+            ph[q].x = fma(fj[u].x, fi[v].x, fma(fj[u].y, fi[v].y, ph[q].x));
+            ph[q].y = fma(fj[u].y, fi[v].x, fma(-fj[u].x, fi[v].y, ph[q].y));
           }
       }
-    }
-    // Legendre epilogue for this l
-    const double dll1 = (double)(2 * l + 1);
-    const double xl = (l >= 2) ? (double)(l - 1) / (double)l : 0.0;
 #pragma unroll
-    for (int u = 0; u < 4; u++)
-#pragma unroll
-      for (int v = 0; v < 2; v++) {
-        int q = (u * 2 + v) * SPH_THREADS + tid;
-        double x = sLx[q], pm1 = sLp1[q], pm2 = sLp2[q], pl;
-        if (l == 0)
-          pl = 1.0;
-        else if (l == 1)
-          pl = x;
-        else if (fabs(x) < 0.9999999) {
-          double pplx = x * pm1;
-          double pply = pplx - pm2;
-          pl = pplx + xl * pply;
-        } else
-          pl = x * pm1;
-        sLp2[q] = pm1;
-        sLp1[q] = pl;
-        double w = dll1 * pl;
-        aH[u][v].x = fma(w, gH[u][v].x, aH[u][v].x);
-        aH[u][v].y = fma(w, gH[u][v].y, aH[u][v].y);
-        aS[u][v].x = fma(w, gS[u][v].x, aS[u][v].x);
-        aS[u][v].y = fma(w, gS[u][v].y, aS[u][v].y);
+      for (int q = 0; q < 4; q++) {
+        aS[q].x = fma(ph[q].x, tS[q], aS[q].x);
+        aS[q].y = fma(ph[q].y, tS[q], aS[q].y);
+        aH[q].x = fma(ph[q].x, tH[q], aH[q].x);
+        aH[q].y = fma(ph[q].y, tH[q], aH[q].y);
       }
+    }
   }
   // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
   const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
 #pragma unroll
   for (int v = 0; v < 2; v++) {
-    int I = i0 + ti * 2 + v;
+    const int I = i0 + ti + 16 * v;
     if (I >= nv) continue;
     const int k1 = P.kzz[3 * I], k2 = P.kzz[3 * I + 1], k3 = P.kzz[3 * I + 2];
     const double xi = P.xk[I], yi = P.yk[I], zi = P.zk[I];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      int J = j0 + tj * 4 + u;
+    for (int u = 0; u < 2; u++) {
+      const int J = j0 + tj + 16 * u;
       if (J > I) continue;
-      double x2 = P.xk[J] * xi + P.yk[J] * yi + P.zk[J] * zi;
-      double2 th, wp;
-      if (J == I) {
-        size_t c0 = ((size_t)T.d3 * ny + T.d2) * nx + T.d1;
-        th = tab[2 * c0];
-        wp = tab[2 * c0 + 1];
-      } else {
-        int d1 = P.kzz[3 * J] - k1 + T.d1, d2 = P.kzz[3 * J + 1] - k2 + T.d2, d3 = P.kzz[3 * J + 2] - k3 + T.d3;
-        size_t c = ((size_t)d3 * ny + d2) * nx + d1;
-        th = tab[2 * c];
-        wp = tab[2 * c + 1];
-      }
-      double2 s = cadd(th, aS[u][v]);
-      double2 h = cadd(cadd(cscale(th, x2), wp), aH[u][v]);
+      const int q = u * 2 + v;
+      const double x2 = P.xk[J] * xi + P.yk[J] * yi + P.zk[J] * zi;
+      const int d1 = P.kzz[3 * J] - k1 + T.d1, d2 = P.kzz[3 * J + 1] - k2 + T.d2, d3 = P.kzz[3 * J + 2] - k3 + T.d3;
+      const size_t c = ((size_t)d3 * ny + d2) * nx + d1;
+      const double2 th = tab[2 * c], wp = tab[2 * c + 1];
+      const double2 s = cadd(th, aS[q]);
+      const double2 h = cadd(cadd(cscale(th, x2), wp), aH[q]);
       if (J == I) {
         hs[(size_t)I * ld + I] = h;
         hsdiag[I] = s;
       } else {
-        hs[(size_t)I * ld + J] = s;   // S upper: HS(J,I)
-        hs[(size_t)J * ld + I] = h;   // H lower: HS(I,J)
+        hs[(size_t)I * ld + J] = s;  // S upper: HS(J,I)
+        hs[(size_t)J * ld + I] = h;  // H lower: HS(I,J)
       }
     }
   }
@@ -689,11 +688,13 @@ __global__ void __launch_bounds__(256, 2)
     __syncthreads();
 #pragma unroll 4
     for (int kk = 0; kk < HNS_KT; kk++) {
+      // thread (ti, tj) owns rows i0 + ti + 16u and columns j0 + tj + 16v:
+      // consecutive threads read consecutive shared-memory words
       double2 lv[4], rv[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) lv[u] = sL[kk][ti * 4 + u];
+      for (int u = 0; u < 4; u++) lv[u] = sL[kk][ti + 16 * u];
 #pragma unroll
-      for (int v = 0; v < 4; v++) rv[v] = sR[kk][tj * 4 + v];
+      for (int v = 0; v < 4; v++) rv[v] = sR[kk][tj + 16 * v];
 #pragma unroll
       for (int u = 0; u < 4; u++)
 #pragma unroll
@@ -707,11 +708,11 @@ __global__ void __launch_bounds__(256, 2)
   }
 #pragma unroll
   for (int v = 0; v < 4; v++) {
-    int j = j0 + tj * 4 + v;
+    int j = j0 + tj + 16 * v;
     if (j >= n) continue;
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      int i = i0 + ti * 4 + u;
+      int i = i0 + ti + 16 * u;
       if (i >= n || i < j) continue;
       double2* dst = hs + (size_t)j * ld + i;
       *dst = cadd(*dst, acc[u][v]);
