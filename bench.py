@@ -58,10 +58,14 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0:  # sampling is live before timing starts
+                time.sleep(0.02)
+            self.rows.clear()
         except Exception:
             self.proc = None
         return self
@@ -127,28 +131,36 @@ def problem_input_bytes(p):
     return int(sum(a.nbytes for a in cp._keep))
 
 
-def cpu_reference(p, budget_s=12.0):
-    """Bounded CPU sample of the reference algorithm (the oracle on all host
-    cores): HAMILT over a contiguous slice of plane-wave columns, the LO
-    columns, and HNS for one atom; scaled to a full k-point by the work
-    fractions (column I of HAMILT costs ~I, each HNS atom the same)."""
+def _cpu_sample(p, frac):
+    """The oracle over a fraction `frac` of one k-point's work: HAMILT over
+    the last plane-wave columns worth `frac` of its work (column I of HAMILT
+    costs ~I) and HNS for round(frac * NDF) atoms (each atom costs the
+    same).  Returns (extrapolated ms per k-point, description, seconds)."""
     from oracle import oracle as O
     nv = p.nv
-    # columns [c0, nv]: work sum_{I=c0..nv} I; take the slice worth ~3%
-    frac_target = 0.03
-    c0 = int(nv * math.sqrt(1.0 - frac_target))
+    c0 = max(1, int(nv * math.sqrt(1.0 - frac)))
     t = time.perf_counter()
     O.hamilt_sample(p, c0, nv)
     t_h = time.perf_counter() - t
     frac_h = (nv * (nv + 1) / 2 - (c0 - 1) * c0 / 2) / (nv * (nv + 1) / 2)
+    na = max(1, min(p.ndf, int(round(frac * p.ndf))))
     t = time.perf_counter()
-    O.hns_sample(p, 1, 1)
+    O.hns_sample(p, 1, na)
     t_ns = time.perf_counter() - t
-    frac_ns = 1.0 / p.ndf
-    est_s = t_h / frac_h + t_ns / frac_ns
+    est_s = t_h / frac_h + t_ns * p.ndf / na
     sample = (f"HAMILT PW columns {c0}..{nv} of {nv} ({100 * frac_h:.1f}% of its work) + "
-              f"HNS atom 1 of {p.ndf}; extrapolated to one k-point")
+              f"HNS atoms 1..{na} of {p.ndf}; extrapolated to one k-point")
     return est_s * 1e3, sample, t_h + t_ns
+
+
+def cpu_reference(p, budget_s=8.0):
+    """Bounded CPU sample of the reference algorithm (the oracle, OpenMP on
+    all host cores) sized to about `budget_s` seconds: a 2% calibration
+    sample estimates the full k-point, then a sample of budget_s worth (the
+    whole k-point when it fits) is timed."""
+    est_ms, _, _ = _cpu_sample(p, 0.02)
+    frac = min(1.0, max(0.02, budget_s / (est_ms * 1e-3)))
+    return _cpu_sample(p, frac)
 
 
 def run_reference(args):
@@ -160,8 +172,9 @@ def run_reference(args):
     cores = os.cpu_count()
     vals = []
     sample = ""
+    budget = min(8.0, max(0.5, 120.0 / (args.warmup + args.steps)))  # whole run within a few minutes
     for i in range(args.warmup + args.steps):
-        v, sample, _ = cpu_reference(p)
+        v, sample, _ = cpu_reference(p, budget)
         if i >= args.warmup:
             vals.append(v)
     val = statistics.median(vals)
@@ -182,7 +195,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--prec", choices=["fp64", "split"], default="fp64")
     ap.add_argument("--slices", type=int, default=6)
@@ -230,18 +243,13 @@ def main():
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    stage_ms = {}
-    launches = 0
     with ClockSampler(local) as clk:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
-            st = step(stats=True)
-            for k, v in st.items():
-                stage_ms[k] = stage_ms.get(k, 0.0) + v
-            launches += int(st["kernel_launches"])
+            step(stats=False)  # queued on the library's stream, no host sync between k-points
         e1.record(stream)
         torch.cuda.synchronize()
     if dist is not None:
@@ -253,6 +261,17 @@ def main():
         ms = float(t.item())
     ms_step = ms / args.steps
     value = ms_step / world  # ms per k-point of the whole job (world k-points per step)
+
+    # ---- per-stage breakdown (separate pass, synchronised per k-point) ----
+    stage_ms = {}
+    n_stage = max(1, min(args.steps, 10))
+    per_step_launches = 0
+    for _ in range(n_stage):
+        st = step(stats=True)
+        for k, v in st.items():
+            stage_ms[k] = stage_ms.get(k, 0.0) + v
+        per_step_launches = int(st["kernel_launches"])
+    launches = per_step_launches * args.steps
 
     # ---- e2e through the host entry point ----
     hs_h = torch.empty((n, n, 2), dtype=torch.float64).pin_memory()
@@ -283,20 +302,27 @@ def main():
 
     # ---- roofline of the dominant kernel ----
     clocks = clk.summary()
-    avg = {k: v / args.steps for k, v in stage_ms.items()}
+    avg = {k: v / n_stage for k, v in stage_ms.items()}
     nsl2 = (p.lnsmax + 1) ** 2
-    f_sph = 8.0 * 2.0 * (2.0 * p.ndf) * p.ltop * (p.nv * (p.nv + 1) / 2.0)
+    pairs = p.nv * (p.nv + 1) / 2.0
+    # k_spherical: per pair, 6 FMA per (atom type, l), 4 per equivalent
+    # atom's phase product, 4 per type to add PHASE * t into S and H
+    f_sph = 2.0 * (6.0 * p.ltop * p.nat + 4.0 * p.ndf + 4.0 * p.nat) * pairs
+    # HNS: complex rank-K update of the lower triangle, K = 2 NDF (lmax_ns+1)^2
     f_hns = 8.0 * (2.0 * p.ndf * nsl2) * (n * (n + 1) / 2.0)
-    kern = {"k_spherical (K-b)": (f_sph, avg["ms_spherical"]), "HNS GEMM (K-ns)": (f_hns, avg["ms_hns"])}
+    kern = {"k_spherical (K-b)": (f_sph, avg["ms_spherical"]), "HNS update (K-ns)": (f_hns, avg["ms_hns"])}
     dom = max(kern, key=lambda k: kern[k][1])
     fl, t_ms = kern[dom]
-    peak = fp64_peak_tflops(torch, device) if args.prec == "fp64" else None
-    peak_src = "measured by bench.py: cuBLAS DGEMM 8192^3 best of 5 (no FP64 figure in MEASURED_PEAKS.json)"
-    if args.prec == "split":
+    fp64_peak = fp64_peak_tflops(torch, device)
+    if dom.startswith("HNS") and args.prec == "split":
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
-        peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
-        peak_src = "2 x measured dense bf16 (int8 tcgen05 rate), MEASURED_PEAKS.json"
+        bound, peak = "tensor", 2.0 * peaks.get("bf16_tflops", 1590.0)
+        peak_src = "2 x measured dense bf16 (the int8 tcgen05 rate), MEASURED_PEAKS.json; achieved in FP64-equivalent flops"
+    else:
+        bound, peak = "fp64", fp64_peak
+        peak_src = ("measured here: cuBLAS DGEMM 8192^3, best of 5 (MEASURED_PEAKS.json has no FP64 figure); "
+                    "FP64 FMA pipe, not tensor cores or HBM")
     achieved = fl / (t_ms * 1e-3) / 1e12
     traffic = None
     tj = os.path.join(ROOT, "profiles", "traffic.json")
@@ -321,10 +347,13 @@ def main():
         "fp64_equiv_tflops": (f_sph + f_hns) / (ms_step * 1e-3) / 1e12,
         "fp64_equiv_tflops_baseline_def": baseline_def_flops(p) / (ms_step * 1e-3) / 1e12,
         "stage_ms": {k: v for k, v in avg.items() if k.startswith("ms_")},
-        "roofline": {"kernel": dom, "bound": "tensor" if args.prec == "split" else "fp64",
+        "roofline": {"kernel": dom, "bound": bound,
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "peak_source": peak_src, "flops_per_launch": fl, "ms_per_launch": t_ms},
+                     "peak_source": peak_src, "flops_per_launch": fl, "ms_per_launch": t_ms,
+                     "fp64_peak_tflops": fp64_peak,
+                     "kernels": {k: {"flops": f, "ms": t, "tflops": f / (t * 1e-3) / 1e12,
+                                     "frac_fp64": f / (t * 1e-3) / 1e12 / fp64_peak} for k, (f, t) in kern.items()}},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks,

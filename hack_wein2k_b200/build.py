@@ -15,9 +15,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblapw1gpu.so")
 SOURCES = ["lapw1gpu.cu"]
-HEADERS = ["common.cuh", "kernels_fp64.cuh", "split_tc.cuh"]
+HEADERS = ["common.cuh", "kernels_fp64.cuh", "split_tc.cuh", "forces.cuh", "sph_tc.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-ccbin", "/usr/bin/g++"]
+              "-Xcompiler", "-fPIC", "-shared", "-ccbin", "/usr/bin/g++",
+              "-lcublas", "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
 
 
 def _inputs():

@@ -1,0 +1,441 @@
+// forces.cuh -- adjoint of the H/S setup: band-energy gradients on the atoms.
+//
+// E = sum_n f_n eps_n of the generalized problem H c = eps S c that SECLR4
+// solves from the packed state: H from conj of the lower triangle, S the
+// transpose of the conj of the upper one (ZHCGST factors S**T), so that
+// H(I,J) = conj(HS(I,J)) and S(I,J) = conj(HS(J,I)) for I > J.  Hellmann-Feynman for that problem gives
+//   dE/dr = sum_n f_n c_n^H (dH/dr - eps_n dS/dr) c_n.
+// Atom positions r_a (POS, lattice coordinates) enter the setup only through
+// the structure-factor phases exp(2 pi i KZZ . r_a): every contribution of
+// atom a to the packed element HS(I,J), I > J (lower, H) or HS(J,I) (upper,
+// S) carries exp(2 pi i (KZZ_J - KZZ_I) . r_a).  With D = 2 pi (KZZ_I -
+// KZZ_J), h = conj(HS_a(I,J)) and s = conj(HS_a(J,I)) the pair adds
+//   dE/dr_a,c += -2 D_c [ Im(h rho(J,I)) - Im(s rhoE(J,I)) ]
+// where rho(J,I) = sum_n f_n c_n(J) conj(c_n(I)) and rhoE carries f_n eps_n.
+// Diagonal elements do not depend on the positions (D = 0).  Radial
+// functions, rotations (ROTIJ, ROTLOC) and the warped potential are held
+// fixed: the result is the gradient of the setup as a function of POS.
+//   k_force_sph   PW x PW pairs: the spherical sums of k_spherical plus the
+//                 step-function term 3 V BESR of each atom type (k_table)
+//   k_force_lo    local-orbital columns, per equivalent atom (k_lo's terms)
+//   k_force_hns_reduce  the HNS update through its factors.  HNS adds
+//                 A(I,J) = X_J^T T conj(X_I) with X = (ALM, BLM, CLM) per atom
+//                 and T the Hermitian 3x3 block of (TUU TDU TUU21 / TUD TDD
+//                 TUD21 / TUU12 TDU12 TUU22), so A is Hermitian, the summand
+//                 is symmetric in (I, J) and the lower-triangle sum is half
+//                 the full one, which factors as
+//                   -Im sum_n f_n sum_k [Y0 conj(Zc) - Yc conj(Z0)],
+//                 Y = conj(X)^T (G c), Z = T Y.  For the (ALM, BLM) rows
+//                 Y = R^H (G c) and Z = L^T (G c) (library ZGEMMs; L carries
+//                 the TUU21/TUD21 terms of the LO rows); for the CLM rows
+//                 Y = CLM^H (G c) over the LO rows and Z = T_C Y over all
+//                 rows (k_force_hns_zc): the full matrix needs the CLM row
+//                 of T applied to plane-wave rows too, which the lower
+//                 triangle never uses
+#pragma once
+#include "kernels_fp64.cuh"
+
+#define FRC_RED_ATOMS SPH_MAXA
+#define FRC_2PI 6.283185307179586476925287
+
+__global__ void __launch_bounds__(SPH_THREADS, 1)
+    k_force_sph(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef, TabDesc T,
+                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, double* __restrict__ F) {
+  extern __shared__ double2 sm2[];
+  double2* sJ = sm2;
+  double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
+  double2* sPJ = sI + 2 * SPH_TC * SPH_LMAX * SPH_T;
+  double2* sPI = sPJ + SPH_MAXA * SPH_T;
+  __shared__ double red[FRC_RED_ATOMS][3][SPH_THREADS / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tj = tid & 15, ti = tid >> 4;
+  const int2 t = tiles[blockIdx.x];
+  const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
+  const int nv = P.nv, ltop = P.ltop, nat = P.nat;
+
+  double w[4][SPH_LMAX];
+  double dx[4][3], slen[4], x2[4];
+  double2 rj[4], re[4];  // rho(J,I) and rhoE(J,I) of the owned pairs
+  bool act[4];
+#pragma unroll
+  for (int u = 0; u < 2; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+      const int q = u * 2 + v;
+      const int J = j0 + tj + 16 * u, I = i0 + ti + 16 * v;
+      act[q] = (J < nv && I < nv && J < I);
+      double x = 0.0;
+      dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
+      slen[q] = 1.0;
+      x2[q] = 0.0;
+      rj[q] = re[q] = cmk(0.0, 0.0);
+      if (act[q]) {
+        x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
+        x2[q] = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
+        double den = P.rk[I] * P.rk[J];
+        if (den > 1.0e-8) x = x / den;
+        const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
+                  d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
+        dx[q][0] = FRC_2PI * d0;
+        dx[q][1] = FRC_2PI * d1;
+        dx[q][2] = FRC_2PI * d2;
+        // |dK| as k_table forms it (the step function's argument)
+        const double g0 = T.bk[0] * d0 + T.bk[1] * d1 + T.bk[2] * d2;
+        const double g1 = T.bk[3] * d0 + T.bk[4] * d1 + T.bk[5] * d2;
+        const double g2 = T.bk[6] * d0 + T.bk[7] * d1 + T.bk[8] * d2;
+        slen[q] = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+        rj[q] = rho[(size_t)I * ldr + J];
+        re[q] = rhoe[(size_t)I * ldr + J];
+      }
+      const bool top = !(fabs(x) < 0.9999999);
+      double pm2 = 1.0, pm1 = x;
+      w[q][0] = 1.0;
+      w[q][1] = 3.0 * x;
+#pragma unroll
+      for (int l = 2; l < SPH_LMAX; l++) {
+        double pl;
+        if (!top) {
+          const double pplx = x * pm1;
+          pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2);
+        } else {
+          pl = x * pm1;
+        }
+        pm2 = pm1;
+        pm1 = pl;
+        w[q][l] = (double)(2 * l + 1) * pl;
+      }
+    }
+
+  for (int t0 = 0; t0 < nat;) {
+    int ntc = 0, na = 0;
+    while (ntc < SPH_TC && t0 + ntc < nat && na + P.mult[t0 + ntc] <= SPH_MAXA) na += P.mult[t0 + ntc++];
+    const bool staged = ntc > 0;
+    if (!staged) ntc = 1;
+    const int a0c = P.afirst[t0];
+    __syncthreads();
+    for (int idx = tid; idx < ntc * ltop * SPH_T; idx += SPH_THREADS) {
+      const int r = idx % SPH_T, l = (idx / SPH_T) % ltop, tc = idx / (SPH_T * ltop);
+      const int jn = t0 + tc;
+      const size_t ob = ((size_t)jn * ltop + l) * P.nvpad;
+      const int J = j0 + r, I = i0 + r;
+      double aj = 0.0, bj = 0.0, ai = 0.0, bi = 0.0;
+      if (J < nv) {
+        aj = P.al[ob + J];
+        bj = P.bl[ob + J];
+      }
+      if (I < nv) {
+        ai = P.al[ob + I];
+        bi = P.bl[ob + I];
+      }
+      const SphCoef c = coef[jn * ltop + l];
+      const int s = (tc * SPH_LMAX + l) * SPH_T + r;
+      sJ[s] = cmk(aj, bj);
+      sI[2 * s] = cmk(c.vif * ai, c.vif * (c.chn * bi));
+      sI[2 * s + 1] = cmk(c.vif * (c.mAA * ai + c.mAB * bi), c.vif * (c.mBA * ai + c.mBB * bi));
+    }
+    if (staged)
+      for (int idx = tid; idx < na * SPH_T; idx += SPH_THREADS) {
+        const int r = idx % SPH_T, e = idx / SPH_T;
+        const double2* pa = P.phase + (size_t)(a0c + e) * P.npad;
+        sPJ[idx] = pa[j0 + r];
+        sPI[idx] = pa[i0 + r];
+      }
+    __syncthreads();
+    int nred = 0;  // atoms of this chunk reduced through red[]
+    for (int tc = 0; tc < ntc; tc++) {
+      const int jn = t0 + tc;
+      double tS[4], tH[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
+#pragma unroll
+      for (int l = 0; l < SPH_LMAX; l++) {
+        if (l < ltop) {
+          const int s = (tc * SPH_LMAX + l) * SPH_T;
+          double2 jv[2], is[2], ih[2];
+#pragma unroll
+          for (int u = 0; u < 2; u++) jv[u] = sJ[s + tj + 16 * u];
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            is[v] = sI[2 * (s + ti + 16 * v)];
+            ih[v] = sI[2 * (s + ti + 16 * v) + 1];
+          }
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+              const int q = u * 2 + v;
+              const double sv = fma(jv[u].y, is[v].y, jv[u].x * is[v].x);
+              const double hv = fma(jv[u].y, ih[v].y, jv[u].x * ih[v].x);
+              tS[q] = fma(w[q][l], sv, tS[q]);
+              tH[q] = fma(w[q][l], hv, tH[q]);
+            }
+        }
+      }
+      // interstitial step function of this type (hamilt.F:297-326)
+      const double v3 = 3.0 * P.v[jn], rt = P.rmt[jn];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (act[q]) {
+          const double h = slen[q] * rt;
+          double sn, cs;
+          sincos(h, &sn, &cs);
+          const double besr = (h * cs - sn) * (1.0 / (h * h * h));
+          tS[q] += v3 * besr;
+          tH[q] += x2[q] * (v3 * besr);
+        }
+      }
+      const int ae = P.afirst[jn], me = P.mult[jn];
+      for (int e = 0; e < me; e++) {
+        double fr[3] = {0.0, 0.0, 0.0};
+        double2 fj[2], fi[2];
+        if (staged) {
+          const int b = (ae - a0c + e) * SPH_T;
+#pragma unroll
+          for (int u = 0; u < 2; u++) fj[u] = sPJ[b + tj + 16 * u];
+#pragma unroll
+          for (int v = 0; v < 2; v++) fi[v] = sPI[b + ti + 16 * v];
+        } else {
+          const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
+#pragma unroll
+          for (int u = 0; u < 2; u++) fj[u] = pa[j0 + tj + 16 * u];
+#pragma unroll
+          for (int v = 0; v < 2; v++) fi[v] = pa[i0 + ti + 16 * v];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            const int q = u * 2 + v;
+            if (!act[q]) continue;
+            // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I))
+            const double cpr = fj[u].x * fi[v].x + fj[u].y * fi[v].y;
+            const double cpi = fj[u].x * fi[v].y - fj[u].y * fi[v].x;
+            const double uim = cpr * rj[q].y + cpi * rj[q].x;  // Im(cP rho(J,I))
+            const double vim = cpr * re[q].y + cpi * re[q].x;  // Im(cP rhoE(J,I))
+            const double g = -2.0 * (tH[q] * uim - tS[q] * vim);
+            fr[0] = fma(g, dx[q][0], fr[0]);
+            fr[1] = fma(g, dx[q][1], fr[1]);
+            fr[2] = fma(g, dx[q][2], fr[2]);
+          }
+        // warp partials of this atom
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          double s = fr[c];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+          if (lane == 0) {
+            if (staged && nred < FRC_RED_ATOMS)
+              red[nred][c][warp] = s;
+            else
+              atomicAdd(&F[(ae + e) * 3 + c], s);
+          }
+        }
+        if (staged) nred++;
+      }
+    }
+    __syncthreads();
+    if (staged)
+      for (int q = tid; q < nred * 3; q += SPH_THREADS) {
+        const int e = q / 3, c = q % 3;
+        double s = 0.0;
+        for (int wq = 0; wq < SPH_THREADS / 32; wq++) s += red[e][c][wq];
+        atomicAdd(&F[(a0c + e) * 3 + c], s);
+      }
+    t0 += ntc;
+  }
+}
+
+// local-orbital columns: k_lo's terms per equivalent atom, reduced per warp
+__global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const double2* __restrict__ rho,
+                           const double2* __restrict__ rhoe, int ldr, double* __restrict__ F) {
+  const LoCol c = cols[blockIdx.y];
+  const int nv = P.nv;
+  const int I = nv + c.nnlo - 1;
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int jn = c.jn, l = c.l, jlo = c.jlo, jeqo = c.jeqo, mo1 = c.mo1, mult = P.mult[jn];
+  const double pi = 3.141592653589793238462643;
+  const double r = P.rmt[jn], r2 = r * r;
+  const double pi4r2v = 4.0 * pi * sqrt(P.vi) * r * r;
+  const int o = jn * P.ldl + l;
+  const double U = P.p[o], UP = P.pe[o], DU = P.dp[o], DUP = P.dpe[o], CHN = P.pei[o], E = P.e[o];
+  const int lo4 = jn * (L1G_LOMAX + 1) + l;
+#define LOV(arr, jj) P.arr[(jn * L1G_NLOAT + (jj)-1) * (L1G_LOMAX + 1) + l]
+  const double ALO = LOV(alo, jlo), BLO = LOV(blo, jlo), CLO = LOV(clo, jlo), ELO = LOV(elo, jlo);
+  const double PI12 = P.pi12lo[lo4], PE12 = P.pe12lo[lo4], DPL = P.dplo[lo4];
+  const double c1r = ALO + PI12 * CLO;
+  const double c2r = BLO * CHN + PE12 * CLO;
+  const double c11r = ALO * E + 0.5 * (BLO + CLO * PI12 * (ELO + E));
+  const double c12r = BLO * CHN * E + 0.5 * (ALO + CLO * PI12 + CLO * PE12 * (ELO + E));
+  const double c3r = CLO + PE12 * BLO + ALO * PI12;
+  const double c13r = CLO * ELO + 0.5 * (BLO * PI12 + (ELO + E) * (ALO * PI12 + PE12 * BLO));
+  const double akinlor = 0.5 * r2 * (ALO * DU + BLO * DUP + CLO * DPL);
+  const double clr = c.clr, cli = c.cli;
+  bool inlo[L1G_NLOAT + 1];
+  const int Jf = J + 1;
+  bool any_lo = false;
+  for (int jlop = 1; jlop <= jlo; jlop++) {
+    int jbeg = nv + c.nnlo - (mo1 + l) - (2 * l + 1) * (jeqo - 1) - (jlo - jlop) * (2 * l + 1) * mult;
+    int jend = nv + c.nnlo - (jlo - jlop) * (mo1 + l + 1) - (jlo - jlop) * (jeqo - 1) * (2 * l + 1);
+    inlo[jlop] = (Jf >= jbeg && Jf <= jend);
+    any_lo |= inlo[jlop];
+  }
+  const bool act = (J < I) && (J < nv || any_lo);
+  double dxc[3] = {0.0, 0.0, 0.0};
+  double2 rj = cmk(0.0, 0.0), re = cmk(0.0, 0.0);
+  double alj = 0.0, blj = 0.0;
+  if (act) {
+    dxc[0] = FRC_2PI * (P.kzz[3 * I] - P.kzz[3 * J]);
+    dxc[1] = FRC_2PI * (P.kzz[3 * I + 1] - P.kzz[3 * J + 1]);
+    dxc[2] = FRC_2PI * (P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
+    rj = rho[(size_t)I * ldr + J];
+    re = rhoe[(size_t)I * ldr + J];
+    if (J < nv) {
+      size_t oo = ((size_t)jn * P.ltop + l) * P.nvpad + J;
+      alj = P.al[oo];
+      blj = P.bl[oo];
+    }
+  }
+  for (int jeq = 0; jeq < mult; jeq++) {
+    const int a = c.a0 + jeq;
+    double2 S = cmk(0.0, 0.0), H = cmk(0.0, 0.0);
+    if (act) {
+      const double* ra = P.pos + 3 * a;
+      double s = ra[0] * (double)(P.kzz[3 * I] - P.kzz[3 * J]) + ra[1] * (double)(P.kzz[3 * I + 1] - P.kzz[3 * J + 1]) +
+                 ra[2] * (double)(P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
+      const double2 ph = cconj(cexp2pi(s));
+      double2 yi[16], yj[16];
+      dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yi);
+      dev_ylm_row<3>(P.xk[J], P.yk[J], P.zk[J], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yj);
+      for (int mo2 = -l; mo2 <= l; mo2++) {
+        const int lm = l * (l + 1) + mo2;
+        const double clylnr = clr * yi[lm].x + cli * yi[lm].y;
+        const double clylni = cli * yi[lm].x - clr * yi[lm].y;
+        const double c1rup = c1r * clylnr * pi4r2v, c1iup = c1r * clylni * pi4r2v;
+        const double c2rup = c2r * clylnr * pi4r2v, c2iup = c2r * clylni * pi4r2v;
+        const double c3rup = c3r * clylnr * pi4r2v, c3iup = c3r * clylni * pi4r2v;
+        const double c11rup = c11r * clylnr * pi4r2v, c11iup = c11r * clylni * pi4r2v;
+        const double c12rup = c12r * clylnr * pi4r2v, c12iup = c12r * clylni * pi4r2v;
+        const double c13rup = c13r * clylnr * pi4r2v, c13iup = c13r * clylni * pi4r2v;
+        const double akinlorup = akinlor * clylnr * pi4r2v, akinloiup = akinlor * clylni * pi4r2v;
+        const double clylr = clr * yj[lm].x + cli * yj[lm].y;
+        const double clyli = cli * yj[lm].x - clr * yj[lm].y;
+        if (J < nv) {
+          const double c6r = clylr * alj * pi4r2v, c6i = clyli * alj * pi4r2v;
+          const double c7r = clylr * blj * pi4r2v, c7i = clyli * blj * pi4r2v;
+          double cabr = c6r * c1rup + c7r * c2rup + c6i * c1iup + c7i * c2iup;
+          double cabi = -c6i * c1rup - c7i * c2rup + c6r * c1iup + c7r * c2iup;
+          S = cadd(S, cmk(cabr * ph.x - cabi * ph.y, cabr * ph.y + cabi * ph.x));
+          cabr = c6r * c11rup + c7r * c12rup + c6i * c11iup + c7i * c12iup;
+          cabi = -c6i * c11rup - c7i * c12rup + c6r * c11iup + c7r * c12iup;
+          const double ua = c6r * U + c7r * UP, ub = c6i * U + c7i * UP;
+          const double akinbr = ua * akinlorup + ub * akinloiup;
+          const double akinbi = ua * akinloiup - ub * akinlorup;
+          H = cadd(H, cmk(cabr * ph.x - cabi * ph.y, cabr * ph.y + cabi * ph.x));
+          H = cadd(H, cmk(akinbr * ph.x - akinbi * ph.y, akinbr * ph.y + akinbi * ph.x));
+        } else {
+          for (int jlop = 1; jlop <= jlo; jlop++) {
+            if (!inlo[jlop]) continue;
+            const double alop = LOV(alo, jlop), blop = LOV(blo, jlop), clop = LOV(clo, jlop);
+            const double c6r = clylr * alop * pi4r2v, c6i = clyli * alop * pi4r2v;
+            const double c7r = clylr * blop * pi4r2v, c7i = clyli * blop * pi4r2v;
+            const double c8r = clylr * clop * pi4r2v, c8i = clyli * clop * pi4r2v;
+            double cr = c6r * c1rup + c6i * c1iup + c7r * c2rup + c7i * c2iup + c8r * c3rup + c8i * c3iup;
+            double ci = -c6i * c1rup + c6r * c1iup - c7i * c2rup + c7r * c2iup - c8i * c3rup + c8r * c3iup;
+            S = cadd(S, cmk(cr * ph.x - ci * ph.y, cr * ph.y + ci * ph.x));
+            cr = c6r * c11rup + c6i * c11iup + c7r * c12rup + c7i * c12iup + c8r * c13rup + c8i * c13iup;
+            ci = -c6i * c11rup + c6r * c11iup - c7i * c12rup + c7r * c12iup - c8i * c13rup + c8r * c13iup;
+            H = cadd(H, cmk(cr * ph.x - ci * ph.y, cr * ph.y + ci * ph.x));
+          }
+        }
+      }
+    }
+    // HS(I,J) = H (lower), HS(J,I) = S (upper): h = conj(H), s = conj(S)
+    const double uim = H.x * rj.y - H.y * rj.x;  // Im(conj(H) rho(J,I))
+    const double vim = S.x * re.y - S.y * re.x;  // Im(conj(S) rhoE(J,I))
+    const double g = act ? -2.0 * (uim - vim) : 0.0;
+#pragma unroll
+    for (int cc = 0; cc < 3; cc++) {
+      double v = g * dxc[cc];
+#pragma unroll
+      for (int o2 = 16; o2 > 0; o2 >>= 1) v += __shfl_down_sync(0xffffffffu, v, o2);
+      if (lane == 0) atomicAdd(&F[a * 3 + cc], v);
+    }
+  }
+#undef LOV
+}
+
+// GC[g][b][i] = G_g(i) C(i, b): g = 0 the plain block, g = 1..3 the rows
+// scaled by 2 pi KZZ_g(i), for the HNS gradient GEMMs
+__global__ void k_force_gscale(int n, int nb, const int* __restrict__ kzz, const double2* __restrict__ C, int ldc,
+                               double2* __restrict__ GC) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (i >= n) return;
+  const double2 v = C[(size_t)b * ldc + i];
+  GC[(size_t)b * n + i] = v;
+#pragma unroll
+  for (int c = 0; c < 3; c++) GC[((size_t)(c + 1) * nb + b) * n + i] = cscale(v, FRC_2PI * kzz[3 * i + c]);
+}
+
+// occupation- and energy-weighted copies of the eigenvector block
+__global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int ldc, const double* __restrict__ f,
+                               const double* __restrict__ eps, double2* __restrict__ Cf, double2* __restrict__ Ce) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (i >= n) return;
+  const double2 v = C[(size_t)b * ldc + i];
+  Cf[(size_t)b * n + i] = cscale(v, f[b]);
+  Ce[(size_t)b * n + i] = cscale(v, f[b] * eps[b]);
+}
+
+// Z_C[a][lm][col] = sum_(r,b) T_(C,r)[lm][b] Y[a][(r,b)][col] + TUU22 Y_C:
+// the CLM row of T applied to Y over all rows.  Y: [col][K] (k = (a*2 +
+// r)*nsl2 + b), Yc and Zc: [col][Kc] (k = a*nsl2 + lm), col < 4 nb
+__global__ void k_force_hns_zc(int nsl2, int K, int Kc, const int* __restrict__ atype,
+                               const double2* __restrict__ tns, const double2* __restrict__ Y,
+                               const double2* __restrict__ Yc, double2* __restrict__ Zc) {
+  const int col = blockIdx.x, a = blockIdx.y, la = threadIdx.x;
+  if (la >= nsl2) return;
+  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  const double2* y = Y + (size_t)col * K + (size_t)a * 2 * nsl2;
+  const double2* yc = Yc + (size_t)col * Kc + (size_t)a * nsl2;
+  double2 z = cmk(0.0, 0.0);
+  for (int b = 0; b < nsl2; b++) {
+    z = cadd(z, cmul(T[((size_t)6 * L1G_NSL2 + la) * L1G_NSL2 + b], y[b]));          // TUU12
+    z = cadd(z, cmul(T[((size_t)7 * L1G_NSL2 + la) * L1G_NSL2 + b], y[nsl2 + b]));   // TDU12
+    z = cadd(z, cmul(T[((size_t)8 * L1G_NSL2 + la) * L1G_NSL2 + b], yc[b]));         // TUU22
+  }
+  Zc[(size_t)col * Kc + (size_t)a * nsl2 + la] = z;
+}
+
+// F_a,c -= Im sum_n f_n sum_{k in a} [Y0 conj(Zc) - Yc conj(Z0)]; Y*, Z* are
+// [4][nb][K] (index 0: no G, 1..3: G_x, G_y, G_z), K = kper per atom
+__global__ void k_force_hns_reduce(int kper, int K, int nb, const double2* __restrict__ Y, const double2* __restrict__ Z,
+                                   const double* __restrict__ f, double* __restrict__ F) {
+  const int a = blockIdx.x;
+  __shared__ double red[3][256];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int q = threadIdx.x; q < kper * nb; q += blockDim.x) {
+    const int kk = a * kper + q % kper, b = q / kper;
+    const size_t o0 = (size_t)b * K + kk;
+    const double2 y0 = Y[o0], z0 = Z[o0];
+    const double fb = f[b];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const size_t oc = ((size_t)(c + 1) * nb + b) * K + kk;
+      const double2 yc = Y[oc], zc = Z[oc];
+      // Im(y0 conj(zc) - yc conj(z0))
+      const double im = (y0.y * zc.x - y0.x * zc.y) - (yc.y * z0.x - yc.x * z0.y);
+      acc[c] -= fb * im;
+    }
+  }
+  for (int c = 0; c < 3; c++) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int c = 0; c < 3; c++) red[c][threadIdx.x] += red[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) atomicAdd(&F[a * 3 + threadIdx.x], red[threadIdx.x][0]);
+}

@@ -207,8 +207,10 @@ __global__ void k_table(DevProb P, TabDesc T, const double2* warp, double2* tab)
 #define SPH_TC 8
 #define SPH_THREADS 256
 #define SPH_LMAX 13
-// dynamic shared memory: per staged type 2 J-side and 4 I-side values per (l, row)
-#define SPH_DYN_SMEM (SPH_TC * 6 * SPH_LMAX * SPH_T * 8)
+#define SPH_MAXA 32  // equivalent atoms whose phases one chunk stages
+// dynamic shared memory: per staged type 1 J-side and 2 I-side double2 per
+// (l, row), plus the J and I phases of up to SPH_MAXA atoms
+#define SPH_DYN_SMEM ((3 * SPH_TC * SPH_LMAX * SPH_T + 2 * SPH_MAXA * SPH_T) * 16)
 
 struct SphCoef {  // per (type, l)
   double vif, chn, mAA, mAB, mBA, mBB;
@@ -236,10 +238,13 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
     k_spherical(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef,
                 const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs, int ld,
                 double2* __restrict__ hsdiag) {
-  extern __shared__ double sm[];
-  // staged operands: J side [tc][l][2][32], I side [tc][l][4][32]
-  double* sJ = sm;
-  double* sI = sm + SPH_TC * SPH_LMAX * 2 * SPH_T;
+  extern __shared__ double2 sm2[];
+  // staged per type chunk: J side (AL, BL) [tc][l][32], I side VIF-scaled
+  // (AL, CHN BL) and (hA, hB) [tc][l][32][2], phases [atom][32] for J and I
+  double2* sJ = sm2;
+  double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
+  double2* sPJ = sI + 2 * SPH_TC * SPH_LMAX * SPH_T;
+  double2* sPI = sPJ + SPH_MAXA * SPH_T;
   const int tid = threadIdx.x;
   const int tj = tid & 15, ti = tid >> 4;
   const int2 t = tiles[blockIdx.x];
@@ -284,10 +289,14 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
 #pragma unroll
   for (int q = 0; q < 4; q++) aS[q] = aH[q] = cmk(0.0, 0.0);
 
-  for (int t0 = 0; t0 < nat; t0 += SPH_TC) {
-    const int ntc = min(SPH_TC, nat - t0);
+  for (int t0 = 0; t0 < nat;) {
+    // chunk of types whose equivalent atoms fit the staged phase rows
+    int ntc = 0, na = 0;
+    while (ntc < SPH_TC && t0 + ntc < nat && na + P.mult[t0 + ntc] <= SPH_MAXA) na += P.mult[t0 + ntc++];
+    const bool staged = ntc > 0;
+    if (!staged) ntc = 1;  // one type with more atoms than SPH_MAXA: phases from global memory
+    const int a0c = P.afirst[t0];
     __syncthreads();
-    // stage AL/BL (J side) and VIF-scaled {AL, CHN BL, hA, hB} (I side)
     for (int idx = tid; idx < ntc * ltop * SPH_T; idx += SPH_THREADS) {
       const int r = idx % SPH_T, l = (idx / SPH_T) % ltop, tc = idx / (SPH_T * ltop);
       const int jn = t0 + tc;
@@ -303,15 +312,18 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
         bi = P.bl[ob + I];
       }
       const SphCoef c = coef[jn * ltop + l];
-      double* dj = sJ + ((size_t)(tc * SPH_LMAX + l) * 2) * SPH_T + r;
-      dj[0] = aj;
-      dj[SPH_T] = bj;
-      double* di = sI + ((size_t)(tc * SPH_LMAX + l) * 4) * SPH_T + r;
-      di[0] = c.vif * ai;
-      di[SPH_T] = c.vif * (c.chn * bi);
-      di[2 * SPH_T] = c.vif * (c.mAA * ai + c.mAB * bi);
-      di[3 * SPH_T] = c.vif * (c.mBA * ai + c.mBB * bi);
+      const int s = (tc * SPH_LMAX + l) * SPH_T + r;
+      sJ[s] = cmk(aj, bj);
+      sI[2 * s] = cmk(c.vif * ai, c.vif * (c.chn * bi));
+      sI[2 * s + 1] = cmk(c.vif * (c.mAA * ai + c.mAB * bi), c.vif * (c.mBA * ai + c.mBB * bi));
     }
+    if (staged)
+      for (int idx = tid; idx < na * SPH_T; idx += SPH_THREADS) {
+        const int r = idx % SPH_T, e = idx / SPH_T;
+        const double2* pa = P.phase + (size_t)(a0c + e) * P.npad;
+        sPJ[idx] = pa[j0 + r];
+        sPI[idx] = pa[i0 + r];
+      }
     __syncthreads();
     for (int tc = 0; tc < ntc; tc++) {
       const int jn = t0 + tc;
@@ -321,30 +333,24 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
 #pragma unroll
       for (int l = 0; l < SPH_LMAX; l++) {
         if (l < ltop) {
-          const double* dj = sJ + ((size_t)(tc * SPH_LMAX + l) * 2) * SPH_T;
-          const double* di = sI + ((size_t)(tc * SPH_LMAX + l) * 4) * SPH_T;
-          double aJ[2], bJ[2], s0[2], s1[2], h0[2], h1[2];
+          const int s = (tc * SPH_LMAX + l) * SPH_T;
+          double2 jv[2], is[2], ih[2];
 #pragma unroll
-          for (int u = 0; u < 2; u++) {
-            aJ[u] = dj[tj + 16 * u];
-            bJ[u] = dj[SPH_T + tj + 16 * u];
-          }
+          for (int u = 0; u < 2; u++) jv[u] = sJ[s + tj + 16 * u];
 #pragma unroll
           for (int v = 0; v < 2; v++) {
-            s0[v] = di[ti + 16 * v];
-            s1[v] = di[SPH_T + ti + 16 * v];
-            h0[v] = di[2 * SPH_T + ti + 16 * v];
-            h1[v] = di[3 * SPH_T + ti + 16 * v];
+            is[v] = sI[2 * (s + ti + 16 * v)];
+            ih[v] = sI[2 * (s + ti + 16 * v) + 1];
           }
 #pragma unroll
           for (int u = 0; u < 2; u++)
 #pragma unroll
             for (int v = 0; v < 2; v++) {
               const int q = u * 2 + v;
-              const double s = fma(bJ[u], s1[v], aJ[u] * s0[v]);
-              const double h = fma(bJ[u], h1[v], aJ[u] * h0[v]);
-              tS[q] = fma(w[q][l], s, tS[q]);
-              tH[q] = fma(w[q][l], h, tH[q]);
+              const double sv = fma(jv[u].y, is[v].y, jv[u].x * is[v].x);
+              const double hv = fma(jv[u].y, ih[v].y, jv[u].x * ih[v].x);
+              tS[q] = fma(w[q][l], sv, tS[q]);
+              tH[q] = fma(w[q][l], hv, tH[q]);
             }
         }
       }
@@ -352,14 +358,22 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
       double2 ph[4];
 #pragma unroll
       for (int q = 0; q < 4; q++) ph[q] = cmk(0.0, 0.0);
-      const int a0 = P.afirst[jn], me = P.mult[jn];
+      const int ae = P.afirst[jn], me = P.mult[jn];
       for (int e = 0; e < me; e++) {
-        const double2* pa = P.phase + (size_t)(a0 + e) * P.npad;
         double2 fj[2], fi[2];
+        if (staged) {
+          const int b = (ae - a0c + e) * SPH_T;
 #pragma unroll
-        for (int u = 0; u < 2; u++) fj[u] = pa[min(j0 + tj + 16 * u, P.npad - 1)];
+          for (int u = 0; u < 2; u++) fj[u] = sPJ[b + tj + 16 * u];
 #pragma unroll
-        for (int v = 0; v < 2; v++) fi[v] = pa[min(i0 + ti + 16 * v, P.npad - 1)];
+          for (int v = 0; v < 2; v++) fi[v] = sPI[b + ti + 16 * v];
+        } else {
+          const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
+#pragma unroll
+          for (int u = 0; u < 2; u++) fj[u] = pa[j0 + tj + 16 * u];
+#pragma unroll
+          for (int v = 0; v < 2; v++) fi[v] = pa[i0 + ti + 16 * v];
+        }
 #pragma unroll
         for (int u = 0; u < 2; u++)
 #pragma unroll
@@ -377,6 +391,7 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
         aH[q].y = fma(ph[q].y, tH[q], aH[q].y);
       }
     }
+    t0 += ntc;
   }
   // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
   const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
@@ -525,17 +540,23 @@ __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restr
 }
 
 // ---------------------------------------------------------------------
-// K-ns operands (hns.F:165-437) for one atom a: right operand R = {ALM, BLM}
-// and left operand L = {A2, B2} in [k][row] layout, plus CLM / C2 of the LO
-// rows.  k = (a*2 + r)*nsl2 + lm.
+// K-ns operands (hns.F:165-437).  For atom a, k = (a*2 + r)*nsl2 + lm:
+//   R[k][i] = {ALM, BLM}(i, lm)            (hns.F:190-259; r = 0, 1)
+//   L[k][i] = {A2, B2}(i, lm)              (hns.F:381-434)
+// with A2 = sum_b TUU conj(ALM) + TDU conj(BLM) + TUU21 conj(CLM), B2 the
+// same with TUD, TDD, TUD21 (the TMP sums of hns.F:387-417: T times the
+// conjugate).  CLM is non-zero only on the atom's own LO rows, so
+//   k_hns_alm     builds R (and CLM, C-side of the LO rows) per row,
+//   k_hns_tmul    forms L = M conj(R) per atom as a small complex GEMM,
+//                 M = [[TUU, TDU], [TUD, TDD]] (2 nsl2 x 2 nsl2),
+//   k_hns_lo_ops  adds the CLM terms of the LO rows and their C2.
 // ---------------------------------------------------------------------
 struct LoRange {
   int jn, l, jlo, i1, i2;  // rows nv+i1..nv+i2 (1-based LO indices)
 };
 
-__global__ void k_hns_ops(DevProb P, const double2* __restrict__ tns, const LoRange* __restrict__ lor, int nlor,
-                          double2* __restrict__ Lop, double2* __restrict__ Rop, double2* __restrict__ Clo,
-                          double2* __restrict__ C2lo) {
+__global__ void k_hns_alm(DevProb P, const LoRange* __restrict__ lor, int nlor, double2* __restrict__ Rop,
+                          double2* __restrict__ Clo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
   const int a = blockIdx.y;                              // atom
   const int nsl = P.lnsmax + 1, nsl2 = nsl * nsl;
@@ -543,10 +564,8 @@ __global__ void k_hns_ops(DevProb P, const double2* __restrict__ tns, const LoRa
   const size_t Kst = (size_t)P.npad;
   double2* RA = Rop + ((size_t)(a * 2 + 0) * nsl2) * Kst + i;
   double2* RB = Rop + ((size_t)(a * 2 + 1) * nsl2) * Kst + i;
-  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2) * Kst + i;
-  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2) * Kst + i;
   if (i >= P.n) {
-    for (int lm = 0; lm < nsl2; lm++) RA[lm * Kst] = RB[lm * Kst] = LA[lm * Kst] = LB[lm * Kst] = cmk(0.0, 0.0);
+    for (int lm = 0; lm < nsl2; lm++) RA[lm * Kst] = RB[lm * Kst] = cmk(0.0, 0.0);
     return;
   }
   const int jn = P.atype[a];
@@ -555,11 +574,10 @@ __global__ void k_hns_ops(DevProb P, const double2* __restrict__ tns, const LoRa
   const double2 ph = P.phase[(size_t)a * P.npad + i];
   double2 y[25];
   dev_ylm_row<4>(P.xk[i], P.yk[i], P.zk[i], P.rotij + 9 * a, P.rotloc + 9 * jn, nsl - 1, y);
-  double2 alm[25], blm[25], clm[25];
-  // LO identity of this row for this atom type
+  // LO identity of this row for this atom's type (hns.F:223-255, LOHNS)
   int myl = -1, myjlo = 0;
   if (i >= P.nv) {
-    int li = i - P.nv + 1;
+    const int li = i - P.nv + 1;
     for (int q = 0; q < nlor; q++)
       if (lor[q].jn == jn && li >= lor[q].i1 && li <= lor[q].i2) {
         myl = lor[q].l;
@@ -570,88 +588,112 @@ __global__ void k_hns_ops(DevProb P, const double2* __restrict__ tns, const LoRa
   int lm = 0;
   for (int l0 = 0; l0 < nsl; l0++) {
     for (int m0 = -l0; m0 <= l0; m0++, lm++) {
-      double2 tt = cmul(cmul(cil, ph), cconj(y[lm]));
-      double almr = rhoatm * tt.x, almi = rhoatm * tt.y;
+      const double2 tt = cmul(cmul(cil, ph), cconj(y[lm]));
+      const double almr = rhoatm * tt.x, almi = rhoatm * tt.y;
+      double2 A = cmk(0.0, 0.0), B = A, Cc = A;
       if (i < P.nv) {
-        size_t o = ((size_t)jn * P.ltop + l0) * P.nvpad + i;
-        double alv = P.al[o], blv = P.bl[o];
-        blm[lm] = cmk(blv * almr, blv * almi);
-        alm[lm] = cmk(alv * almr, alv * almi);
-        clm[lm] = cmk(0.0, 0.0);
+        const size_t o = ((size_t)jn * P.ltop + l0) * P.nvpad + i;
+        const double alv = P.al[o], blv = P.bl[o];
+        B = cmk(blv * almr, blv * almi);
+        A = cmk(alv * almr, alv * almi);
       } else if (l0 == myl) {
-        int oo = (jn * L1G_NLOAT + myjlo - 1) * (L1G_LOMAX + 1) + l0;
-        blm[lm] = cmk(P.blo[oo] * almr, P.blo[oo] * almi);
-        clm[lm] = cmk(P.clo[oo] * almr, P.clo[oo] * almi);
-        alm[lm] = cmk(P.alo[oo] * almr, P.alo[oo] * almi);
-      } else {
-        alm[lm] = blm[lm] = clm[lm] = cmk(0.0, 0.0);
+        const int oo = (jn * L1G_NLOAT + myjlo - 1) * (L1G_LOMAX + 1) + l0;
+        B = cmk(P.blo[oo] * almr, P.blo[oo] * almi);
+        Cc = cmk(P.clo[oo] * almr, P.clo[oo] * almi);
+        A = cmk(P.alo[oo] * almr, P.alo[oo] * almi);
       }
+      RA[lm * Kst] = A;
+      RB[lm * Kst] = B;
+      if (i >= P.nv) Clo[((size_t)a * nsl2 + lm) * (size_t)P.nlo + (i - P.nv)] = Cc;
     }
     cil = cmk(-cil.y, cil.x);
   }
-  // A2/B2/C2 = T (x) conj(ALM/BLM/CLM) summed over (lp,mp) (hns.F:387-433)
-  const double2* T = tns + (size_t)jn * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+}
+
+#define TMUL_I 64
+#define TMUL_SMEM ((2 * L1G_NSL2) * (2 * L1G_NSL2) * 16 + (2 * L1G_NSL2) * TMUL_I * 16)
+// L[(a, r_out, la)][i] = sum_{(r, b)} M[(r_out, la)][(r, b)] conj(R[(a, r, b)][i])
+__global__ void __launch_bounds__(256) k_hns_tmul(int npad, int nsl2, const int* __restrict__ atype,
+                                                  const double2* __restrict__ tns, const double2* __restrict__ Rop,
+                                                  double2* __restrict__ Lop) {
+  extern __shared__ double2 tm[];
+  const int K = 2 * nsl2;
+  double2* sM = tm;          // [K][K]
+  double2* sR = tm + K * K;  // [K][TMUL_I]
+  const int a = blockIdx.y, i0 = blockIdx.x * TMUL_I;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  for (int idx = tid; idx < K * K; idx += 256) {
+    const int row = idx / K, col = idx % K;
+    const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
+    const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
+    sM[idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
+  }
+  const double2* R = Rop + (size_t)a * K * npad;
+  for (int idx = tid; idx < K * TMUL_I; idx += 256) {
+    const int k = idx / TMUL_I, ii = idx % TMUL_I;
+    sR[idx] = R[(size_t)k * npad + i0 + ii];
+  }
+  __syncthreads();
+  constexpr int PR = (2 * L1G_NSL2 + 7) / 8;  // output rows per thread
+  double2 acc[PR][2];
+#pragma unroll
+  for (int p = 0; p < PR; p++) acc[p][0] = acc[p][1] = cmk(0.0, 0.0);
+  for (int k = 0; k < K; k++) {
+    const double2 x0 = sR[k * TMUL_I + tx], x1 = sR[k * TMUL_I + tx + 32];
+#pragma unroll
+    for (int p = 0; p < PR; p++) {
+      const int row = ty + 8 * p;
+      if (row < K) {
+        const double2 m = sM[row * K + k];
+        acc[p][0].x = fma(m.x, x0.x, fma(m.y, x0.y, acc[p][0].x));
+        acc[p][0].y = fma(m.y, x0.x, fma(-m.x, x0.y, acc[p][0].y));
+        acc[p][1].x = fma(m.x, x1.x, fma(m.y, x1.y, acc[p][1].x));
+        acc[p][1].y = fma(m.y, x1.x, fma(-m.x, x1.y, acc[p][1].y));
+      }
+    }
+  }
+  double2* L = Lop + (size_t)a * K * npad;
+#pragma unroll
+  for (int p = 0; p < PR; p++) {
+    const int row = ty + 8 * p;
+    if (row < K) {
+      L[(size_t)row * npad + i0 + tx] = acc[p][0];
+      L[(size_t)row * npad + i0 + tx + 32] = acc[p][1];
+    }
+  }
+}
+
+// LO rows: A2 += TUU21 conj(CLM), B2 += TUD21 conj(CLM),
+// C2 = TUU12 conj(ALM) + TDU12 conj(BLM) + TUU22 conj(CLM)  (hns.F:391-433)
+__global__ void k_hns_lo_ops(DevProb P, const double2* __restrict__ tns, double2* __restrict__ Lop,
+                             const double2* __restrict__ Rop, const double2* __restrict__ Clo,
+                             double2* __restrict__ C2lo) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;  // LO row index
+  const int a = blockIdx.y;
+  if (c >= P.nlo) return;
+  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
+  const size_t npad = P.npad, i = P.nv + c;
+  const double2* T = tns + (size_t)P.atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  const double2* RA = Rop + ((size_t)(a * 2 + 0) * nsl2) * npad + i;
+  const double2* RB = Rop + ((size_t)(a * 2 + 1) * nsl2) * npad + i;
+  const double2* CL = Clo + (size_t)a * nsl2 * P.nlo + c;
+  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2) * npad + i;
+  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2) * npad + i;
   for (int la = 0; la < nsl2; la++) {
-    double a2r = 0, a2i = 0, b2r = 0, b2i = 0, c2r = 0, c2i = 0;
+    double2 da = cmk(0, 0), db = cmk(0, 0), dc = cmk(0, 0);
     for (int b = 0; b < nsl2; b++) {
-#define TT(blk) __ldg(&T[((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b])
-      const double2 tuu = TT(0), tdu = TT(1), tuu21 = TT(2), tud = TT(3), tdd = TT(4), tud21 = TT(5),
-                    tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
+      const double2 A = RA[b * npad], B = RB[b * npad], Cc = CL[(size_t)b * P.nlo];
+#define TT(blk) T[((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b]
+      const double2 tuu21 = TT(2), tud21 = TT(5), tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
 #undef TT
-      const double2 A = alm[b], B = blm[b], Cc = clm[b];
-      double t;
-      t = tuu.x * A.x;
-      t = t + tuu.y * A.y;
-      t = t + tdu.x * B.x;
-      t = t + tdu.y * B.y;
-      t = t + tuu21.x * Cc.x;
-      t = t + tuu21.y * Cc.y;
-      a2r = a2r + t;
-      t = tuu.y * A.x;
-      t = t - tuu.x * A.y;
-      t = t - tdu.x * B.y;
-      t = t + tdu.y * B.x;
-      t = t - tuu21.x * Cc.y;
-      t = t + tuu21.y * Cc.x;
-      a2i = a2i + t;
-      t = tud.x * A.x;
-      t = t + tud.y * A.y;
-      t = t + tdd.x * B.x;
-      t = t + tdd.y * B.y;
-      t = t + tud21.x * Cc.x;
-      t = t + tud21.y * Cc.y;
-      b2r = b2r + t;
-      t = tud.y * A.x;
-      t = t - tud.x * A.y;
-      t = t - tdd.x * B.y;
-      t = t + tdd.y * B.x;
-      t = t - tud21.x * Cc.y;
-      t = t + tud21.y * Cc.x;
-      b2i = b2i + t;
-      t = tuu12.x * A.x;
-      t = t + tuu12.y * A.y;
-      t = t + tdu12.x * B.x;
-      t = t + tdu12.y * B.y;
-      t = t + tuu22.x * Cc.x;
-      t = t + tuu22.y * Cc.y;
-      c2r = c2r + t;
-      t = tuu12.y * A.x;
-      t = t - tuu12.x * A.y;
-      t = t - tdu12.x * B.y;
-      t = t + tdu12.y * B.x;
-      t = t - tuu22.x * Cc.y;
-      t = t + tuu22.y * Cc.x;
-      c2i = c2i + t;
+      da = cadd(da, cmul(tuu21, cconj(Cc)));
+      db = cadd(db, cmul(tud21, cconj(Cc)));
+      dc = cadd(dc, cadd(cadd(cmul(tuu12, cconj(A)), cmul(tdu12, cconj(B))), cmul(tuu22, cconj(Cc))));
     }
-    RA[la * Kst] = alm[la];
-    RB[la * Kst] = blm[la];
-    LA[la * Kst] = cmk(a2r, a2i);
-    LB[la * Kst] = cmk(b2r, b2i);
-    if (i >= P.nv) {
-      size_t oc = ((size_t)a * nsl2 + la) * (size_t)(P.nlo > 0 ? P.nlo : 1) + (i - P.nv);
-      Clo[oc] = clm[la];
-      C2lo[oc] = cmk(c2r, c2i);
-    }
+    LA[la * npad] = cadd(LA[la * npad], da);
+    LB[la * npad] = cadd(LB[la * npad], db);
+    C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc;
   }
 }
 

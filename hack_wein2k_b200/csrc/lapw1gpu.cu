@@ -4,9 +4,11 @@
 // one k-point's inputs, and the stage sequence of calkpt.F:153-185:
 //   HAMILT  -> k_albl, k_phase, k_table, k_sph_coef, k_spherical, k_lo
 //   ZSWAP   -> folded into the HAMILT writes (diag(HS) = H, HSDIAG = S)
-//   HNS     -> k_hns_ops, k_hns_gemm (FP64) or the split-precision tcgen05
-//              path, k_hns_lo
+//   HNS     -> k_hns_alm, k_hns_tmul, k_hns_lo_ops (operands), then
+//              k_hns_gemm + library ZGEMM panels (FP64) or the
+//              split-precision tcgen05 path, and k_hns_lo
 //   HORB    -> k_horb_rows, k_horb_pairs per U-atom and l
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,6 +20,7 @@
 #include <vector>
 
 #include "kernels_fp64.cuh"
+#include "forces.cuh"
 
 #define L1G_VERSION "lapw1gpu 0.1 (sm_100a)"
 
@@ -39,7 +42,9 @@ struct lapw1gpu_context {
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 6;
   bool sph_attr = false;
+  cublasHandle_t blas = nullptr;  // library ZGEMM of the FP64 HNS panels
   std::map<std::string, DevBuf> bufs;
+  std::map<std::string, std::pair<long, int>> tile_keys;  // tile lists already on the device: shape, count
 
   // grow-only scratch buffer; returns nullptr on allocation failure
   void* buf(const char* name, size_t bytes) {
@@ -60,6 +65,7 @@ struct lapw1gpu_context {
 };
 
 #include "split_tc.cuh"
+#include "sph_tc.cuh"
 
 struct lapw1gpu_kpoint {
   lapw1gpu_context* ctx = nullptr;
@@ -181,6 +187,7 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   if (!c) return LAPW1GPU_ERR_ARG;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->blas) cublasDestroy(c->blas);
   for (auto& kv : c->bufs)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (c->d_status) cudaFree(c->d_status);
@@ -457,17 +464,178 @@ int lapw1gpu_kpoint_free(lapw1gpu_kpoint* k) {
 
 // tile lists (device) for the triangle kernels, cached per shape in the context
 static const int2* tiles_tri(lapw1gpu_context* c, const char* name, int n, int T, int* count) {
+  const long key = (long)n * 4096 + T;
+  auto it = c->tile_keys.find(name);
+  if (it != c->tile_keys.end() && it->second.first == key) {  // uploaded by an earlier run
+    *count = it->second.second;
+    return (const int2*)c->bufs[name].ptr;
+  }
   int nb = (n + T - 1) / T;
   std::vector<int2> t;
   for (int bi = 0; bi < nb; bi++)
     for (int bj = 0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
   *count = (int)t.size();
+  c->tile_keys.erase(name);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;  // earlier runs may still read it
   int2* d = (int2*)c->buf(name, sizeof(int2) * t.size());
   if (!d) return nullptr;
-  if (cudaMemcpyAsync(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-    return nullptr;
+  if (cudaMemcpy(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+  c->tile_keys[name] = std::make_pair(key, *count);
   return d;
 }
+
+// HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom, LO-row terms
+static int launch_hns_ops(const DevProb& P, const double2* tns, const LoRange* lor, int nlor, double2* Lop,
+                          double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl) {
+  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
+  k_hns_alm<<<dim3((P.npad + 127) / 128, P.ndf), 128, 0, s>>>(P, lor, nlor, Rop, Clo);
+  if (cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  k_hns_tmul<<<dim3(P.npad / TMUL_I, P.ndf), 256, TMUL_SMEM, s>>>(P.npad, nsl2, P.atype, tns, Rop, Lop);
+  *nl += 2;
+  if (P.nlo > 0) {
+    k_hns_lo_ops<<<dim3((P.nlo + 127) / 128, P.ndf), 128, 0, s>>>(P, tns, Lop, Rop, Clo, C2lo);
+    *nl += 1;
+  }
+  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+// Block width of the FP64 HNS update: diagonal blocks of HNS_DIAG_B rows run
+// in k_hns_gemm (64-row tiles, lower triangle only), the rows below each
+// diagonal block in one library ZGEMM per block column, as zher2m.f:69-80
+// splits its update (ZGEMV on the diagonal block, ZGEMM below).
+#define HNS_DIAG_B 512
+
+static const int2* tiles_hns_diag(lapw1gpu_context* c, int n, int* count) {
+  auto it = c->tile_keys.find("tiles_hns_diag");
+  if (it != c->tile_keys.end() && it->second.first == n) {
+    *count = it->second.second;
+    return (const int2*)c->bufs["tiles_hns_diag"].ptr;
+  }
+  std::vector<int2> t;
+  const int per = HNS_DIAG_B / HNS_T;
+  const int nt = (n + HNS_T - 1) / HNS_T;
+  for (int b0 = 0; b0 < nt; b0 += per)
+    for (int bi = b0; bi < std::min(nt, b0 + per); bi++)
+      for (int bj = b0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
+  *count = (int)t.size();
+  c->tile_keys.erase("tiles_hns_diag");
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;  // earlier runs may still read it
+  int2* d = (int2*)c->buf("tiles_hns_diag", sizeof(int2) * t.size());
+  if (!d) return nullptr;
+  if (cudaMemcpy(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+  c->tile_keys["tiles_hns_diag"] = std::make_pair((long)n, *count);
+  return d;
+}
+
+static int hns_panels_zgemm(lapw1gpu_context* c, int n, int npad, int K, const double2* Lop, const double2* Rop,
+                            double2* hs, int ld, cudaStream_t s) {
+  if (!c->blas) {
+    if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  }
+  if (cublasSetStream(c->blas, s) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  for (int c0 = 0; c0 < n; c0 += HNS_DIAG_B) {
+    const int w = std::min(HNS_DIAG_B, n - c0);
+    const int r0 = c0 + w, m = n - r0;
+    if (m <= 0) continue;
+    // HS(r0:n, c0:c0+w) += L(r0:n, :) R(c0:c0+w, :)^T ; L, R column-major npad x K
+    if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, w, K, &one, (const cuDoubleComplex*)(Lop + r0), npad,
+                    (const cuDoubleComplex*)(Rop + c0), npad, &one, (cuDoubleComplex*)(hs + (size_t)c0 * ld + r0),
+                    ld) != CUBLAS_STATUS_SUCCESS)
+      return LAPW1GPU_ERR_CUDA;
+  }
+  return LAPW1GPU_OK;
+}
+
+}  // extern "C"
+
+// Spherical part on tcgen05 (sph_tc.cuh): slice the per-l operands, then
+// one CTA per (128 J, IT I) tile of the triangle.
+template <int S, bool PAIR>
+static int sph_tc_launch(lapw1gpu_context* c, const lapw1gpu_kpoint* k, const DevProb& P, const SphCoef* coef,
+                         const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
+  using Cf = sphtc::Cfg<S>;
+  const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
+  const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;
+  const int npA = round_up(nv, 128), npB = round_up(nv, Cf::IT);
+  int8_t* A = (int8_t*)c->buf("sphA", (size_t)S * L * npA * Kp);
+  int8_t* B = (int8_t*)c->buf("sphB", (size_t)S * L * 4 * npB * Kp);
+  int* exA = (int*)c->buf("sphExA", sizeof(int) * (size_t)L * npA);
+  int* exB = (int*)c->buf("sphExB", sizeof(int) * (size_t)L * 2 * npB);
+  if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
+  const int sl_smem = Kc * 33 * (int)sizeof(double2);
+  if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
+  if (cudaFuncSetAttribute(sphtc::k_sph_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, sl_smem) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  sphtc::k_sph_slice<<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, S, A, exA);
+  sphtc::k_sph_slice<<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, S, B, exB);
+  *nl += 2;
+  CUtensorMap ta, tb;
+  if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128) || l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N))
+    return LAPW1GPU_ERR_CUDA;
+  const long key = (long)nv * 1024 + Cf::IT;
+  int ntile = 0;
+  int2* dt = nullptr;
+  auto it = c->tile_keys.find("tiles_sphtc");
+  if (it != c->tile_keys.end() && it->second.first == key) {
+    ntile = it->second.second;
+    dt = (int2*)c->bufs["tiles_sphtc"].ptr;
+  } else {
+    std::vector<int2> t;
+    const int nbj = npA / 128, nbi = npB / Cf::IT;
+    for (int bj = 0; bj < nbj; bj++)
+      for (int bi = 0; bi < nbi; bi++)
+        if (bj * 128 <= bi * Cf::IT + Cf::IT - 1) t.push_back(make_int2(bj, bi));
+    c->tile_keys.erase("tiles_sphtc");
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;  // earlier runs may still read it
+    dt = (int2*)c->buf("tiles_sphtc", sizeof(int2) * t.size());
+    if (!dt) return LAPW1GPU_ERR_NOMEM;
+    if (cudaMemcpy(dt, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return LAPW1GPU_ERR_CUDA;
+    ntile = (int)t.size();
+    c->tile_keys["tiles_sphtc"] = std::make_pair(key, ntile);
+  }
+  if (cudaFuncSetAttribute(sphtc::k_sph_tc<S, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM) !=
+      cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  sphtc::k_sph_tc<S, PAIR><<<ntile, Cf::THREADS, Cf::SMEM, s>>>(ta, tb, P, dt, Kp / 64, npA, npB, exA, exB, tab,
+                                                                k->tab, hs, ld, hsdiag, c->d_status);
+  *nl += 1;
+  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+// Pairing two levels in int32 before the conversion is exact while
+// (d+1) 4096 Kp 128 + (d+2) 4096 Kp < 2^31 for every level d < S-1
+// (|slice| <= 64, level d sums d+1 products per k).
+static bool sph_pair_ok(int S, int Kp) {
+  const double worst = (double)S * 4096.0 * Kp * 128.0 + (double)(S + 1) * 4096.0 * Kp;
+  return worst < 2147483647.0;
+}
+
+// true when the split-precision spherical path handles this slice count
+static bool sph_tc_supported(int S) { return false && S >= 4 && S <= 7; }
+
+static int sph_tc_dispatch(lapw1gpu_context* c, const lapw1gpu_kpoint* k, const DevProb& P, const SphCoef* coef,
+                           const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
+  const int Kp = 2 * round_up(2 * k->ndf, 32);
+  const bool pair = sph_pair_ok(c->slices, Kp);
+#define SPH_CASE(SS)                                                                   \
+  case SS:                                                                             \
+    return pair ? sph_tc_launch<SS, true>(c, k, P, coef, tab, hs, ld, hsdiag, s, nl)   \
+                : sph_tc_launch<SS, false>(c, k, P, coef, tab, hs, ld, hsdiag, s, nl);
+  switch (c->slices) {
+    SPH_CASE(4)
+    SPH_CASE(5)
+    SPH_CASE(6)
+    SPH_CASE(7)
+    default:
+      return LAPW1GPU_ERR_RANGE;
+  }
+#undef SPH_CASE
+}
+
+extern "C" {
 
 // algorithmic FP64-equivalent flops of the contractions (see DESIGN.md roofline)
 static double alg_flops(const lapw1gpu_kpoint* k) {
@@ -518,12 +686,17 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     int ntiles = 0;
     const int2* tl = tiles_tri(c, "tiles_sph", nv, SPH_T, &ntiles);
     if (!tl) return LAPW1GPU_ERR_NOMEM;
-    if (!c->sph_attr) {  // function attributes are per device: once per context
-      CK(cudaFuncSetAttribute(k_spherical, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
-      c->sph_attr = true;
+    if (c->prec == LAPW1GPU_PREC_SPLIT && sph_tc_supported(c->slices)) {
+      int rc = sph_tc_dispatch(c, k, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl);
+      if (rc) return rc;
+    } else {
+      if (!c->sph_attr) {  // function attributes are per device: once per context
+        CK(cudaFuncSetAttribute(k_spherical, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
+        c->sph_attr = true;
+      }
+      nl++;
+      k_spherical<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, tab, k->tab, d_hs, ldhs, d_hsdiag);
     }
-    nl++;
-    k_spherical<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, tab, k->tab, d_hs, ldhs, d_hsdiag);
     CK(cudaGetLastError());
     if (st) CK(cudaEventRecord(c->ev[2], s));
     // ---- K-b': local-orbital columns ----
@@ -546,19 +719,19 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
     double2* C2lo = (double2*)c->buf("hnsC2lo", sizeof(double2) * nloc);
     if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
-    nl++;
-    k_hns_ops<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P, k->d_tns, k->d_loranges,
-                                                               (int)k->loranges.size(), Lop, Rop, Clo, C2lo);
-    CK(cudaGetLastError());
-    int rc = LAPW1GPU_OK;
+    int rc = launch_hns_ops(P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    if (rc) return rc;
     if (c->prec == LAPW1GPU_PREC_SPLIT)
       rc = split_hns_gemm(c, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices, s, &nl);
     else {
+      // the blocked form of ZHER2M (zher2m.f:69-80): diagonal blocks of the
+      // lower triangle by k_hns_gemm, the panels below them by ZGEMM
       int ntiles = 0;
-      const int2* tl = tiles_tri(c, "tiles_hns", n, HNS_T, &ntiles);
+      const int2* tl = tiles_hns_diag(c, n, &ntiles);
       if (!tl) return LAPW1GPU_ERR_NOMEM;
       nl++;
       k_hns_gemm<<<ntiles, 256, 0, s>>>(n, k->npad, K, tl, Lop, Rop, d_hs, ldhs);
+      rc = hns_panels_zgemm(c, n, k->npad, K, Lop, Rop, d_hs, ldhs, s);
     }
     if (rc) return rc;
     if (k->nlo > 0) {
@@ -739,6 +912,97 @@ int lapw1gpu_setup(lapw1gpu_context* c, const lapw1gpu_problem* p, double* hs, i
   return lapw1gpu_setup_stages(c, p, 7, hs, ldhs, hsdiag, st);
 }
 
+// Band-energy gradient (forces.cuh): rho = C f C^H and rhoE = C f eps C^H by
+// library ZGEMM, the PW x PW and LO parts by k_force_sph / k_force_lo, the
+// HNS part through its factors (four ZGEMMs and a per-atom reduction).
+int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_, int ldc, int nb, const double* d_occ,
+                    const double* d_eps, double* d_grad) {
+  if (!c || !k || k->ctx != c || !d_c_ || !d_occ || !d_eps || !d_grad || nb < 1 || ldc < k->n)
+    return LAPW1GPU_ERR_ARG;
+  if (!k->orbs.empty()) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  const double2* C = reinterpret_cast<const double2*>(d_c_);
+  cudaStream_t s = c->stream;
+  DevProb P = k->P;
+  const int n = k->n, nv = k->nv, ltop = k->ltop, ndf = k->ndf, nat = k->nat, nlo = k->nlo;
+  P.al = (double*)c->buf("al", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.bl = (double*)c->buf("bl", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.phase = (double2*)c->buf("phase", sizeof(double2) * (size_t)ndf * k->npad);
+  double2* Cf = (double2*)c->buf("frc_cf", sizeof(double2) * (size_t)n * nb);
+  double2* Ce = (double2*)c->buf("frc_ce", sizeof(double2) * (size_t)n * nb);
+  double2* rho = (double2*)c->buf("frc_rho", sizeof(double2) * (size_t)n * n);
+  double2* rhoe = (double2*)c->buf("frc_rhoe", sizeof(double2) * (size_t)n * n);
+  SphCoef* coef = (SphCoef*)c->buf("coef", sizeof(SphCoef) * nat * ltop);
+  if (!P.al || !P.bl || !P.phase || !Cf || !Ce || !rho || !rhoe || !coef) return LAPW1GPU_ERR_NOMEM;
+  if (!c->blas && cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  if (cublasSetStream(c->blas, s) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * ndf, s));
+  k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
+  k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
+  k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
+  k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, Cf, Ce);
+  CK(cudaGetLastError());
+  // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)): column-major n x n
+  if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Cf, n,
+                  (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
+      cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Ce, n,
+                  (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
+    return LAPW1GPU_ERR_CUDA;
+  int ntiles = 0;
+  const int2* tl = tiles_tri(c, "tiles_sph", nv, SPH_T, &ntiles);
+  if (!tl) return LAPW1GPU_ERR_NOMEM;
+  CK(cudaFuncSetAttribute(k_force_sph, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
+  k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, d_grad);
+  CK(cudaGetLastError());
+  if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, d_grad);
+  CK(cudaGetLastError());
+  if (!k->nohns) {
+    const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
+    const int K = ndf * 2 * nsl2, Kc = ndf * nsl2;
+    double2* Lop = (double2*)c->buf("hnsL", sizeof(double2) * (size_t)K * k->npad);
+    double2* Rop = (double2*)c->buf("hnsR", sizeof(double2) * (size_t)K * k->npad);
+    size_t nloc = (size_t)Kc * std::max(1, nlo);
+    double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
+    double2* C2lo = (double2*)c->buf("hnsC2lo", sizeof(double2) * nloc);
+    double2* GC = (double2*)c->buf("frc_gc", sizeof(double2) * (size_t)4 * nb * n);
+    double2* Y = (double2*)c->buf("frc_y", sizeof(double2) * (size_t)4 * nb * K);
+    double2* Z = (double2*)c->buf("frc_z", sizeof(double2) * (size_t)4 * nb * K);
+    if (!Lop || !Rop || !Clo || !C2lo || !GC || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
+    int nl = 0;
+    int rc = launch_hns_ops(P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    if (rc) return rc;
+    k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
+    CK(cudaGetLastError());
+    // Y = R^H (G c), Z = L^T (G c): K x 4nb, rows of R and L beyond n unused
+    if (cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
+                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS ||
+        cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Lop, k->npad,
+                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Z, K) != CUBLAS_STATUS_SUCCESS)
+      return LAPW1GPU_ERR_CUDA;
+    k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
+    CK(cudaGetLastError());
+    if (nlo > 0) {
+      // CLM rows: Yc = CLM^H (G c) over the LO rows, Zc = T_C (Y; Yc)
+      double2* Yc = (double2*)c->buf("frc_yc", sizeof(double2) * (size_t)4 * nb * Kc);
+      double2* Zc = (double2*)c->buf("frc_zc", sizeof(double2) * (size_t)4 * nb * Kc);
+      if (!Yc || !Zc) return LAPW1GPU_ERR_NOMEM;
+      if (cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
+                      (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc, Kc) != CUBLAS_STATUS_SUCCESS)
+        return LAPW1GPU_ERR_CUDA;
+      k_force_hns_zc<<<dim3(4 * nb, ndf), 32, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Zc);
+      k_force_hns_reduce<<<ndf, 256, 0, s>>>(nsl2, Kc, nb, Yc, Zc, d_occ, d_grad);
+      CK(cudaGetLastError());
+    }
+  }
+  int hstat = 0;
+  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  c->last_status = hstat;
+  return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------
@@ -900,7 +1164,9 @@ extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, in
   k_noalloc_tables<<<1, 32, 0, s>>>(nat, P.mult, P.ilo, ntri, d_atype, d_afirst, d_lor, d_tiles);
   k_albl<<<dim3((nvpad + 127) / 128, nat), 128, 0, s>>>(P, d_status);
   k_phase<<<dim3((npad + 127) / 128, ndf), 128, 0, s>>>(P);
-  k_hns_ops<<<dim3((npad + 127) / 128, ndf), 128, 0, s>>>(P, d_tns, d_lor, nlor, Lop, Rop, Clo, C2lo);
+  int nops = 0;
+  rc = launch_hns_ops(P, d_tns, d_lor, nlor, Lop, Rop, Clo, C2lo, s, &nops);
+  if (rc) return rc;
   k_hns_gemm<<<(unsigned)ntiles, 256, 0, s>>>(n, npad, K, d_tiles, Lop, Rop, d_hs, ldhs);
   if (p->nlo > 0)
     k_hns_lo<<<dim3((p->nlo + 127) / 128, p->nlo), 128, 0, s>>>(nv, p->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);

@@ -1,0 +1,441 @@
+// sph_tc.cuh -- the spherical muffin-tin part of H and S (hamilt.F:371-440)
+// on the 5th-generation tensor cores, split precision, sm_100a.
+//
+// For a pair (J <= I) HAMILT accumulates, per atom type and l,
+//   S(J,I) += PHASE(J,I) (2l+1) P_l(x_JI) VIF [AL_J AL_I + CHN BL_J BL_I]
+// and the same with the non-symmetric 2x2 block for H.  With PHASE =
+// sum_eq phi_a(J) conj(phi_a(I)) the type and equivalent-atom sums at fixed
+// l are one complex GEMM over k = (atom a, r in {AL, BL}):
+//   G_l(J, I) = sum_k u_l(J,k) conj(v_l(I,k)),
+//   u_l(J, (a,r)) = phi_a(J) {AL, BL}_(type a, l, J),
+//   v_l(I, (a,r)) = phi_a(I) VIF {AL, CHN BL} (S) or VIF {hA, hB} (H),
+// and the Legendre weight w_l(J,I) = (2l+1) P_l(x_JI), which couples J and I
+// non-separably, is applied per pair as G_l leaves the accumulator:
+//   aS(J,I) = sum_l w_l(J,I) G^S_l(J,I), aH likewise.
+// The GEMMs run as Ozaki int8 slice products (the scheme of split_tc.cuh:
+// power-of-two row scales, S slices, one exact int32 TMEM accumulator per
+// level p+q-2 < S) with kind::i8 tcgen05.mma, M = 128 rows J, N = 4 real
+// columns per I (S re, S im, H re, H im).  The accumulator is double
+// buffered over l (2 x S levels x N columns of TMEM), so the FP64 epilogue
+// of l (combine levels, scale, weight, accumulate per pair in registers)
+// overlaps the MMAs of l+1.  After the last l the interstitial terms are
+// gathered from the Theta/WARP table and HS is written as k_spherical does.
+//
+// Warp roles: warps 0-7 epilogue (warp w reads TMEM lanes 32 (w%4).. and
+// the I half w/4 of the tile), warp 8 lane 0 issues TMA and MMA.  Every
+// mbarrier wait is bounded; a timeout sets a status bit and ends the CTA's
+// work cleanly (copies drained, MMAs complete, TMEM freed).
+#pragma once
+
+namespace sphtc {
+
+using split::desc_sw64;
+using split::idesc_i8;
+using split::mbar_expect_tx;
+using split::mbar_init;
+using split::mbar_wait;
+using split::smem_u32;
+using split::tc_fence_after;
+using split::tc_fence_before;
+using split::tma_load_3d;
+
+template <int S>
+struct Cfg {
+  static constexpr int N = ((512 / (2 * S)) / 16) * 16;  // real columns per accumulator buffer
+  static constexpr int IT = N / 4;                        // I per tile
+  static constexpr int A_BYTES = S * 128 * 64;
+  static constexpr int B_BYTES = S * N * 64;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int STAGES = (4 * STAGE + 1024 <= 200 * 1024) ? 4 : 3;
+  static constexpr int SMEM = STAGES * STAGE + 1024;
+  static constexpr int THREADS = 288;
+};
+
+// Operand rows of one l, built from AL/BL, phases and the per-(type, l)
+// coefficients, then cut into S int8 slices with a power-of-two scale per
+// complex row.  isB = 0: complex row J -> real row J = [Re u | Im u].
+// isB = 1: complex row c = 2 I + m (m = 0 S, 1 H) -> real rows 2c =
+// [Re v | Im v] and 2c+1 = [-Im v | Re v], so that a real dot product with
+// [Re u | Im u] gives Re and Im of u conj(v).  out: [S][L][rows][Kp] int8,
+// Kp = 2 Kcp; ex: [L][complex rows] exponents.  32 complex rows per block.
+__global__ void __launch_bounds__(256) k_sph_slice(DevProb P, const SphCoef* __restrict__ coef, int isB, int Kcp,
+                                                   int ncrow, int S, int8_t* __restrict__ out, int* __restrict__ ex) {
+  extern __shared__ double2 tile[];  // [Kc][33]
+  __shared__ double red[8][32];
+  __shared__ int rexp[32];
+  const int l = blockIdx.y, L = P.ltop;
+  const int rc0 = blockIdx.x * 32;
+  const int tid = threadIdx.x;
+  const int Kc = 2 * P.ndf, Kp = 2 * Kcp;
+  const int nrow_real = isB ? 2 * ncrow : ncrow;  // real rows per l
+  // values
+  for (int idx = tid; idx < 32 * Kc; idx += 256) {
+    const int r = idx & 31, k = idx >> 5;
+    const int rc = rc0 + r;
+    const int row = isB ? (rc >> 1) : rc;  // J or I
+    double2 v = make_double2(0.0, 0.0);
+    if (rc < ncrow && row < P.nv) {
+      const int a = k >> 1, rr = k & 1, t = P.atype[a];
+      const size_t o = ((size_t)t * L + l) * P.nvpad + row;
+      const double al = P.al[o], bl = P.bl[o];
+      double x;
+      if (!isB) {
+        x = rr ? bl : al;
+      } else {
+        const SphCoef c = coef[t * L + l];
+        if ((rc & 1) == 0)
+          x = c.vif * (rr ? c.chn * bl : al);
+        else
+          x = c.vif * (rr ? (c.mBA * al + c.mBB * bl) : (c.mAA * al + c.mAB * bl));
+      }
+      const double2 ph = P.phase[(size_t)a * P.npad + row];
+      v = make_double2(ph.x * x, ph.y * x);
+    }
+    tile[k * 33 + r] = v;
+  }
+  __syncthreads();
+  {
+    const int r = tid & 31, part = tid >> 5;
+    double m = 0.0;
+    for (int k = part; k < Kc; k += 8) {
+      const double2 v = tile[k * 33 + r];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+    red[part][r] = m;
+    __syncthreads();
+    if (tid < 32) {
+      double mm = 0.0;
+      for (int q = 0; q < 8; q++) mm = fmax(mm, red[q][tid]);
+      const int e = (mm > 0.0) ? ilogb(mm) + 1 : 0;
+      rexp[tid] = e;
+      if (rc0 + tid < ncrow) ex[(size_t)l * ncrow + rc0 + tid] = e;
+    }
+    __syncthreads();
+  }
+  const int rr = tid >> 3;       // complex row within the block
+  const int kq = (tid & 7) * 8;  // 8 consecutive k
+  const int rc = rc0 + rr;
+  const int e = rexp[rr];
+  const size_t plane = (size_t)L * nrow_real * Kp;  // one slice plane
+  for (int k0 = 0; k0 < Kcp; k0 += 64) {
+    const int col = k0 + kq;
+    if (col >= Kcp || rc >= ncrow) continue;
+    uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
+#pragma unroll
+    for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const int k = col + t;
+      const double2 v = (k < Kc) ? tile[k * 33 + rr] : make_double2(0.0, 0.0);
+      double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
+#pragma unroll
+      for (int p = 0; p < L1G_MAX_SLICES; p++) {
+        if (p < S) {
+          const double ar = rint(tr), ai = rint(ti);
+          tr = (tr - ar) * 128.0;
+          ti = (ti - ai) * 128.0;
+          pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
+          pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < L1G_MAX_SLICES; p++) {
+      if (p >= S) break;
+      int8_t* base = out + (size_t)p * plane + (size_t)l * nrow_real * Kp;
+      if (!isB) {
+        *(uint64_t*)(base + (size_t)rc * Kp + col) = pre[p];
+        *(uint64_t*)(base + (size_t)rc * Kp + Kcp + col) = pim[p];
+      } else {
+        uint64_t nim = 0;
+#pragma unroll
+        for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
+        *(uint64_t*)(base + (size_t)(2 * rc) * Kp + col) = pre[p];
+        *(uint64_t*)(base + (size_t)(2 * rc) * Kp + Kcp + col) = pim[p];
+        *(uint64_t*)(base + (size_t)(2 * rc + 1) * Kp + col) = nim;
+        *(uint64_t*)(base + (size_t)(2 * rc + 1) * Kp + Kcp + col) = pre[p];
+      }
+    }
+  }
+}
+
+// level sum of one accumulator column: sum_d c_d 2^(-7d), levels paired in
+// int32 (c_d 128 + c_(d+1), exact when PAIR holds) before the conversion
+template <int S, bool PAIR>
+__device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
+  double v = 0.0, w = 1.0;
+  if (PAIR) {
+#pragma unroll
+    for (int d = 0; d < S; d += 2) {
+      if (d + 1 < S) {
+        const int pr = (int)r[d] * 128 + (int)r[d + 1];
+        v = fma((double)pr, w * 0.0078125, v);
+      } else {
+        v = fma((double)(int)r[d], w, v);
+      }
+      w *= 6.103515625e-05;  // 2^-14
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < S; d++) {
+      v = fma((double)(int)r[d], w, v);
+      w *= 0.0078125;
+    }
+  }
+  return v;
+}
+
+template <int S, bool PAIR>
+__global__ void __launch_bounds__(288, 1)
+    k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
+             const int2* __restrict__ tiles, int nkb, int npA, int npB, const int* __restrict__ exA,
+             const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs,
+             int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
+  using C = Cfg<S>;
+  constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = IT / 2;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 tt = tiles[blockIdx.x];
+  const int j0 = tt.x * 128, i0 = tt.y * IT;
+  const int L = P.ltop, nv = P.nv;
+
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 8);  // one arrival per epilogue warp
+    }
+    mbar_init(&accbar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_i8(128, N);
+      const int nit = L * nkb;
+      int issued = 0;
+      bool ok = true;
+      auto load = [&](int it) {
+        const int st = it % STAGES, l = it / nkb, kb = it % nkb;
+        uint8_t* a = smem + st * C::STAGE;
+        uint8_t* b = a + C::A_BYTES;
+        mbar_expect_tx(&full[st], C::STAGE);
+        tma_load_3d(a, &tmA, &full[st], kb * 64, l * npA + j0, 0);
+        tma_load_3d(b, &tmB, &full[st], kb * 64, l * 4 * npB + 4 * i0, 0);
+      };
+      for (int it = 0; it < STAGES - 1 && it < nit; it++) load(issued++);
+      for (int it = 0; it < nit && ok; it++) {
+        const int st = it % STAGES, l = it / nkb, kb = it % nkb, buf = l & 1;
+        if (kb == 0 && l >= 2 && !mbar_wait(&tempty[buf], ((l - 2) >> 1) & 1)) {
+          ok = false;
+          break;
+        }
+        if (!mbar_wait(&full[st], (it / STAGES) & 1)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(smem + st * C::STAGE);
+        const uint32_t b0 = a0 + C::A_BYTES;
+#pragma unroll
+        for (int p = 0; p < S; p++)
+#pragma unroll
+          for (int q = 0; q < S - p; q++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
+              const uint64_t bd = desc_sw64(b0 + q * N * 64 + h * 32);
+              const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
+              const uint32_t d = tmem + (uint32_t)(buf * S * N + (p + q) * N);
+              asm volatile(
+                  "{\n\t.reg .pred pa;\n\t"
+                  "setp.ne.b32 pa, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
+                  "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                  : "memory");
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&empty[st]))
+                     : "memory");
+        if (kb == nkb - 1)
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_u32(&tfull[buf]))
+                       : "memory");
+        const int nx = it + STAGES - 1;
+        if (nx < nit) {
+          const int rs = nx % STAGES;
+          if (nx >= STAGES && !mbar_wait(&empty[rs], ((nx - STAGES) / STAGES) & 1)) {
+            ok = false;
+            break;
+          }
+          load(nx);
+          issued = nx + 1;
+        }
+      }
+      if (!ok) {
+        atomicOr(status, L1G_STATUS_TIMEOUT);
+        abort_flag = 1;
+        for (int it = issued - STAGES > 0 ? issued - STAGES : 0; it < issued; it++)
+          mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&accbar))
+                   : "memory");
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue warps ----
+    const int g = warp & 3, hh = warp >> 2;
+    const int J = j0 + 32 * g + lane;
+    const bool jin = J < nv;
+    const double xj = jin ? P.xk[J] : 0.0, yj = jin ? P.yk[J] : 0.0, zj = jin ? P.zk[J] : 0.0;
+    const double rj = jin ? P.rk[J] : 0.0;
+    double x[HALF], pm1[HALF], pm2[HALF];
+    double2 aS[HALF], aH[HALF];
+#pragma unroll
+    for (int u = 0; u < HALF; u++) {
+      const int I = i0 + hh * HALF + u;
+      double xx = 0.0;
+      if (jin && I < nv) {
+        xx = P.xk[I] * xj + P.yk[I] * yj + P.zk[I] * zj;
+        const double den = P.rk[I] * rj;
+        if (den > 1.0e-8) xx = xx / den;
+      }
+      x[u] = xx;
+      pm1[u] = xx;   // P_1
+      pm2[u] = 1.0;  // P_0
+      aS[u] = aH[u] = make_double2(0.0, 0.0);
+    }
+    const uint32_t trow = tmem + ((uint32_t)(32 * g) << 16);
+    bool ok = true;
+    for (int l = 0; l < L && ok; l++) {
+      const int buf = l & 1;
+      // warp-uniform outcome: the TMEM loads below are .sync.aligned
+      if (!__all_sync(0xffffffffu, mbar_wait(&tfull[buf], (l >> 1) & 1))) {
+        ok = false;
+        if (lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
+        break;
+      }
+      if (*(volatile int*)&abort_flag) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      // Legendre weights of this l (hamilt.F:250-281 recursion, UTOP branch)
+      double w[HALF];
+#pragma unroll
+      for (int u = 0; u < HALF; u++) {
+        double pl;
+        if (l == 0)
+          pl = 1.0;
+        else if (l == 1)
+          pl = x[u];
+        else {
+          if (fabs(x[u]) < 0.9999999) {
+            const double pplx = x[u] * pm1[u];
+            pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2[u]);
+          } else {
+            pl = x[u] * pm1[u];
+          }
+          pm2[u] = pm1[u];
+          pm1[u] = pl;
+        }
+        w[u] = (double)(2 * l + 1) * pl;
+      }
+      const int ea = jin ? exA[(size_t)l * npA + J] : 0;
+      // 4 real columns per I: S re, S im, H re, H im; this thread's HALF I
+      // start at column 4 * HALF * hh; read 8 columns (2 I) at a time
+#pragma unroll
+      for (int c = 0; c < HALF / 2; c++) {
+        uint32_t r[S][8];
+#pragma unroll
+        for (int d = 0; d < S; d++)
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+              : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
+                "=r"(r[d][6]), "=r"(r[d][7])
+              : "r"(trow + (uint32_t)(buf * S * N + d * N + 4 * HALF * hh + 8 * c)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (c == HALF / 2 - 1) {
+          // all columns of this buffer read: hand it back to the MMA issuer
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf])) : "memory");
+        }
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int u = 2 * c + q;
+          const int I = i0 + hh * HALF + u;
+          const int cI = (I < nv) ? I : 0;
+          const int ebS = exB[(size_t)l * 2 * npB + 2 * cI], ebH = exB[(size_t)l * 2 * npB + 2 * cI + 1];
+          const double sS = ldexp(w[u], ea + ebS - 12);
+          const double sH = ldexp(w[u], ea + ebH - 12);
+          double v[4];
+#pragma unroll
+          for (int m = 0; m < 4; m++) {
+            uint32_t rr[S];
+#pragma unroll
+            for (int d = 0; d < S; d++) rr[d] = r[d][4 * q + m];
+            v[m] = level_sum<S, PAIR>(rr);
+          }
+          aS[u].x = fma(v[0], sS, aS[u].x);
+          aS[u].y = fma(v[1], sS, aS[u].y);
+          aH[u].x = fma(v[2], sH, aH[u].x);
+          aH[u].y = fma(v[3], sH, aH[u].y);
+        }
+      }
+    }
+    // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
+    if (ok && jin) {
+      const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
+      const int k1 = P.kzz[3 * J], k2 = P.kzz[3 * J + 1], k3 = P.kzz[3 * J + 2];
+#pragma unroll
+      for (int u = 0; u < HALF; u++) {
+        const int I = i0 + hh * HALF + u;
+        if (I >= nv || J > I) continue;
+        const double x2 = xj * P.xk[I] + yj * P.yk[I] + zj * P.zk[I];
+        const int d1 = k1 - P.kzz[3 * I] + T.d1, d2 = k2 - P.kzz[3 * I + 1] + T.d2, d3 = k3 - P.kzz[3 * I + 2] + T.d3;
+        const size_t ci = ((size_t)d3 * ny + d2) * nx + d1;
+        const double2 th = tab[2 * ci], wp = tab[2 * ci + 1];
+        const double2 s = cadd(th, aS[u]);
+        const double2 h = cadd(cadd(cscale(th, x2), wp), aH[u]);
+        if (J == I) {
+          hs[(size_t)I * ld + I] = h;
+          hsdiag[I] = s;
+        } else {
+          hs[(size_t)I * ld + J] = s;  // S upper: HS(J,I)
+          hs[(size_t)J * ld + I] = h;  // H lower: HS(I,J)
+        }
+      }
+    }
+  }
+  // every MMA issued has completed before TMEM is freed
+  if (warp == 8) mbar_wait(&accbar, 0);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+}  // namespace sphtc

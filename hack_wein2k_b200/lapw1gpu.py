@@ -32,7 +32,7 @@ EXPORTS = [
     "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
-    "lapw1gpu_hns_noalloc",
+    "lapw1gpu_hns_noalloc", "lapw1gpu_forces",
 ]
 
 _lib = None
@@ -70,6 +70,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
                                             dp, dp, dp, ip, dp]
     lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p]
+    lib.lapw1gpu_forces.argtypes = [vp, vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 
@@ -99,6 +100,13 @@ class KPoint:
                                               C.c_void_p(d_hsdiag_ptr), C.byref(st) if st is not None else None)
         _check("lapw1gpu_kpoint_run", rc)
         return st.as_dict() if st is not None else None
+
+    def forces(self, d_c_ptr: int, ldc: int, nb: int, d_occ_ptr: int, d_eps_ptr: int, d_grad_ptr: int) -> None:
+        """dE/dPOS of E = sum occ*eps into the device array at d_grad_ptr
+        (ndf x 3 doubles); eigenvectors column-major n x nb on the device."""
+        rc = self.ctx.lib.lapw1gpu_forces(self.ctx.h, self.h, C.c_void_p(d_c_ptr), ldc, nb, C.c_void_p(d_occ_ptr),
+                                          C.c_void_p(d_eps_ptr), C.c_void_p(d_grad_ptr))
+        _check("lapw1gpu_forces", rc)
 
     def free(self):
         if self.h:

@@ -203,13 +203,17 @@ class Problem:
 
 
 def hermitian_from_packed(hs: np.ndarray, hsdiag: np.ndarray):
-    """Hermitian H and S as SECLR4 reads the packed state (seclr4.F:158-296):
-    it conjugates HS and HSDIAG, factors S from the upper triangle
-    (ZPOTRF 'U', the S diagonal swapped in from HSDIAG) and reduces H from
-    the lower triangle including the diagonal (ZHCGST / ZHEEVX2 'L')."""
+    """Hermitian H and S of the generalized problem H x = e S x that SECLR4
+    solves from the packed state (seclr4.F:158-296): it conjugates HS and
+    HSDIAG, reduces H from the lower triangle including the diagonal
+    (ZHCGST / ZHEEVX2 'L'), and factors the upper triangle with HSDIAG as
+    its diagonal (ZPOTRF 'U'), which ZHCGST takes as the Cholesky factor of
+    S**T (zhcgst.f:34-42).  So S(i,j) = conj(HS(j,i)) for i > j: S is the
+    transpose of the Hermitian matrix the upper triangle stores, and H and S
+    carry the same structure-factor phases."""
     hc = np.conj(hs)
     low = np.tril(hc, -1)
     H = low + low.conj().T + np.diag(np.diag(hc).real)
-    up = np.triu(hc, 1)
+    up = np.triu(hc, 1).T                      # S(i,j) = conj(HS(j,i)), i > j
     S = up + up.conj().T + np.diag(np.conj(hsdiag).real)
     return H, S

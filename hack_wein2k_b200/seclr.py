@@ -1,8 +1,8 @@
 """Generalized eigen-solve of the packed H,S on the GPU (SECLR4's role).
 
-SECLR4 (seclr4.F:158-345) conjugates HS/HSDIAG, factors S = U^H U from the
-upper triangle (ZPOTRF 'U'), reduces H from the lower triangle to the
-standard problem (ZHCGST), solves it (ZHEEVX2, energy window EL..EU) and
+SECLR4 (seclr4.F:158-345) conjugates HS/HSDIAG, factors the upper triangle
+(ZPOTRF 'U', which ZHCGST takes as the factor of S**T), reduces H from the
+lower triangle to the standard problem (ZHCGST), solves it (ZHEEVX2, energy window EL..EU) and
 back-transforms the eigenvectors (ZTRSM).  This module does the same on
 the device with the cuSOLVER routines torch.linalg exposes (Cholesky,
 triangular solves, Hermitian eigen-decomposition); it is the consumer of
@@ -19,11 +19,13 @@ def hermitian_from_packed_device(hs: torch.Tensor, hsdiag: torch.Tensor) -> Tupl
     """H and S (complex128, n x n, row-major torch layout of the math
     matrices) from the packed state on the device.  `hs` is the caller's
     column-major HS viewed as a torch tensor of shape [n(col)][n(row)]
-    complex (i.e. hs[c, r] = HS(r, c)); `hsdiag` is HSDIAG."""
-    n = hsdiag.shape[0]
+    complex (i.e. hs[c, r] = HS(r, c)); `hsdiag` is HSDIAG.  H comes from
+    the lower triangle; S is the transpose of the Hermitian matrix the upper
+    triangle stores (ZHCGST factors S**T, zhcgst.f:34-42), so
+    S(i,j) = conj(HS(j,i)) for i > j."""
     m = hs.transpose(0, 1).conj()              # m[r, c] = conj(HS(r, c))
     low = torch.tril(m, -1)
-    up = torch.triu(m, 1)
+    up = torch.triu(m, 1).transpose(0, 1)      # up[i, j] = conj(HS(j, i)), i > j
     H = low + low.conj().transpose(0, 1) + torch.diag(torch.diagonal(m).real.to(m.dtype))
     S = up + up.conj().transpose(0, 1) + torch.diag(hsdiag.conj().real.to(m.dtype))
     return H, S

@@ -233,6 +233,22 @@ int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx,
 int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs, int ldhs,
                          void* stream);
 
+/* Gradient of the band energy E = sum_b occ[b] eps[b] with respect to the
+ * atom positions POS (lattice coordinates), for the eigenpairs of the H, S
+ * that lapw1gpu_kpoint_run builds for kp (H c = eps S c as SECLR4 forms it).
+ * d_c: device, complex, column-major n x nb (ldc >= n), S-normalized
+ * eigenvectors; d_occ, d_eps: device, nb doubles each; d_grad: device,
+ * ndf x 3 doubles, overwritten with dE/dPOS (Ry per lattice unit; Cartesian
+ * forces follow as -(1/2pi) BKZZ dE/dPOS per atom).  Hellmann-Feynman for the
+ * fixed basis: radial functions, rotations and the warped potential held
+ * fixed.  No counterpart in lapw1 (it has no derivative code); the
+ * reference's forces are lapw2's (SRC_lapw2/fomai1.f, l2main.F:630-634) on
+ * another formulation.  Problems with HORB potentials (natorb > 0) return
+ * LAPW1GPU_ERR_ARG.  Synchronous. */
+int lapw1gpu_forces(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp,
+                    const double* d_c, int ldc, int nb, const double* d_occ,
+                    const double* d_eps, double* d_grad);
+
 /* version string of the library */
 const char* lapw1gpu_version(void);
 

@@ -1,0 +1,92 @@
+"""Band-energy gradients on the GPU (lapw1gpu_forces, the adjoint of the setup).
+
+lapw1 has no force code and the reference's forces (lapw2 fomai1.f) use a
+different formulation, so the adjoint is pinned by
+  * the Hellmann-Feynman sum over the ORACLE's dH/dPOS, dS/dPOS (central
+    differences of the oracle's matrices, exact to rounding): relative
+    tolerance 1e-8 of the largest component;
+  * central differences of E itself through the GPU setup and the device
+    eigen-solve (the torch.autograd path): 2e-6 of the largest component.
+"""
+import numpy as np
+import pytest
+import torch
+
+from hack_wein2k_b200 import forces as FO
+from hack_wein2k_b200 import lapw1gpu, synth
+from tests import force_ref as FR
+
+# "multilo" is left out: its seeded overlap is indefinite (no eigen-solve)
+KINDS = ["plain", "lo", "apw", "ins", "gamma"]
+TOL_HF = 1e-8
+TOL_FD = 2e-6
+
+
+def _occ(p, nb):
+    return torch.ones(nb, dtype=torch.float64)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", KINDS)
+def test_adjoint_matches_oracle_hellmann_feynman(ctx, kind):
+    p = synth.small_case(kind)
+    w, _ = FR.eigh(p)
+    nb, gap = FR.gapped_nb(w)
+    ref = FR.hf_gradient(p, nb)
+    dev = torch.device("cuda", ctx.device)
+    occ = _occ(p, nb).to(dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    g = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    kp.free()
+    assert np.abs(eps.cpu().numpy() - w[:nb]).max() <= 1e-9
+    scale = np.abs(ref).max()
+    assert np.abs(g - ref).max() <= TOL_HF * scale, (g, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["lo", "ins"])
+def test_autograd_matches_band_energy_fd(ctx, kind):
+    p = synth.small_case(kind)
+    w, _ = FR.eigh(p)
+    nb, _ = FR.gapped_nb(w)
+    occ = _occ(p, nb)
+    pos = torch.tensor(p.pos, dtype=torch.float64, requires_grad=True)
+    E = FO.BandEnergy.apply(pos, ctx, p, occ)
+    E.backward()
+    g = pos.grad.numpy()
+    scale = np.abs(g).max()
+    for a, c in [(0, 0), (1, 1), (2, 2)]:
+        fd = FO.finite_difference(ctx, p, occ, a, c)
+        assert abs(fd - g[a, c]) <= TOL_FD * scale, (a, c, fd, g[a, c])
+
+
+@pytest.mark.gpu
+def test_adjoint_on_the_40_atom_cell(ctx):
+    """The 40-atom ABO3 supercell (n = 4953): two components against FD of E."""
+    p = synth.config("c1")[0]
+    dev = torch.device("cuda", ctx.device)
+    E, eps, X, kp = FO.band_energy(ctx, p, torch.ones(p.n // 4, dtype=torch.float64, device=dev))
+    w = eps.cpu().numpy()
+    nb, gap = FR.gapped_nb(w, lo=8, hi=len(w) - 1)
+    kp.free()
+    occ = torch.ones(nb, dtype=torch.float64, device=dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    g = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    kp.free()
+    scale = np.abs(g).max()
+    assert scale > 0
+    for a, c in [(0, 0), (p.ndf - 1, 2)]:
+        fd = FO.finite_difference(ctx, p, occ.cpu(), a, c)
+        assert abs(fd - g[a, c]) <= TOL_FD * scale, (a, c, fd, g[a, c])
+
+
+@pytest.mark.gpu
+def test_horb_problems_are_rejected(ctx):
+    p = synth.small_case("orb")
+    dev = torch.device("cuda", ctx.device)
+    occ = torch.ones(4, dtype=torch.float64, device=dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    with pytest.raises(lapw1gpu.Lapw1GpuError) as ei:
+        FO.gradient(ctx, kp, X, occ, eps)
+    kp.free()
+    assert ei.value.code == 1
