@@ -8,6 +8,11 @@ GPU the workload is the 40-atom 2x2x2 ABO3 supercell (RKmax 7, ~4950 basis
 functions, one LO per atom for l<=2, one general k).  With N GPUs each rank
 sets up its own k-point of the same cell (k-points are independent: weak
 scaling, no collective on the data path).  Prints ONE JSON line (rank 0).
+The default arithmetic is the split-precision path (6 int8 slices; the
+plain FP64 GPU path on the same k-point is timed beside it in
+`fp64_path`, with the split path's per-matrix error against it), after the
+autotuner has picked the tile/schedule parameters (untimed).  `batch` is a
+captured graph of 16 c2 k-points per GPU.
 
 `value` is ms per k-point of the whole job with inputs resident in HBM
 (device timed, CUDA events on the library's stream, max over ranks).
@@ -192,15 +197,41 @@ def run_reference(args):
     return 0
 
 
+def _timed_loop(torch, stream, fn, steps):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _rel_err(torch, a, b, n):
+    """per-matrix max relative error of packed HS a against b ([col][row][2])"""
+    ca = torch.view_as_complex(a).transpose(0, 1)  # [row][col]
+    cb = torch.view_as_complex(b).transpose(0, 1)
+    low = torch.tril(torch.ones(n, n, dtype=torch.bool, device=a.device))
+    out = {}
+    for name, mask in (("H", low), ("S", ~low)):
+        d = ((ca - cb).abs() * mask).max().item()
+        m = ((cb.abs()) * mask).max().item()
+        out[name] = d / m if m > 0 else 0.0
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--prec", choices=["fp64", "split"], default="fp64")
+    ap.add_argument("--prec", choices=["fp64", "split"], default="split")
     ap.add_argument("--slices", type=int, default=6)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -234,6 +265,7 @@ def main():
     d_hs = torch.empty((n, n, 2), dtype=torch.float64, device=device)  # column-major view: [col][row]
     d_hd = torch.empty((n, 2), dtype=torch.float64, device=device)
     torch.cuda.synchronize()
+    tuning = ctx.autotune(kp, d_hs.data_ptr(), n, d_hd.data_ptr())  # untimed: picks tile/schedule parameters
 
     def step(stats=True):
         return kp.run(d_hs.data_ptr(), n, d_hd.data_ptr(), stages=7, stats=stats)
@@ -244,18 +276,10 @@ def main():
     if dist is not None:
         dist.barrier()
     with ClockSampler(local) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            step(stats=False)  # queued on the library's stream, no host sync between k-points
-        e1.record(stream)
-        torch.cuda.synchronize()
+        # queued on the library's stream, no host sync between k-points
+        ms = _timed_loop(torch, stream, lambda: step(stats=False), args.steps)
     if dist is not None:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
         t = torch.tensor([ms], device=device, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
@@ -282,16 +306,8 @@ def main():
         ctx.setup(p, hs=hs_np, hsdiag=hd_np)
     if dist is not None:
         dist.barrier()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    f0.record(stream)
     e2e_steps = max(1, min(args.steps, 5))
-    for _ in range(e2e_steps):
-        ctx.setup(p, hs=hs_np, hsdiag=hd_np)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
+    e2e_ms = _timed_loop(torch, stream, lambda: ctx.setup(p, hs=hs_np, hsdiag=hd_np), e2e_steps)
     if dist is not None:
         t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -300,25 +316,84 @@ def main():
     h2d = problem_input_bytes(p)
     d2h = n * n * 16 + n * 16
 
+    # ---- the plain FP64 GPU path on the same k-point, and the split error ----
+    fp64_cmp = None
+    if args.prec == "split" and not args.no_extras:
+        cf = lapw1gpu.Context(local, prec=lapw1gpu.PREC_FP64)
+        sf = torch.cuda.ExternalStream(cf.stream_handle, device=device)
+        kf = cf.upload(p)
+        f_hs = torch.empty_like(d_hs)
+        f_hd = torch.empty_like(d_hd)
+        tf = cf.autotune(kf, f_hs.data_ptr(), n, f_hd.data_ptr())
+        for _ in range(2):
+            kf.run(f_hs.data_ptr(), n, f_hd.data_ptr(), stats=True)
+        nf = max(3, min(args.steps, 20))
+        ms_f = _timed_loop(torch, sf, lambda: kf.run(f_hs.data_ptr(), n, f_hd.data_ptr(), stats=False), nf) / nf
+        stf = kf.run(f_hs.data_ptr(), n, f_hd.data_ptr(), stats=True)
+        step(stats=True)
+        err = _rel_err(torch, d_hs, f_hs, n)
+        fp64_cmp = {"ms_per_kpoint": ms_f, "speedup_split_over_fp64": ms_f / ms_step,
+                    "stage_ms": {k: v for k, v in stf.items() if k.startswith("ms_")},
+                    "split_rel_error_vs_fp64": err, "tuning": tf}
+        kf.free()
+        cf.close()
+        del f_hs, f_hd
+
+    # ---- one captured batch of c2 k-points (uneven N) per rank ----
+    batch = None
+    if not args.no_extras:
+        nkb = 16
+        probs = synth.config("c2", nk=nkb * world)[rank::world][:nkb]
+        kps = [ctx.upload(q) for q in probs]
+        bh = [torch.empty((q.n, q.n, 2), dtype=torch.float64, device=device) for q in probs]
+        bd = [torch.empty((q.n, 2), dtype=torch.float64, device=device) for q in probs]
+        args_b = (kps, [t.data_ptr() for t in bh], [q.n for q in probs], [t.data_ptr() for t in bd])
+        best = None
+        for sets in (1, 2, 3):  # the batch schedule is tuned too: concurrent k-point chains
+            ctx.set_tuning(batch_sets=sets)
+            ctx.setup_batch(*args_b)  # capture
+            t_b = min(ctx.setup_batch(*args_b)["ms_total"] for _ in range(2))
+            if best is None or t_b < best[1]:
+                best = (sets, t_b)
+        ctx.set_tuning(batch_sets=best[0])
+        reps = 3
+        ms_b = min(ctx.setup_batch(*args_b)["ms_total"] for _ in range(reps))
+        if dist is not None:
+            t = torch.tensor([ms_b], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_b = float(t.item())
+        batch = {"workload": f"c2: {nkb} seeded wedge k-points per GPU of the 40-atom cell, N {min(q.n for q in probs)}"
+                             f"..{max(q.n for q in probs)}, one CUDA graph launch",
+                 "ms_per_batch": ms_b, "ms_per_kpoint": ms_b / nkb / 1.0, "kpoints_per_s": nkb * world / (ms_b * 1e-3),
+                 "batch_sets": best[0]}
+        for k in kps:
+            k.free()
+        del bh, bd
+
     # ---- roofline of the dominant kernel ----
     clocks = clk.summary()
     avg = {k: v / n_stage for k, v in stage_ms.items()}
     nsl2 = (p.lnsmax + 1) ** 2
     pairs = p.nv * (p.nv + 1) / 2.0
-    # k_spherical: per pair, 6 FMA per (atom type, l), 4 per equivalent
-    # atom's phase product, 4 per type to add PHASE * t into S and H
+    # spherical: per pair, 6 FMA per (atom type, l), 4 per equivalent atom's
+    # phase product, 4 per type to add PHASE * t into S and H
     f_sph = 2.0 * (6.0 * p.ltop * p.nat + 4.0 * p.ndf + 4.0 * p.nat) * pairs
     # HNS: complex rank-K update of the lower triangle, K = 2 NDF (lmax_ns+1)^2
     f_hns = 8.0 * (2.0 * p.ndf * nsl2) * (n * (n + 1) / 2.0)
-    kern = {"k_spherical (K-b)": (f_sph, avg["ms_spherical"]), "HNS update (K-ns)": (f_hns, avg["ms_hns"])}
+    split = args.prec == "split"
+    sph_name = "k_sph_tc spherical (K-b)" if split and tuning.get("sph_tc", 0) and 4 <= args.slices <= 7 \
+        else "k_spherical (K-b)"
+    kern = {sph_name: (f_sph, avg["ms_spherical"]), "HNS update (K-ns)": (f_hns, avg["ms_hns"])}
     dom = max(kern, key=lambda k: kern[k][1])
     fl, t_ms = kern[dom]
     fp64_peak = fp64_peak_tflops(torch, device)
-    if dom.startswith("HNS") and args.prec == "split":
+    on_tensor = split and (dom.startswith("HNS") or dom.startswith("k_sph_tc"))
+    if on_tensor:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
         bound, peak = "tensor", 2.0 * peaks.get("bf16_tflops", 1590.0)
-        peak_src = "2 x measured dense bf16 (the int8 tcgen05 rate), MEASURED_PEAKS.json; achieved in FP64-equivalent flops"
+        peak_src = ("2 x measured dense bf16 (the int8 tcgen05 rate), MEASURED_PEAKS.json; achieved counts "
+                    "FP64-equivalent flops, so frac understates the int8 slice-product rate by the products per MAC")
     else:
         bound, peak = "fp64", fp64_peak
         peak_src = ("measured here: cuBLAS DGEMM 8192^3, best of 5 (MEASURED_PEAKS.json has no FP64 figure); "
@@ -338,15 +413,17 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.prec == "fp64" else "int8-slices(f64 accum)",
+        "vs_baseline": None, "dtype": "f64" if args.prec == "fp64" else f"int8 x{args.slices} slices, f64 combine",
         "data": "synthetic (seeded)",
         "config": {"workload": workload, "n": n, "nv": p.nv, "nlo": p.nlo, "atoms": p.ndf, "lmax": p.ltop - 1,
-                   "lmax_ns": p.lnsmax, "precision": args.prec, "parallelism": f"k-shard x{world}",
+                   "lmax_ns": p.lnsmax, "precision": args.prec, "slices": args.slices if split else None,
+                   "parallelism": f"k-shard x{world}",
                    "l2": "HS output 0.39 GB and HNS operands 0.32 GB per k-point exceed the 126 MB L2"},
         "kpoints_per_s": 1e3 / value,
         "fp64_equiv_tflops": (f_sph + f_hns) / (ms_step * 1e-3) / 1e12,
         "fp64_equiv_tflops_baseline_def": baseline_def_flops(p) / (ms_step * 1e-3) / 1e12,
         "stage_ms": {k: v for k, v in avg.items() if k.startswith("ms_")},
+        "tuning": tuning,
         "roofline": {"kernel": dom, "bound": bound,
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
@@ -358,6 +435,10 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if fp64_cmp is not None:
+        line["fp64_path"] = fp64_cmp
+    if batch is not None:
+        line["batch"] = batch
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:

@@ -33,25 +33,57 @@ struct DevBuf {
 
 }  // namespace
 
+#define L1G_MAX_SETS 4  // concurrent k-point chains in a batch (scratch sets)
+
 struct lapw1gpu_context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side[L1G_MAX_SETS] = {};  // streams of scratch sets 1.. in a batch
   cudaEvent_t ev[12] = {};
+  cudaEvent_t fork = nullptr, join[L1G_MAX_SETS] = {};
   int* d_status = nullptr;
   int last_status = 0;
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 6;
-  bool sph_attr = false;
-  cublasHandle_t blas = nullptr;  // library ZGEMM of the FP64 HNS panels
+  cublasHandle_t blas[L1G_MAX_SETS] = {};  // library ZGEMMs, one handle (and workspace) per scratch set
+  // tunables (lapw1gpu_autotune)
+  int hns_diag_b = 512;    // FP64 HNS: diagonal block of the blocked ZHER2M form
+  int split_group = 16;    // split HNS: row tiles per rasterisation group
+  int sph_tc = 1;          // split precision: spherical part on tcgen05 (1) or FP64 (0)
+  int batch_sets = 2;      // concurrent k-point chains in a batch
   std::map<std::string, DevBuf> bufs;
-  std::map<std::string, std::pair<long, int>> tile_keys;  // tile lists already on the device: shape, count
+  std::map<std::string, std::pair<int2*, int>> tiles;  // tile lists per shape (kp_tiles)
+  struct Graph {
+    std::vector<uintptr_t> key;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+  };
+  std::vector<Graph> graphs;  // captured batches
+  std::map<const void*, int> smem_attr;  // kernels whose dynamic shared memory limit is raised
+
+  // raise a kernel's dynamic shared-memory limit once per context (not a
+  // stream operation, and kept out of captured sequences)
+  bool smem(const void* fn, int bytes) {
+    auto it = smem_attr.find(fn);
+    if (it != smem_attr.end() && it->second >= bytes) return true;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    smem_attr[fn] = bytes;
+    return true;
+  }
 
   // grow-only scratch buffer; returns nullptr on allocation failure
-  void* buf(const char* name, size_t bytes) {
+  void* buf(const std::string& name, size_t bytes) {
     DevBuf& b = bufs[name];
     if (bytes == 0) bytes = 16;
     if (b.bytes < bytes) {
-      if (b.ptr) cudaFree(b.ptr);
+      if (b.ptr) {
+        cudaDeviceSynchronize();  // a captured batch or a queued run may still use it
+        cudaFree(b.ptr);
+        drop_graphs();
+      }
       b.ptr = nullptr;
       b.bytes = 0;
       if (cudaMalloc(&b.ptr, bytes) != cudaSuccess) {
@@ -61,6 +93,20 @@ struct lapw1gpu_context {
       b.bytes = bytes;
     }
     return b.ptr;
+  }
+  // scratch of one set: buffers of concurrent k-point chains never alias
+  void* sbuf(int set, const char* name, size_t bytes) {
+    return set == 0 ? buf(name, bytes) : buf(std::string(name) + "#" + std::to_string(set), bytes);
+  }
+  cublasHandle_t handle(int set, cudaStream_t s) {
+    if (!blas[set] && cublasCreate(&blas[set]) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    if (cublasSetStream(blas[set], s) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    return blas[set];
+  }
+  void drop_graphs() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
   }
 };
 
@@ -94,6 +140,34 @@ struct lapw1gpu_kpoint {
   const LoRange* d_loranges = nullptr;
   const double2* d_pots = nullptr;
 };
+
+// Device tile list for the shape named by `key` (sizes and tile parameters),
+// built by `make` on first use and kept by the context: lists depend on the
+// shape only, so k-points of equal shape share them and a list, once built,
+// never changes under a queued run or a captured batch.
+template <class F>
+static const int2* kp_tiles(lapw1gpu_kpoint* k, const std::string& key, int* count, F make) {
+  auto& tiles = k->ctx->tiles;
+  auto it = tiles.find(key);
+  if (it != tiles.end()) {
+    *count = it->second.second;
+    return it->second.first;
+  }
+  std::vector<int2> t;
+  make(t);
+  int2* d = nullptr;
+  if (t.empty() || cudaMalloc(&d, sizeof(int2) * t.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (cudaMemcpy(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  tiles[key] = std::make_pair(d, (int)t.size());
+  *count = (int)t.size();
+  return d;
+}
 
 namespace {
 
@@ -173,6 +247,11 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
     return LAPW1GPU_ERR_CUDA;
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+  for (int i = 1; i < L1G_MAX_SETS; i++) {
+    cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming);
+  }
   if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     delete c;
@@ -186,12 +265,20 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
 int lapw1gpu_finalize(lapw1gpu_context* c) {
   if (!c) return LAPW1GPU_ERR_ARG;
   cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
-  if (c->blas) cublasDestroy(c->blas);
+  cudaDeviceSynchronize();
+  c->drop_graphs();
+  for (auto& h : c->blas)
+    if (h) cublasDestroy(h);
   for (auto& kv : c->bufs)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
+  for (auto& kv : c->tiles) cudaFree(kv.second.first);
   if (c->d_status) cudaFree(c->d_status);
   for (auto& e : c->ev) cudaEventDestroy(e);
+  cudaEventDestroy(c->fork);
+  for (int i = 1; i < L1G_MAX_SETS; i++) {
+    cudaEventDestroy(c->join[i]);
+    cudaStreamDestroy(c->side[i]);
+  }
   cudaStreamDestroy(c->stream);
   delete c;
   return LAPW1GPU_OK;
@@ -453,43 +540,43 @@ int lapw1gpu_kpoint_upload(lapw1gpu_context* ctx, const lapw1gpu_problem* p, lap
 
 int lapw1gpu_kpoint_free(lapw1gpu_kpoint* k) {
   if (!k) return LAPW1GPU_ERR_ARG;
+  cudaSetDevice(k->ctx->device);
   if (k->arena && k->owns_arena) {
-    cudaSetDevice(k->ctx->device);
-    cudaStreamSynchronize(k->ctx->stream);
+    cudaDeviceSynchronize();
     cudaFree(k->arena);
+  }
+  // captured batches that name this k-point are stale
+  lapw1gpu_context* c = k->ctx;
+  for (auto it = c->graphs.begin(); it != c->graphs.end();) {
+    if (std::find(it->key.begin(), it->key.end(), (uintptr_t)k) != it->key.end()) {
+      cudaGraphExecDestroy(it->exec);
+      it = c->graphs.erase(it);
+    } else {
+      ++it;
+    }
   }
   delete k;
   return LAPW1GPU_OK;
 }
 
-// tile lists (device) for the triangle kernels, cached per shape in the context
-static const int2* tiles_tri(lapw1gpu_context* c, const char* name, int n, int T, int* count) {
-  const long key = (long)n * 4096 + T;
-  auto it = c->tile_keys.find(name);
-  if (it != c->tile_keys.end() && it->second.first == key) {  // uploaded by an earlier run
-    *count = it->second.second;
-    return (const int2*)c->bufs[name].ptr;
-  }
-  int nb = (n + T - 1) / T;
-  std::vector<int2> t;
-  for (int bi = 0; bi < nb; bi++)
-    for (int bj = 0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
-  *count = (int)t.size();
-  c->tile_keys.erase(name);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;  // earlier runs may still read it
-  int2* d = (int2*)c->buf(name, sizeof(int2) * t.size());
-  if (!d) return nullptr;
-  if (cudaMemcpy(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-  c->tile_keys[name] = std::make_pair(key, *count);
-  return d;
+// tile list of the lower triangle in T x T tiles, rows outer (a prefix of
+// the list for a larger n covers a smaller one)
+static const int2* tiles_tri(lapw1gpu_kpoint* k, const char* name, int n, int T, int* count) {
+  return kp_tiles(k, std::string(name) + ":" + std::to_string(n) + ":" + std::to_string(T), count,
+                  [&](std::vector<int2>& t) {
+                    const int nb = (n + T - 1) / T;
+                    for (int bi = 0; bi < nb; bi++)
+                      for (int bj = 0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
+                  });
 }
 
 // HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom, LO-row terms
-static int launch_hns_ops(const DevProb& P, const double2* tns, const LoRange* lor, int nlor, double2* Lop,
-                          double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl) {
+static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* tns, const LoRange* lor, int nlor,
+                          double2* Lop, double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl) {
   const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
   k_hns_alm<<<dim3((P.npad + 127) / 128, P.ndf), 128, 0, s>>>(P, lor, nlor, Rop, Clo);
-  if (cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
+  if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
+        : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
     return LAPW1GPU_ERR_CUDA;
   k_hns_tmul<<<dim3(P.npad / TMUL_I, P.ndf), 256, TMUL_SMEM, s>>>(P.npad, nsl2, P.atype, tns, Rop, Lop);
   *nl += 2;
@@ -500,47 +587,30 @@ static int launch_hns_ops(const DevProb& P, const double2* tns, const LoRange* l
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
-// Block width of the FP64 HNS update: diagonal blocks of HNS_DIAG_B rows run
-// in k_hns_gemm (64-row tiles, lower triangle only), the rows below each
-// diagonal block in one library ZGEMM per block column, as zher2m.f:69-80
-// splits its update (ZGEMV on the diagonal block, ZGEMM below).
-#define HNS_DIAG_B 512
-
-static const int2* tiles_hns_diag(lapw1gpu_context* c, int n, int* count) {
-  auto it = c->tile_keys.find("tiles_hns_diag");
-  if (it != c->tile_keys.end() && it->second.first == n) {
-    *count = it->second.second;
-    return (const int2*)c->bufs["tiles_hns_diag"].ptr;
-  }
-  std::vector<int2> t;
-  const int per = HNS_DIAG_B / HNS_T;
-  const int nt = (n + HNS_T - 1) / HNS_T;
-  for (int b0 = 0; b0 < nt; b0 += per)
-    for (int bi = b0; bi < std::min(nt, b0 + per); bi++)
-      for (int bj = b0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
-  *count = (int)t.size();
-  c->tile_keys.erase("tiles_hns_diag");
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;  // earlier runs may still read it
-  int2* d = (int2*)c->buf("tiles_hns_diag", sizeof(int2) * t.size());
-  if (!d) return nullptr;
-  if (cudaMemcpy(d, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-  c->tile_keys["tiles_hns_diag"] = std::make_pair((long)n, *count);
-  return d;
+// The FP64 HNS update in the blocked form of ZHER2M (zher2m.f:69-80):
+// diagonal blocks of B rows run in k_hns_gemm (64-row tiles, lower triangle
+// only), the rows below each diagonal block in one library ZGEMM per block
+// column.  B is a tunable (lapw1gpu_autotune), 512 by default.
+static const int2* tiles_hns_diag(lapw1gpu_kpoint* k, int n, int B, int* count) {
+  return kp_tiles(k, "hnsdiag:" + std::to_string(n) + ":" + std::to_string(B), count, [&](std::vector<int2>& t) {
+    const int per = B / HNS_T;
+    const int nt = (n + HNS_T - 1) / HNS_T;
+    for (int b0 = 0; b0 < nt; b0 += per)
+      for (int bi = b0; bi < std::min(nt, b0 + per); bi++)
+        for (int bj = b0; bj <= bi; bj++) t.push_back(make_int2(bi, bj));
+  });
 }
 
-static int hns_panels_zgemm(lapw1gpu_context* c, int n, int npad, int K, const double2* Lop, const double2* Rop,
-                            double2* hs, int ld, cudaStream_t s) {
-  if (!c->blas) {
-    if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
-  }
-  if (cublasSetStream(c->blas, s) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+static int hns_panels_zgemm(cublasHandle_t h, int n, int npad, int K, int B, const double2* Lop, const double2* Rop,
+                            double2* hs, int ld) {
+  if (!h) return LAPW1GPU_ERR_CUDA;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  for (int c0 = 0; c0 < n; c0 += HNS_DIAG_B) {
-    const int w = std::min(HNS_DIAG_B, n - c0);
+  for (int c0 = 0; c0 < n; c0 += B) {
+    const int w = std::min(B, n - c0);
     const int r0 = c0 + w, m = n - r0;
     if (m <= 0) continue;
     // HS(r0:n, c0:c0+w) += L(r0:n, :) R(c0:c0+w, :)^T ; L, R column-major npad x K
-    if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, w, K, &one, (const cuDoubleComplex*)(Lop + r0), npad,
+    if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, m, w, K, &one, (const cuDoubleComplex*)(Lop + r0), npad,
                     (const cuDoubleComplex*)(Rop + c0), npad, &one, (cuDoubleComplex*)(hs + (size_t)c0 * ld + r0),
                     ld) != CUBLAS_STATUS_SUCCESS)
       return LAPW1GPU_ERR_CUDA;
@@ -553,52 +623,39 @@ static int hns_panels_zgemm(lapw1gpu_context* c, int n, int npad, int K, const d
 // Spherical part on tcgen05 (sph_tc.cuh): slice the per-l operands, then
 // one CTA per (128 J, IT I) tile of the triangle.
 template <int S, bool PAIR>
-static int sph_tc_launch(lapw1gpu_context* c, const lapw1gpu_kpoint* k, const DevProb& P, const SphCoef* coef,
+static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
                          const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
   using Cf = sphtc::Cfg<S>;
   const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
   const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;
   const int npA = round_up(nv, 128), npB = round_up(nv, Cf::IT);
-  int8_t* A = (int8_t*)c->buf("sphA", (size_t)S * L * npA * Kp);
-  int8_t* B = (int8_t*)c->buf("sphB", (size_t)S * L * 4 * npB * Kp);
-  int* exA = (int*)c->buf("sphExA", sizeof(int) * (size_t)L * npA);
-  int* exB = (int*)c->buf("sphExB", sizeof(int) * (size_t)L * 2 * npB);
+  int8_t* A = (int8_t*)c->sbuf(set, "sphA", (size_t)S * L * npA * Kp);
+  int8_t* B = (int8_t*)c->sbuf(set, "sphB", (size_t)S * L * 4 * npB * Kp);
+  int* exA = (int*)c->sbuf(set, "sphExA", sizeof(int) * (size_t)L * npA);
+  int* exB = (int*)c->sbuf(set, "sphExB", sizeof(int) * (size_t)L * 2 * npB);
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
   const int sl_smem = Kc * 33 * (int)sizeof(double2);
   if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
-  if (cudaFuncSetAttribute(sphtc::k_sph_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, sl_smem) != cudaSuccess)
-    return LAPW1GPU_ERR_CUDA;
+  if (!c->smem((const void*)sphtc::k_sph_slice, sl_smem)) return LAPW1GPU_ERR_CUDA;
   sphtc::k_sph_slice<<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, S, A, exA);
   sphtc::k_sph_slice<<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, S, B, exB);
   *nl += 2;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128) || l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;
-  const long key = (long)nv * 1024 + Cf::IT;
   int ntile = 0;
-  int2* dt = nullptr;
-  auto it = c->tile_keys.find("tiles_sphtc");
-  if (it != c->tile_keys.end() && it->second.first == key) {
-    ntile = it->second.second;
-    dt = (int2*)c->bufs["tiles_sphtc"].ptr;
-  } else {
-    std::vector<int2> t;
-    const int nbj = npA / 128, nbi = npB / Cf::IT;
-    for (int bj = 0; bj < nbj; bj++)
-      for (int bi = 0; bi < nbi; bi++)
-        if (bj * 128 <= bi * Cf::IT + Cf::IT - 1) t.push_back(make_int2(bj, bi));
-    c->tile_keys.erase("tiles_sphtc");
-    if (cudaStreamSynchronize(s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;  // earlier runs may still read it
-    dt = (int2*)c->buf("tiles_sphtc", sizeof(int2) * t.size());
-    if (!dt) return LAPW1GPU_ERR_NOMEM;
-    if (cudaMemcpy(dt, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-      return LAPW1GPU_ERR_CUDA;
-    ntile = (int)t.size();
-    c->tile_keys["tiles_sphtc"] = std::make_pair(key, ntile);
-  }
-  if (cudaFuncSetAttribute(sphtc::k_sph_tc<S, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM) !=
-      cudaSuccess)
-    return LAPW1GPU_ERR_CUDA;
+  // I tiles outer: the CTAs resident at one time share few I tiles (B
+  // operand, streamed from DRAM once) and sweep the J tiles (A operand,
+  // 11 l x NV rows x S slices ~ 50 MB at NV = 4600, L2-resident)
+  const int2* dt = kp_tiles(k, "sphtc:" + std::to_string(nv) + ":" + std::to_string(Cf::IT), &ntile,
+                            [&](std::vector<int2>& t) {
+                              const int nbj = npA / 128, nbi = npB / Cf::IT;
+                              for (int bi = 0; bi < nbi; bi++)
+                                for (int bj = 0; bj < nbj; bj++)
+                                  if (bj * 128 <= bi * Cf::IT + Cf::IT - 1) t.push_back(make_int2(bj, bi));
+                            });
+  if (!dt) return LAPW1GPU_ERR_NOMEM;
+  if (!c->smem((const void*)sphtc::k_sph_tc<S, PAIR>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
   sphtc::k_sph_tc<S, PAIR><<<ntile, Cf::THREADS, Cf::SMEM, s>>>(ta, tb, P, dt, Kp / 64, npA, npB, exA, exB, tab,
                                                                 k->tab, hs, ld, hsdiag, c->d_status);
   *nl += 1;
@@ -614,16 +671,16 @@ static bool sph_pair_ok(int S, int Kp) {
 }
 
 // true when the split-precision spherical path handles this slice count
-static bool sph_tc_supported(int S) { return false && S >= 4 && S <= 7; }
+static bool sph_tc_supported(int S) { return S >= 4 && S <= 7; }
 
-static int sph_tc_dispatch(lapw1gpu_context* c, const lapw1gpu_kpoint* k, const DevProb& P, const SphCoef* coef,
+static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
                            const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
   const int Kp = 2 * round_up(2 * k->ndf, 32);
   const bool pair = sph_pair_ok(c->slices, Kp);
-#define SPH_CASE(SS)                                                                   \
-  case SS:                                                                             \
-    return pair ? sph_tc_launch<SS, true>(c, k, P, coef, tab, hs, ld, hsdiag, s, nl)   \
-                : sph_tc_launch<SS, false>(c, k, P, coef, tab, hs, ld, hsdiag, s, nl);
+#define SPH_CASE(SS)                                                                        \
+  case SS:                                                                                  \
+    return pair ? sph_tc_launch<SS, true>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl)   \
+                : sph_tc_launch<SS, false>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl);
   switch (c->slices) {
     SPH_CASE(4)
     SPH_CASE(5)
@@ -634,8 +691,6 @@ static int sph_tc_dispatch(lapw1gpu_context* c, const lapw1gpu_kpoint* k, const 
   }
 #undef SPH_CASE
 }
-
-extern "C" {
 
 // algorithmic FP64-equivalent flops of the contractions (see DESIGN.md roofline)
 static double alg_flops(const lapw1gpu_kpoint* k) {
@@ -648,21 +703,19 @@ static double alg_flops(const lapw1gpu_kpoint* k) {
   return sph + hns;
 }
 
-int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, double* d_hs_, int ldhs,
-                        double* d_hsdiag_, lapw1gpu_stats* st) {
-  if (!c || !k || !d_hs_ || !d_hsdiag_ || ldhs < k->n || k->ctx != c) return LAPW1GPU_ERR_ARG;
-  CK(cudaSetDevice(c->device));
-  double2* d_hs = reinterpret_cast<double2*>(d_hs_);
-  double2* d_hsdiag = reinterpret_cast<double2*>(d_hsdiag_);
-  cudaStream_t s = c->stream;
+// The stage sequence of one k-point on stream s with scratch set `set`.
+// ev: events to record between stages (null in a batch).  Host-side work
+// is limited to launches: every buffer and tile list already exists when
+// the same k-point ran once before, so the sequence can be captured.
+static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, double2* d_hs, int ldhs,
+                           double2* d_hsdiag, cudaStream_t s, int set, const cudaEvent_t* ev, int* nlaunch) {
   DevProb P = k->P;
   const int n = k->n, nv = k->nv, ltop = k->ltop, ndf = k->ndf, nat = k->nat;
-  P.al = (double*)c->buf("al", sizeof(double) * (size_t)nat * ltop * k->nvpad);
-  P.bl = (double*)c->buf("bl", sizeof(double) * (size_t)nat * ltop * k->nvpad);
-  P.phase = (double2*)c->buf("phase", sizeof(double2) * (size_t)ndf * k->npad);
+  P.al = (double*)c->sbuf(set, "al", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.bl = (double*)c->sbuf(set, "bl", sizeof(double) * (size_t)nat * ltop * k->nvpad);
+  P.phase = (double2*)c->sbuf(set, "phase", sizeof(double2) * (size_t)ndf * k->npad);
   if (!P.al || !P.bl || !P.phase) return LAPW1GPU_ERR_NOMEM;
-  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
-  if (st) CK(cudaEventRecord(c->ev[0], s));
+  if (ev) CK(cudaEventRecord(ev[0], s));
   int nl = 0;  // kernels launched by this run
 
   // ---- K-a: matching coefficients and phases (always needed) ----
@@ -671,67 +724,64 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
   nl++;
   k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
   CK(cudaGetLastError());
-  if (st) CK(cudaEventRecord(c->ev[1], s));
+  if (ev) CK(cudaEventRecord(ev[1], s));
 
   if (stages & 1) {
     // ---- K-c table + K-b spherical ----
     size_t ntab = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
-    double2* tab = (double2*)c->buf("tab", sizeof(double2) * 2 * ntab);
-    SphCoef* coef = (SphCoef*)c->buf("coef", sizeof(SphCoef) * nat * ltop);
+    double2* tab = (double2*)c->sbuf(set, "tab", sizeof(double2) * 2 * ntab);
+    SphCoef* coef = (SphCoef*)c->sbuf(set, "coef", sizeof(SphCoef) * nat * ltop);
     if (!tab || !coef) return LAPW1GPU_ERR_NOMEM;
     nl++;
     k_table<<<(unsigned)((ntab + 127) / 128), 128, 0, s>>>(P, k->tab, k->d_warp, tab);
     nl++;
     k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
-    int ntiles = 0;
-    const int2* tl = tiles_tri(c, "tiles_sph", nv, SPH_T, &ntiles);
-    if (!tl) return LAPW1GPU_ERR_NOMEM;
-    if (c->prec == LAPW1GPU_PREC_SPLIT && sph_tc_supported(c->slices)) {
-      int rc = sph_tc_dispatch(c, k, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl);
+    if (c->prec == LAPW1GPU_PREC_SPLIT && c->sph_tc && sph_tc_supported(c->slices)) {
+      int rc = sph_tc_dispatch(c, k, set, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl);
       if (rc) return rc;
     } else {
-      if (!c->sph_attr) {  // function attributes are per device: once per context
-        CK(cudaFuncSetAttribute(k_spherical, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
-        c->sph_attr = true;
-      }
+      int ntiles = 0;
+      const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
+      if (!tl) return LAPW1GPU_ERR_NOMEM;
+      if (!c->smem((const void*)k_spherical, SPH_DYN_SMEM)) return LAPW1GPU_ERR_CUDA;
       nl++;
       k_spherical<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, tab, k->tab, d_hs, ldhs, d_hsdiag);
     }
     CK(cudaGetLastError());
-    if (st) CK(cudaEventRecord(c->ev[2], s));
+    if (ev) CK(cudaEventRecord(ev[2], s));
     // ---- K-b': local-orbital columns ----
-    if (k->nlo > 0) nl++;
-    if (k->nlo > 0) k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag);
+    if (k->nlo > 0) {
+      nl++;
+      k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag);
+    }
     CK(cudaGetLastError());
-    if (st) CK(cudaEventRecord(c->ev[3], s));
-  } else if (st) {
-    CK(cudaEventRecord(c->ev[2], s));
-    CK(cudaEventRecord(c->ev[3], s));
+    if (ev) CK(cudaEventRecord(ev[3], s));
+  } else if (ev) {
+    CK(cudaEventRecord(ev[2], s));
+    CK(cudaEventRecord(ev[3], s));
   }
 
   if ((stages & 2) && !k->nohns) {
     // ---- K-ns ----
     const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
     const int K = ndf * 2 * nsl2;
-    double2* Lop = (double2*)c->buf("hnsL", sizeof(double2) * (size_t)K * k->npad);
-    double2* Rop = (double2*)c->buf("hnsR", sizeof(double2) * (size_t)K * k->npad);
+    double2* Lop = (double2*)c->sbuf(set, "hnsL", sizeof(double2) * (size_t)K * k->npad);
+    double2* Rop = (double2*)c->sbuf(set, "hnsR", sizeof(double2) * (size_t)K * k->npad);
     size_t nloc = (size_t)ndf * nsl2 * std::max(1, k->nlo);
-    double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
-    double2* C2lo = (double2*)c->buf("hnsC2lo", sizeof(double2) * nloc);
+    double2* Clo = (double2*)c->sbuf(set, "hnsClo", sizeof(double2) * nloc);
+    double2* C2lo = (double2*)c->sbuf(set, "hnsC2lo", sizeof(double2) * nloc);
     if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
-    int rc = launch_hns_ops(P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
     if (rc) return rc;
     if (c->prec == LAPW1GPU_PREC_SPLIT)
-      rc = split_hns_gemm(c, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices, s, &nl);
+      rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices, s, &nl);
     else {
-      // the blocked form of ZHER2M (zher2m.f:69-80): diagonal blocks of the
-      // lower triangle by k_hns_gemm, the panels below them by ZGEMM
       int ntiles = 0;
-      const int2* tl = tiles_hns_diag(c, n, &ntiles);
+      const int2* tl = tiles_hns_diag(k, n, c->hns_diag_b, &ntiles);
       if (!tl) return LAPW1GPU_ERR_NOMEM;
       nl++;
       k_hns_gemm<<<ntiles, 256, 0, s>>>(n, k->npad, K, tl, Lop, Rop, d_hs, ldhs);
-      rc = hns_panels_zgemm(c, n, k->npad, K, Lop, Rop, d_hs, ldhs, s);
+      rc = hns_panels_zgemm(c->handle(set, s), n, k->npad, K, c->hns_diag_b, Lop, Rop, d_hs, ldhs);
     }
     if (rc) return rc;
     if (k->nlo > 0) {
@@ -740,12 +790,12 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     }
     CK(cudaGetLastError());
   }
-  if (st) CK(cudaEventRecord(c->ev[4], s));
+  if (ev) CK(cudaEventRecord(ev[4], s));
 
   if ((stages & 4) && !k->orbs.empty()) {
-    double2* alm = (double2*)c->buf("orb_alm", sizeof(double2) * 7 * (size_t)n);
-    double2* blm = (double2*)c->buf("orb_blm", sizeof(double2) * 7 * (size_t)n);
-    double2* clm = (double2*)c->buf("orb_clm", sizeof(double2) * 7 * (size_t)n);
+    double2* alm = (double2*)c->sbuf(set, "orb_alm", sizeof(double2) * 7 * (size_t)n);
+    double2* blm = (double2*)c->sbuf(set, "orb_blm", sizeof(double2) * 7 * (size_t)n);
+    double2* clm = (double2*)c->sbuf(set, "orb_clm", sizeof(double2) * 7 * (size_t)n);
     if (!alm || !blm || !clm) return LAPW1GPU_ERR_NOMEM;
     for (auto& it : k->orbs) {
       const double2* pot = k->d_pots + (size_t)it.iat * 49;
@@ -758,12 +808,28 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     }
     CK(cudaGetLastError());
   }
-  if (st) CK(cudaEventRecord(c->ev[5], s));
+  if (ev) CK(cudaEventRecord(ev[5], s));
   nl++;
   k_check_finite<<<296, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
   CK(cudaGetLastError());
+  if (ev) CK(cudaEventRecord(ev[6], s));
+  *nlaunch += nl;
+  return LAPW1GPU_OK;
+}
+
+extern "C" {
+
+int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, double* d_hs_, int ldhs,
+                        double* d_hsdiag_, lapw1gpu_stats* st) {
+  if (!c || !k || !d_hs_ || !d_hsdiag_ || ldhs < k->n || k->ctx != c) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  int nl = 0;
+  int rc = kpoint_run_impl(c, k, stages, reinterpret_cast<double2*>(d_hs_), ldhs, reinterpret_cast<double2*>(d_hsdiag_),
+                           s, 0, st ? c->ev : nullptr, &nl);
+  if (rc) return rc;
   if (st) {
-    CK(cudaEventRecord(c->ev[6], s));
     int hstat = 0;
     CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -783,6 +849,168 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     st->kernel_launches = nl;
     if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
     if (hstat) return LAPW1GPU_ERR_RANGE;
+  }
+  return LAPW1GPU_OK;
+}
+
+// ---- k-point batches: one captured graph per argument set ----
+static int batch_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int nk, int stages, double* const* d_hs,
+                         const int* ldhs, double* const* d_hsdiag, int* nl) {
+  const int sets = std::max(1, std::min(c->batch_sets, L1G_MAX_SETS));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaEventRecord(c->fork, c->stream));
+  for (int q = 1; q < sets; q++) CK(cudaStreamWaitEvent(c->side[q], c->fork, 0));
+  for (int i = 0; i < nk; i++) {
+    const int set = i % sets;
+    cudaStream_t s = set ? c->side[set] : c->stream;
+    int rc = kpoint_run_impl(c, kps[i], stages, reinterpret_cast<double2*>(d_hs[i]), ldhs[i],
+                             reinterpret_cast<double2*>(d_hsdiag[i]), s, set, nullptr, nl);
+    if (rc) return rc;
+  }
+  for (int q = 1; q < sets; q++) {
+    CK(cudaEventRecord(c->join[q], c->side[q]));
+    CK(cudaStreamWaitEvent(c->stream, c->join[q], 0));
+  }
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int nk, int stages, double* const* d_hs,
+                         const int* ldhs, double* const* d_hsdiag, lapw1gpu_stats* st) {
+  if (!c || !kps || nk < 1 || !d_hs || !ldhs || !d_hsdiag || !(stages & 1)) return LAPW1GPU_ERR_ARG;
+  for (int i = 0; i < nk; i++)
+    if (!kps[i] || kps[i]->ctx != c || !d_hs[i] || !d_hsdiag[i] || ldhs[i] < kps[i]->n) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  std::vector<uintptr_t> key = {(uintptr_t)nk,         (uintptr_t)stages,        (uintptr_t)c->prec,
+                                (uintptr_t)c->slices,  (uintptr_t)c->hns_diag_b, (uintptr_t)c->split_group,
+                                (uintptr_t)c->sph_tc,  (uintptr_t)c->batch_sets};
+  for (int i = 0; i < nk; i++) {
+    key.push_back((uintptr_t)kps[i]);
+    key.push_back((uintptr_t)d_hs[i]);
+    key.push_back((uintptr_t)ldhs[i]);
+    key.push_back((uintptr_t)d_hsdiag[i]);
+  }
+  lapw1gpu_context::Graph* g = nullptr;
+  for (auto& x : c->graphs)
+    if (x.key == key) g = &x;
+  if (!g) {
+    // one eager pass sizes every scratch buffer and builds every tile list,
+    // so that the capture below performs no allocation or host copy
+    int nl = 0;
+    int rc = batch_enqueue(c, kps, nk, stages, d_hs, ldhs, d_hsdiag, &nl);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    nl = 0;
+    rc = batch_enqueue(c, kps, nk, stages, d_hs, ldhs, d_hsdiag, &nl);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc || e != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return rc ? rc : LAPW1GPU_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return LAPW1GPU_ERR_CUDA;
+    }
+    c->graphs.push_back({key, exec, nl});
+    g = &c->graphs.back();
+  }
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  CK(cudaGraphLaunch(g->exec, c->stream));
+  CK(cudaEventRecord(c->ev[6], c->stream));
+  int hstat = 0;
+  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_status = hstat;
+  if (st) {
+    memset(st, 0, sizeof(*st));
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]);
+    st->ms_total = tot;
+    for (int i = 0; i < nk; i++) st->flops_fp64_equiv += alg_flops(kps[i]);
+    st->kernel_launches = g->launches;
+  }
+  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+  if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+  if (hstat) return LAPW1GPU_ERR_RANGE;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_get_tuning(lapw1gpu_context* c, lapw1gpu_tuning* t) {
+  if (!c || !t) return LAPW1GPU_ERR_ARG;
+  t->hns_diag_b = c->hns_diag_b;
+  t->split_group = c->split_group;
+  t->sph_tc = c->sph_tc;
+  t->batch_sets = c->batch_sets;
+  t->ms_best = 0.0;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_set_tuning(lapw1gpu_context* c, const lapw1gpu_tuning* t) {
+  if (!c || !t) return LAPW1GPU_ERR_ARG;
+  if (t->hns_diag_b < HNS_T || t->hns_diag_b % HNS_T || t->split_group < 1 || t->batch_sets < 1 ||
+      t->batch_sets > L1G_MAX_SETS || (t->sph_tc != 0 && t->sph_tc != 1))
+    return LAPW1GPU_ERR_RANGE;
+  c->hns_diag_b = t->hns_diag_b;
+  c->split_group = t->split_group;
+  c->sph_tc = t->sph_tc;
+  c->batch_sets = t->batch_sets;
+  return LAPW1GPU_OK;
+}
+
+// Autotuner: every candidate of a tunable is timed on kp (best of two
+// runs, CUDA events around the whole stage sequence) with the others held,
+// tunables one after another; the fastest is kept.
+int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, int ldhs, double* d_hsdiag,
+                      lapw1gpu_tuning* out) {
+  if (!c || !kp || !d_hs || !d_hsdiag || ldhs < kp->n || kp->ctx != c) return LAPW1GPU_ERR_ARG;
+  auto time_once = [&](double* ms) -> int {
+    double best = 1e30;
+    for (int r = 0; r < 2; r++) {
+      lapw1gpu_stats st;
+      int rc = lapw1gpu_kpoint_run(c, kp, 7, d_hs, ldhs, d_hsdiag, &st);
+      if (rc) return rc;
+      best = std::min(best, st.ms_total);
+    }
+    *ms = best;
+    return LAPW1GPU_OK;
+  };
+  auto tune = [&](int* knob, const std::vector<int>& cand, double* best_ms) -> int {
+    int best = *knob;
+    double bm = 1e30;
+    for (int v : cand) {
+      *knob = v;
+      double ms;
+      int rc = time_once(&ms);
+      if (rc) {
+        *knob = best;
+        return rc;
+      }
+      if (ms < bm) {
+        bm = ms;
+        best = v;
+      }
+    }
+    *knob = best;
+    *best_ms = bm;
+    return LAPW1GPU_OK;
+  };
+  double ms = 0.0;
+  int rc = LAPW1GPU_OK;
+  if (c->prec == LAPW1GPU_PREC_FP64) {
+    rc = tune(&c->hns_diag_b, {256, 512, 1024, 2048}, &ms);
+  } else {
+    if (sph_tc_supported(c->slices)) rc = tune(&c->sph_tc, {1, 0}, &ms);
+    if (!rc) rc = tune(&c->split_group, {4, 8, 16, 32}, &ms);
+  }
+  if (rc) return rc;
+  if (out) {
+    lapw1gpu_get_tuning(c, out);
+    out->ms_best = ms;
   }
   return LAPW1GPU_OK;
 }
@@ -934,8 +1162,8 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   double2* rhoe = (double2*)c->buf("frc_rhoe", sizeof(double2) * (size_t)n * n);
   SphCoef* coef = (SphCoef*)c->buf("coef", sizeof(SphCoef) * nat * ltop);
   if (!P.al || !P.bl || !P.phase || !Cf || !Ce || !rho || !rhoe || !coef) return LAPW1GPU_ERR_NOMEM;
-  if (!c->blas && cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
-  if (cublasSetStream(c->blas, s) != CUBLAS_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  cublasHandle_t h = c->handle(0, s);
+  if (!h) return LAPW1GPU_ERR_CUDA;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
   CK(cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * ndf, s));
@@ -945,15 +1173,15 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, Cf, Ce);
   CK(cudaGetLastError());
   // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)): column-major n x n
-  if (cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Cf, n,
+  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Cf, n,
                   (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
-      cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Ce, n,
+      cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Ce, n,
                   (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
     return LAPW1GPU_ERR_CUDA;
   int ntiles = 0;
-  const int2* tl = tiles_tri(c, "tiles_sph", nv, SPH_T, &ntiles);
+  const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
-  CK(cudaFuncSetAttribute(k_force_sph, cudaFuncAttributeMaxDynamicSharedMemorySize, SPH_DYN_SMEM));
+  if (!c->smem((const void*)k_force_sph, SPH_DYN_SMEM)) return LAPW1GPU_ERR_CUDA;
   k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, d_grad);
   CK(cudaGetLastError());
   if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, d_grad);
@@ -971,14 +1199,14 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     double2* Z = (double2*)c->buf("frc_z", sizeof(double2) * (size_t)4 * nb * K);
     if (!Lop || !Rop || !Clo || !C2lo || !GC || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
     int nl = 0;
-    int rc = launch_hns_ops(P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
     if (rc) return rc;
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
     CK(cudaGetLastError());
     // Y = R^H (G c), Z = L^T (G c): K x 4nb, rows of R and L beyond n unused
-    if (cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
+    if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
                     (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS ||
-        cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Lop, k->npad,
+        cublasZgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Lop, k->npad,
                     (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Z, K) != CUBLAS_STATUS_SUCCESS)
       return LAPW1GPU_ERR_CUDA;
     k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
@@ -988,7 +1216,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       double2* Yc = (double2*)c->buf("frc_yc", sizeof(double2) * (size_t)4 * nb * Kc);
       double2* Zc = (double2*)c->buf("frc_zc", sizeof(double2) * (size_t)4 * nb * Kc);
       if (!Yc || !Zc) return LAPW1GPU_ERR_NOMEM;
-      if (cublasZgemm(c->blas, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
+      if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
                       (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc, Kc) != CUBLAS_STATUS_SUCCESS)
         return LAPW1GPU_ERR_CUDA;
       k_force_hns_zc<<<dim3(4 * nb, ndf), 32, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Zc);
@@ -1165,7 +1393,7 @@ extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, in
   k_albl<<<dim3((nvpad + 127) / 128, nat), 128, 0, s>>>(P, d_status);
   k_phase<<<dim3((npad + 127) / 128, ndf), 128, 0, s>>>(P);
   int nops = 0;
-  rc = launch_hns_ops(P, d_tns, d_lor, nlor, Lop, Rop, Clo, C2lo, s, &nops);
+  rc = launch_hns_ops(nullptr, P, d_tns, d_lor, nlor, Lop, Rop, Clo, C2lo, s, &nops);
   if (rc) return rc;
   k_hns_gemm<<<(unsigned)ntiles, 256, 0, s>>>(n, npad, K, d_tiles, Lop, Rop, d_hs, ldhs);
   if (p->nlo > 0)

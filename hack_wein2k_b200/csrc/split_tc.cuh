@@ -375,16 +375,17 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
 }
 
 template <int S>
-static int split_gemm_launch(lapw1gpu_context* c, int n, int npad, int Kc, const double2* Lop, const double2* Rop,
-                             double2* hs, int ld, cudaStream_t s, int* nlaunch) {
+static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
+                             const double2* Lop, const double2* Rop, double2* hs, int ld, cudaStream_t s,
+                             int* nlaunch) {
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
-  const int np = (npad + 127) / 128 * 128;  // slice rows padded to the 128-row tile
-  int8_t* A = (int8_t*)c->buf("splitA", (size_t)S * np * Kp);
-  int8_t* B = (int8_t*)c->buf("splitB", (size_t)S * 2 * np * Kp);
-  int* exA = (int*)c->buf("splitExA", sizeof(int) * np);
-  int* exB = (int*)c->buf("splitExB", sizeof(int) * np);
+  const int np = (npad + 127) / 128 * 128;
+  int8_t* A = (int8_t*)c->sbuf(set, "splitA", (size_t)S * np * Kp);
+  int8_t* B = (int8_t*)c->sbuf(set, "splitB", (size_t)S * 2 * np * Kp);
+  int* exA = (int*)c->sbuf(set, "splitExA", sizeof(int) * np);
+  int* exB = (int*)c->sbuf(set, "splitExB", sizeof(int) * np);
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
   // rows in [npad, np) and the K padding stay zero
   if (cudaMemsetAsync(A, 0, (size_t)S * np * Kp, s) != cudaSuccess ||
@@ -399,47 +400,38 @@ static int split_gemm_launch(lapw1gpu_context* c, int n, int npad, int Kc, const
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;
-  const long key = (long)n * 1024 + Cf::JT;
+  // grouped order: W row tiles of L stay in L2 while every column tile of R
+  // that meets them streams past once, so R is read from DRAM once per
+  // group instead of once per row tile (W is a tunable, 16 by default)
+  const int W = c->split_group;
   int ntile = 0;
-  int2* dt = nullptr;
-  auto it = c->tile_keys.find("tiles_split");
-  if (it != c->tile_keys.end() && it->second.first == key) {  // uploaded by an earlier run
-    ntile = it->second.second;
-    dt = (int2*)c->bufs["tiles_split"].ptr;
-  } else {
-    std::vector<int2> t;
-    const int nbi = (n + 127) / 128, nbj = (n + Cf::JT - 1) / Cf::JT;
-    for (int bi = 0; bi < nbi; bi++)
-      for (int bj = 0; bj < nbj; bj++)
-        if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
-    c->tile_keys.erase("tiles_split");
-    if (cudaStreamSynchronize(s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;  // earlier runs may still read it
-    dt = (int2*)c->buf("tiles_split", sizeof(int2) * t.size());
-    if (!dt) return LAPW1GPU_ERR_NOMEM;
-    if (cudaMemcpy(dt, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-      return LAPW1GPU_ERR_CUDA;
-    ntile = (int)t.size();
-    c->tile_keys["tiles_split"] = std::make_pair(key, ntile);
-  }
-  if (cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM) !=
-      cudaSuccess)
-    return LAPW1GPU_ERR_CUDA;
+  const int2* dt = kp_tiles(k, "split:" + std::to_string(n) + ":" + std::to_string(Cf::JT) + ":" + std::to_string(W),
+                            &ntile, [&](std::vector<int2>& t) {
+                              const int nbi = (n + 127) / 128, nbj = (n + Cf::JT - 1) / Cf::JT;
+                              for (int g0 = 0; g0 < nbi; g0 += W)
+                                for (int bj = 0; bj < nbj; bj++)
+                                  for (int bi = g0; bi < std::min(nbi, g0 + W); bi++)
+                                    if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
+                            });
+  if (!dt) return LAPW1GPU_ERR_NOMEM;
+  if (!c->smem((const void*)split::k_split_gemm<S>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
   split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, exA, exB, hs, ld,
-                                                                   c->d_status);
+                                                                 c->d_status);
   *nlaunch += 1;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
-static int split_hns_gemm(lapw1gpu_context* c, int n, int npad, int Kc, const double2* Lop, const double2* Rop,
-                          double2* hs, int ld, int slices, cudaStream_t s, int* nlaunch) {
+static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
+                          const double2* Lop, const double2* Rop, double2* hs, int ld, int slices, cudaStream_t s,
+                          int* nlaunch) {
   switch (slices) {
-    case 2: return split_gemm_launch<2>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 3: return split_gemm_launch<3>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 4: return split_gemm_launch<4>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 5: return split_gemm_launch<5>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 6: return split_gemm_launch<6>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 7: return split_gemm_launch<7>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 8: return split_gemm_launch<8>(c, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }

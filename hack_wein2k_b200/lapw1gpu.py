@@ -32,10 +32,21 @@ EXPORTS = [
     "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
-    "lapw1gpu_hns_noalloc", "lapw1gpu_forces",
+    "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
+    "lapw1gpu_set_tuning", "lapw1gpu_autotune",
 ]
 
 _lib = None
+
+
+class Tuning(C.Structure):
+    """ctypes mirror of `lapw1gpu_tuning`."""
+
+    _fields_ = [("hns_diag_b", C.c_int), ("split_group", C.c_int), ("sph_tc", C.c_int),
+                ("batch_sets", C.c_int), ("ms_best", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Lapw1GpuError(RuntimeError):
@@ -71,6 +82,11 @@ def load(path: Optional[str] = None):
                                             dp, dp, dp, ip, dp]
     lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p]
     lib.lapw1gpu_forces.argtypes = [vp, vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.lapw1gpu_setup_batch.argtypes = [vp, C.POINTER(vp), C.c_int, C.c_int, C.POINTER(C.c_void_p),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(CStats)]
+    lib.lapw1gpu_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+    lib.lapw1gpu_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+    lib.lapw1gpu_autotune.argtypes = [vp, vp, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(Tuning)]
     _lib = lib
     return lib
 
@@ -164,6 +180,37 @@ class Context:
 
     def upload(self, prob: Problem) -> KPoint:
         return KPoint(self, prob)
+
+    def setup_batch(self, kps, d_hs_ptrs, ldhs, d_hsdiag_ptrs, stages: int = 7) -> dict:
+        """lapw1gpu_setup_batch over resident k-points into device buffers;
+        returns the batch stats (ms_total of the whole batch)."""
+        nk = len(kps)
+        karr = (C.c_void_p * nk)(*[k.h.value if isinstance(k.h, C.c_void_p) else k.h for k in kps])
+        harr = (C.c_void_p * nk)(*d_hs_ptrs)
+        larr = (C.c_int * nk)(*ldhs)
+        darr = (C.c_void_p * nk)(*d_hsdiag_ptrs)
+        st = CStats()
+        _check("lapw1gpu_setup_batch",
+               self.lib.lapw1gpu_setup_batch(self.h, karr, nk, stages, harr, larr, darr, C.byref(st)))
+        return st.as_dict()
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check("lapw1gpu_get_tuning", self.lib.lapw1gpu_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw) -> None:
+        t = Tuning()
+        _check("lapw1gpu_get_tuning", self.lib.lapw1gpu_get_tuning(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check("lapw1gpu_set_tuning", self.lib.lapw1gpu_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, kp: KPoint, d_hs_ptr: int, ldhs: int, d_hsdiag_ptr: int) -> dict:
+        t = Tuning()
+        _check("lapw1gpu_autotune", self.lib.lapw1gpu_autotune(self.h, kp.h, C.c_void_p(d_hs_ptr), ldhs,
+                                                               C.c_void_p(d_hsdiag_ptr), C.byref(t)))
+        return t.as_dict()
 
     def close(self):
         if self.h:

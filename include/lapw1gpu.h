@@ -233,6 +233,36 @@ int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx,
 int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs, int ldhs,
                          void* stream);
 
+/* A k-point batch (a lapw1 k-list, lapw1.F:50-67 calls CALKPT per k) set
+ * up in one launch: the stage sequences of all nk uploaded k-points are
+ * captured once into a CUDA graph, the k-points spread over the context's
+ * concurrent chains (each chain with its own scratch), and the graph is
+ * replayed by later calls with the same arguments.  stages must include 1
+ * (HS is built from scratch).  d_hs[i] / d_hsdiag[i]: device, k-point i's
+ * HS (ldhs[i] >= n_i) and HSDIAG.  Synchronous; st (optional) gets
+ * ms_total of the whole batch and the summed flops and launches. */
+int lapw1gpu_setup_batch(lapw1gpu_context* ctx, lapw1gpu_kpoint* const* kps,
+                         int nk, int stages, double* const* d_hs,
+                         const int* ldhs, double* const* d_hsdiag,
+                         lapw1gpu_stats* st);
+
+/* Tunables of the context (tile and schedule parameters) and the
+ * autotuner that picks them by timing candidates on a k-point. */
+typedef struct {
+  int hns_diag_b;   /* FP64 HNS: diagonal block of the blocked update (256..2048) */
+  int split_group;  /* split HNS: row tiles per L2 rasterisation group           */
+  int sph_tc;       /* split: spherical part on tcgen05 (1) or FP64 (0)          */
+  int batch_sets;   /* concurrent k-point chains in a batch (1..4)               */
+  double ms_best;   /* setup time of the tuned k-point with the choices, ms      */
+} lapw1gpu_tuning;
+int lapw1gpu_get_tuning(lapw1gpu_context* ctx, lapw1gpu_tuning* t);
+int lapw1gpu_set_tuning(lapw1gpu_context* ctx, const lapw1gpu_tuning* t);
+/* Time the candidates of every tunable of the current precision on kp
+ * (stages 7 into d_hs/d_hsdiag) and keep the fastest; out (optional) gets
+ * the choices.  No counterpart in the reference. */
+int lapw1gpu_autotune(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp, double* d_hs,
+                      int ldhs, double* d_hsdiag, lapw1gpu_tuning* out);
+
 /* Gradient of the band energy E = sum_b occ[b] eps[b] with respect to the
  * atom positions POS (lattice coordinates), for the eigenpairs of the H, S
  * that lapw1gpu_kpoint_run builds for kp (H c = eps S c as SECLR4 forms it).

@@ -1,0 +1,126 @@
+"""k-point batches (one captured CUDA graph, concurrent k-point chains) and
+the autotuner.
+
+A batch runs the same kernels as single k-points, so its HS/HSDIAG must be
+bitwise equal to lapw1gpu_kpoint_run's on every k-point, on the first call
+(capture) and on replays; k-points of uneven size share the graph.  The
+oracle pins two of them at the FP64 parity bar (1e-12).
+"""
+import numpy as np
+import pytest
+import torch
+
+from hack_wein2k_b200 import lapw1gpu, synth
+from oracle import oracle as O
+from tests.helpers import rel_errors
+
+TOL_FP64 = 1e-12
+
+
+def _small_batch():
+    """Uneven k-points of the small mixed cell, every branch kind."""
+    return [synth.small_case(k) for k in ("lo", "apw", "ins", "gamma", "plain", "multilo")]
+
+
+def _alloc(probs, dev):
+    hs = [torch.zeros((p.n, p.n), dtype=torch.complex128, device=dev) for p in probs]
+    hd = [torch.zeros(p.n, dtype=torch.complex128, device=dev) for p in probs]
+    return hs, hd
+
+
+def _host(t):
+    """device HS viewed [col][row] -> Fortran-ordered numpy HS(row, col)"""
+    return t.cpu().numpy().T
+
+
+def _single(ctx, probs, dev):
+    out = []
+    for p in probs:
+        kp = ctx.upload(p)
+        hs, hd = _alloc([p], dev)
+        kp.run(hs[0].data_ptr(), p.n, hd[0].data_ptr(), stats=True)
+        out.append((_host(hs[0]), hd[0].cpu().numpy()))
+        kp.free()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,slices", [(lapw1gpu.PREC_FP64, 6), (lapw1gpu.PREC_SPLIT, 5)])
+@pytest.mark.parametrize("sets", [1, 2, 3])
+def test_batch_equals_single_runs(ctx, prec, slices, sets):
+    dev = torch.device("cuda", ctx.device)
+    ctx.set_precision(prec, slices)
+    ctx.set_tuning(batch_sets=sets)
+    probs = _small_batch()
+    ref = _single(ctx, probs, dev)
+    kps = [ctx.upload(p) for p in probs]
+    hs, hd = _alloc(probs, dev)
+    for call in range(2):  # capture, then replay
+        for t in hs + hd:
+            t.zero_()
+        st = ctx.setup_batch(kps, [h.data_ptr() for h in hs], [p.n for p in probs], [d.data_ptr() for d in hd])
+        assert st["ms_total"] > 0 and st["kernel_launches"] > 0
+        for i, p in enumerate(probs):
+            assert np.array_equal(_host(hs[i]), ref[i][0]), (call, i)
+            assert np.array_equal(hd[i].cpu().numpy(), ref[i][1]), (call, i)
+    for k in kps:
+        k.free()
+    ctx.set_tuning(batch_sets=2)
+    ctx.set_precision(lapw1gpu.PREC_FP64)
+
+
+@pytest.mark.gpu
+def test_batch_against_oracle(ctx):
+    dev = torch.device("cuda", ctx.device)
+    ctx.set_precision(lapw1gpu.PREC_FP64)
+    probs = [synth.small_case("lo"), synth.small_case("gamma")]
+    kps = [ctx.upload(p) for p in probs]
+    hs, hd = _alloc(probs, dev)
+    ctx.setup_batch(kps, [h.data_ptr() for h in hs], [p.n for p in probs], [d.data_ptr() for d in hd])
+    for i, p in enumerate(probs):
+        hs_o, hd_o = O.setup(p)
+        err = rel_errors(_host(hs[i]), hd[i].cpu().numpy(), hs_o, hd_o)
+        assert err["H"] <= TOL_FP64 and err["S"] <= TOL_FP64, err
+    for k in kps:
+        k.free()
+
+
+@pytest.mark.gpu
+def test_batch_of_uneven_c2_kpoints(ctx):
+    """Four k-points of the 40-atom cell's wedge (uneven N) in one graph."""
+    dev = torch.device("cuda", ctx.device)
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 6)
+    probs = synth.config("c2", nk=4)
+    assert len({p.n for p in probs}) > 1
+    ref = _single(ctx, probs, dev)
+    kps = [ctx.upload(p) for p in probs]
+    hs, hd = _alloc(probs, dev)
+    ctx.setup_batch(kps, [h.data_ptr() for h in hs], [p.n for p in probs], [d.data_ptr() for d in hd])
+    for i in range(len(probs)):
+        assert np.array_equal(_host(hs[i]), ref[i][0])
+    for k in kps:
+        k.free()
+    ctx.set_precision(lapw1gpu.PREC_FP64)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,slices", [(lapw1gpu.PREC_FP64, 6), (lapw1gpu.PREC_SPLIT, 6)])
+def test_autotune_keeps_results_exact(ctx, prec, slices):
+    """The tuner only picks among equivalent schedules: results after tuning
+    still meet the parity bar of the precision."""
+    dev = torch.device("cuda", ctx.device)
+    ctx.set_precision(prec, slices)
+    p = synth.small_case("lo", rkmax=6.0)
+    kp = ctx.upload(p)
+    hs, hd = _alloc([p], dev)
+    t = ctx.autotune(kp, hs[0].data_ptr(), p.n, hd[0].data_ptr())
+    assert t["hns_diag_b"] in (256, 512, 1024, 2048)
+    assert t["split_group"] in (4, 8, 16, 32) and t["sph_tc"] in (0, 1) and t["ms_best"] > 0
+    kp.run(hs[0].data_ptr(), p.n, hd[0].data_ptr(), stats=True)
+    hs_o, hd_o = O.setup(p)
+    err = rel_errors(_host(hs[0]), hd[0].cpu().numpy(), hs_o, hd_o)
+    tol = TOL_FP64 if prec == lapw1gpu.PREC_FP64 else 2e-11
+    assert err["H"] <= tol and err["S"] <= tol, err
+    kp.free()
+    ctx.set_tuning(hns_diag_b=512, split_group=16, sph_tc=1)
+    ctx.set_precision(lapw1gpu.PREC_FP64)
