@@ -8,7 +8,7 @@ GPU the workload is the 40-atom 2x2x2 ABO3 supercell (RKmax 7, ~4950 basis
 functions, one LO per atom for l<=2, one general k).  With N GPUs each rank
 sets up its own k-point of the same cell (k-points are independent: weak
 scaling, no collective on the data path).  Prints ONE JSON line (rank 0).
-The default arithmetic is the split-precision path (6 int8 slices; the
+The default arithmetic is the split-precision path (5 int8 slices; the
 plain FP64 GPU path on the same k-point is timed beside it in
 `fp64_path`, with the split path's per-matrix error against it), after the
 autotuner has picked the tile/schedule parameters (untimed).  `batch` is a
@@ -228,7 +228,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--prec", choices=["fp64", "split"], default="split")
-    ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--slices", type=int, default=5)
+    ap.add_argument("--slices-hns", type=int, default=None, help="int8 slices of HNS (default: --slices)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
@@ -259,6 +260,9 @@ def main():
 
     prec = lapw1gpu.PREC_SPLIT if args.prec == "split" else lapw1gpu.PREC_FP64
     ctx = lapw1gpu.Context(local, prec=prec, slices=args.slices)
+    slices_hns = args.slices_hns if args.slices_hns else args.slices
+    if prec == lapw1gpu.PREC_SPLIT:
+        ctx.set_slices(args.slices, slices_hns)
     stream = torch.cuda.ExternalStream(ctx.stream_handle, device=device)
     kp = ctx.upload(p)
     n = p.n
@@ -413,10 +417,12 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.prec == "fp64" else f"int8 x{args.slices} slices, f64 combine",
+        "vs_baseline": None,
+        "dtype": "f64" if args.prec == "fp64" else f"int8 x{args.slices}/x{slices_hns} slices (spherical/HNS), f64 combine",
         "data": "synthetic (seeded)",
         "config": {"workload": workload, "n": n, "nv": p.nv, "nlo": p.nlo, "atoms": p.ndf, "lmax": p.ltop - 1,
-                   "lmax_ns": p.lnsmax, "precision": args.prec, "slices": args.slices if split else None,
+                   "lmax_ns": p.lnsmax, "precision": args.prec,
+                   "slices": [args.slices, slices_hns] if split else None,
                    "parallelism": f"k-shard x{world}",
                    "l2": "HS output 0.39 GB and HNS operands 0.32 GB per k-point exceed the 126 MB L2"},
         "kpoints_per_s": 1e3 / value,

@@ -762,6 +762,16 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// LO block of HNS through a library product: HS(nv+i, nv+j) += T(i, j) on
+// the lower triangle i >= j, T = C2^T CLM computed into a scratch block
+__global__ void k_add_lower(int nv, int nlo, const double2* __restrict__ T, double2* __restrict__ hs, int ld) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cj = blockIdx.y;
+  if (ci >= nlo || ci < cj) return;
+  double2* dst = hs + (size_t)(nv + cj) * ld + (nv + ci);
+  *dst = cadd(*dst, T[(size_t)cj * nlo + ci]);
+}
+
 // LO block of HNS: HS(i,j) += sum C2[k][i] CLM[k][j], nv <= j <= i < n
 __global__ void k_hns_lo(int nv, int nlo, int K, const double2* __restrict__ C2lo, const double2* __restrict__ Clo,
                          double2* __restrict__ hs, int ld) {
@@ -910,16 +920,21 @@ __global__ void k_horb_pairs(DevProb P, int a, int lvor, const double2* __restri
 // non-finite scan of the n x n block and hsdiag
 __global__ void k_check_finite(int n, const double2* __restrict__ hs, int ld, const double2* __restrict__ hsdiag,
                                int* status) {
-  size_t tot = (size_t)n * n;
-  bool bad = false;
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
-    size_t j = q / n, i = q % n;
-    double2 v = hs[j * ld + i];
-    if (!isfinite(v.x) || !isfinite(v.y)) bad = true;
-    if (j == 0) {
-      double2 d = hsdiag[i];
-      if (!isfinite(d.x) || !isfinite(d.y)) bad = true;
+  // a component is non-finite when its exponent bits are all ones
+  unsigned bad = 0;
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    const double2* col = hs + (size_t)j * ld;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double2 v = col[i];
+      bad |= ((unsigned)(__double_as_longlong(v.x) >> 52) & 0x7ffu) == 0x7ffu;
+      bad |= ((unsigned)(__double_as_longlong(v.y) >> 52) & 0x7ffu) == 0x7ffu;
     }
   }
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double2 d = hsdiag[i];
+      bad |= ((unsigned)(__double_as_longlong(d.x) >> 52) & 0x7ffu) == 0x7ffu;
+      bad |= ((unsigned)(__double_as_longlong(d.y) >> 52) & 0x7ffu) == 0x7ffu;
+    }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, L1G_STATUS_NONFINITE);
 }

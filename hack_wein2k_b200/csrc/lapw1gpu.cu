@@ -44,7 +44,8 @@ struct lapw1gpu_context {
   int* d_status = nullptr;
   int last_status = 0;
   int prec = LAPW1GPU_PREC_FP64;
-  int slices = 6;
+  int slices = 5;      // int8 slices of the spherical part (split precision)
+  int slices_hns = 5;  // int8 slices of the HNS update
   cublasHandle_t blas[L1G_MAX_SETS] = {};  // library ZGEMMs, one handle (and workspace) per scratch set
   // tunables (lapw1gpu_autotune)
   int hns_diag_b = 512;    // FP64 HNS: diagonal block of the blocked ZHER2M form
@@ -289,7 +290,16 @@ int lapw1gpu_set_precision(lapw1gpu_context* c, int prec, int slices) {
   if (prec != LAPW1GPU_PREC_FP64 && prec != LAPW1GPU_PREC_SPLIT) return LAPW1GPU_ERR_ARG;
   if (prec == LAPW1GPU_PREC_SPLIT && (slices < 2 || slices > L1G_MAX_SLICES)) return LAPW1GPU_ERR_RANGE;
   c->prec = prec;
-  if (prec == LAPW1GPU_PREC_SPLIT) c->slices = slices;
+  if (prec == LAPW1GPU_PREC_SPLIT) c->slices = c->slices_hns = slices;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_set_slices(lapw1gpu_context* c, int slices_sph, int slices_hns) {
+  if (!c) return LAPW1GPU_ERR_ARG;
+  if (slices_sph < 2 || slices_sph > L1G_MAX_SLICES || slices_hns < 2 || slices_hns > L1G_MAX_SLICES)
+    return LAPW1GPU_ERR_RANGE;
+  c->slices = slices_sph;
+  c->slices_hns = slices_hns;
   return LAPW1GPU_OK;
 }
 
@@ -627,7 +637,7 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
                          const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
   using Cf = sphtc::Cfg<S>;
   const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
-  const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;
+  const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;  // Kp: whole 64-byte K blocks
   const int npA = round_up(nv, 128), npB = round_up(nv, Cf::IT);
   int8_t* A = (int8_t*)c->sbuf(set, "sphA", (size_t)S * L * npA * Kp);
   int8_t* B = (int8_t*)c->sbuf(set, "sphB", (size_t)S * L * 4 * npB * Kp);
@@ -641,7 +651,8 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   sphtc::k_sph_slice<<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, S, B, exB);
   *nl += 2;
   CUtensorMap ta, tb;
-  if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128) || l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N))
+  if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, 64) ||
+      l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N, 64))
     return LAPW1GPU_ERR_CUDA;
   int ntile = 0;
   // I tiles outer: the CTAs resident at one time share few I tiles (B
@@ -774,7 +785,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
     if (rc) return rc;
     if (c->prec == LAPW1GPU_PREC_SPLIT)
-      rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices, s, &nl);
+      rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl);
     else {
       int ntiles = 0;
       const int2* tl = tiles_hns_diag(k, n, c->hns_diag_b, &ntiles);
@@ -786,7 +797,17 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     if (rc) return rc;
     if (k->nlo > 0) {
       nl++;
-      k_hns_lo<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);
+      // T = C2^T CLM (nlo x nlo, K = NDF 25) by library ZGEMM, then its
+      // lower triangle into HS
+      double2* T = (double2*)c->sbuf(set, "hnsLoT", sizeof(double2) * (size_t)k->nlo * k->nlo);
+      cublasHandle_t h = c->handle(set, s);
+      if (!T || !h) return LAPW1GPU_ERR_NOMEM;
+      const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+      if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, k->nlo, k->nlo, ndf * nsl2, &one, (const cuDoubleComplex*)C2lo,
+                      k->nlo, (const cuDoubleComplex*)Clo, k->nlo, &zero, (cuDoubleComplex*)T,
+                      k->nlo) != CUBLAS_STATUS_SUCCESS)
+        return LAPW1GPU_ERR_CUDA;
+      k_add_lower<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, T, d_hs, ldhs);
     }
     CK(cudaGetLastError());
   }
@@ -810,11 +831,28 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
   }
   if (ev) CK(cudaEventRecord(ev[5], s));
   nl++;
-  k_check_finite<<<296, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
+  k_check_finite<<<1184, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
   CK(cudaGetLastError());
   if (ev) CK(cudaEventRecord(ev[6], s));
   *nlaunch += nl;
   return LAPW1GPU_OK;
+}
+
+// per-stage timings from the events kpoint_run_impl recorded (ev[0..6])
+static void fill_stats(lapw1gpu_context* c, const lapw1gpu_kpoint* k, int nl, lapw1gpu_stats* st) {
+  float t[6];
+  for (int q = 0; q < 6; q++) cudaEventElapsedTime(&t[q], c->ev[q], c->ev[q + 1]);
+  memset(st, 0, sizeof(*st));
+  st->ms_albl = t[0];
+  st->ms_spherical = t[1];
+  st->ms_lo = t[2];
+  st->ms_hns = t[3];
+  st->ms_horb = t[4];
+  float tot;
+  cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]);
+  st->ms_total = tot;
+  st->flops_fp64_equiv = alg_flops(k);
+  st->kernel_launches = nl;
 }
 
 extern "C" {
@@ -834,20 +872,9 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
     CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c->last_status = hstat;
-    float t[6];
-    for (int q = 0; q < 6; q++) cudaEventElapsedTime(&t[q], c->ev[q], c->ev[q + 1]);
-    memset(st, 0, sizeof(*st));
-    st->ms_albl = t[0];
-    st->ms_spherical = t[1];
-    st->ms_lo = t[2];
-    st->ms_hns = t[3];
-    st->ms_horb = t[4];
-    float tot;
-    cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]);
-    st->ms_total = tot;
-    st->flops_fp64_equiv = alg_flops(k);
-    st->kernel_launches = nl;
+    fill_stats(c, k, nl, st);
     if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+    if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
     if (hstat) return LAPW1GPU_ERR_RANGE;
   }
   return LAPW1GPU_OK;
@@ -881,7 +908,8 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
     if (!kps[i] || kps[i]->ctx != c || !d_hs[i] || !d_hsdiag[i] || ldhs[i] < kps[i]->n) return LAPW1GPU_ERR_ARG;
   CK(cudaSetDevice(c->device));
   std::vector<uintptr_t> key = {(uintptr_t)nk,         (uintptr_t)stages,        (uintptr_t)c->prec,
-                                (uintptr_t)c->slices,  (uintptr_t)c->hns_diag_b, (uintptr_t)c->split_group,
+                                (uintptr_t)(c->slices * 16 + c->slices_hns), (uintptr_t)c->hns_diag_b,
+                                (uintptr_t)c->split_group,
                                 (uintptr_t)c->sph_tc,  (uintptr_t)c->batch_sets};
   for (int i = 0; i < nk; i++) {
     key.push_back((uintptr_t)kps[i]);
@@ -1015,50 +1043,93 @@ int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, in
   return LAPW1GPU_OK;
 }
 
-int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs, int ldhs,
-                          double* hsdiag, lapw1gpu_stats* st) {
-  if (!c || !p || !hs || !hsdiag || ldhs < p->n) return LAPW1GPU_ERR_ARG;
+// Host-buffer form.  When HAMILT runs together with HNS/HORB, the copy of
+// S back to the host overlaps them: S (the strict upper triangle) and
+// HSDIAG are final once HAMILT is done, and the later stages only touch the
+// lower triangle and the diagonal, so a copy stream takes, per panel of
+// columns [c0, c0+w), the rows above c0 as soon as HAMILT ends; the rest of
+// each panel follows the last stage.
+#define L1G_D2H_PANEL 256
+int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs_, int ldhs,
+                          double* hsdiag_, lapw1gpu_stats* st) {
+  if (!c || !p || !hs_ || !hsdiag_ || ldhs < p->n) return LAPW1GPU_ERR_ARG;
   CK(cudaSetDevice(c->device));
-  cudaEvent_t e0 = c->ev[7], e1 = c->ev[8], e2 = c->ev[9], e3 = c->ev[10];
-  cudaEventRecord(e0, c->stream);
+  double2* hs = reinterpret_cast<double2*>(hs_);
+  double2* hsdiag = reinterpret_cast<double2*>(hsdiag_);
+  cudaEvent_t e0 = c->ev[7], e1 = c->ev[8], e2 = c->ev[9], e3 = c->ev[10], ecp = c->ev[11];
+  cudaStream_t s = c->stream, cs = c->side[1];
+  CK(cudaEventRecord(e0, s));
   lapw1gpu_kpoint* k = nullptr;
   int rc = kpoint_upload_impl(c, p, &k, true);
   if (rc) return rc;
   const int n = p->n;
-  double2* d_hs = (double2*)c->buf("hs", sizeof(double2) * (size_t)n * n);
-  double2* d_hd = (double2*)c->buf("hsdiag", sizeof(double2) * (size_t)n);
+  const size_t z = sizeof(double2);
+  double2* d_hs = (double2*)c->buf("hs", z * (size_t)n * n);
+  double2* d_hd = (double2*)c->buf("hsdiag", z * (size_t)n);
   if (!d_hs || !d_hd) {
     lapw1gpu_kpoint_free(k);
     return LAPW1GPU_ERR_NOMEM;
   }
   // stages that only add (HNS/HORB alone) start from the caller's HS
   if (!(stages & 1)) {
-    cudaMemcpy2DAsync(d_hs, sizeof(double2) * n, hs, sizeof(double2) * ldhs, sizeof(double2) * n, n,
-                      cudaMemcpyHostToDevice, c->stream);
-    cudaMemcpyAsync(d_hd, hsdiag, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpy2DAsync(d_hs, z * n, hs, z * ldhs, z * n, n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_hd, hsdiag, z * n, cudaMemcpyHostToDevice, s);
   }
-  cudaEventRecord(e1, c->stream);
-  lapw1gpu_stats st2;
-  rc = lapw1gpu_kpoint_run(c, k, stages, (double*)d_hs, n, (double*)d_hd, &st2);
-  cudaEventRecord(e2, c->stream);
+  CK(cudaEventRecord(e1, s));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  int nl = 0;
+  rc = kpoint_run_impl(c, k, stages, d_hs, n, d_hd, s, 0, c->ev, &nl);
   if (rc == LAPW1GPU_OK) {
-    if (cudaMemcpy2DAsync(hs, sizeof(double2) * ldhs, d_hs, sizeof(double2) * n, sizeof(double2) * n, n,
-                          cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
-        cudaMemcpyAsync(hsdiag, d_hd, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
-      rc = LAPW1GPU_ERR_CUDA;
+    CK(cudaEventRecord(e2, s));
+    const bool overlap = (stages & 1) && (stages & 6);
+    if (overlap) {
+      // c->ev[3] marks the end of HAMILT (+ LO columns) on s
+      CK(cudaStreamWaitEvent(cs, c->ev[3], 0));
+      for (int c0 = L1G_D2H_PANEL; c0 < n; c0 += L1G_D2H_PANEL) {
+        const int w = std::min(L1G_D2H_PANEL, n - c0);
+        if (cudaMemcpy2DAsync(hs + (size_t)c0 * ldhs, z * ldhs, d_hs + (size_t)c0 * n, z * n, z * c0, w,
+                              cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+          rc = LAPW1GPU_ERR_CUDA;
+      }
+      if (cudaMemcpyAsync(hsdiag, d_hd, z * n, cudaMemcpyDeviceToHost, cs) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+      CK(cudaEventRecord(ecp, cs));
+    }
+    if (!overlap) {
+      if (cudaMemcpy2DAsync(hs, z * ldhs, d_hs, z * n, z * n, n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaMemcpyAsync(hsdiag, d_hd, z * n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        rc = LAPW1GPU_ERR_CUDA;
+    } else {
+      for (int c0 = 0; c0 < n; c0 += L1G_D2H_PANEL) {
+        const int w = std::min(L1G_D2H_PANEL, n - c0);
+        // rows [c0, n) of the panel (the first panel: all rows)
+        const int r0 = c0;
+        if (cudaMemcpy2DAsync(hs + (size_t)c0 * ldhs + r0, z * ldhs, d_hs + (size_t)c0 * n + r0, z * n, z * (n - r0),
+                              w, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+          rc = LAPW1GPU_ERR_CUDA;
+      }
+      CK(cudaStreamWaitEvent(s, ecp, 0));
+    }
   }
-  cudaEventRecord(e3, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
-  if (st) {
-    *st = st2;
+  CK(cudaEventRecord(e3, s));
+  int hstat = 0;
+  if (cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = rc ? rc : LAPW1GPU_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+  c->last_status = hstat;
+  if (st && rc == LAPW1GPU_OK) {
+    fill_stats(c, k, nl, st);
     float a, b;
     cudaEventElapsedTime(&a, e0, e1);
     cudaEventElapsedTime(&b, e2, e3);
     st->ms_h2d = a;
-    st->ms_d2h = b;
+    st->ms_d2h = b;  // the copies not hidden behind HNS/HORB
   }
   lapw1gpu_kpoint_free(k);
-  return rc;
+  if (rc) return rc;
+  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+  if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+  if (hstat) return LAPW1GPU_ERR_RANGE;
+  return LAPW1GPU_OK;
 }
 
 // hns.F:317-380 sums over LMSORT's grouping of the gaunt list

@@ -43,12 +43,15 @@ template <int S>
 struct Cfg {
   static constexpr int N = ((512 / (2 * S)) / 16) * 16;  // real columns per accumulator buffer
   static constexpr int IT = N / 4;                        // I per tile
+  // one pipeline stage: all S slices of a 64-byte K block of A (128 rows)
+  // and of B (N rows)
   static constexpr int A_BYTES = S * 128 * 64;
   static constexpr int B_BYTES = S * N * 64;
   static constexpr int STAGE = A_BYTES + B_BYTES;
-  // per-tile scale tables: 2^(eA - 12) per (l, J) and 2^eB per (l, I, S|H)
-  static constexpr int SCALE_BYTES = (SPH_LMAX * 128 + SPH_LMAX * 2 * IT) * 8;
-  static constexpr int STAGES = (4 * STAGE + SCALE_BYTES + 1024 <= 227 * 1024) ? 4 : 3;
+  // per-tile exponent tables: eA - 12 per (l, J) and eB per (l, I, S|H), int16
+  static constexpr int SCALE_BYTES = (SPH_LMAX * 128 + SPH_LMAX * 2 * IT) * 2;
+  static constexpr int STAGES_FIT = (227 * 1024 - SCALE_BYTES - 1024) / STAGE;
+  static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
   static constexpr int SMEM = STAGES * STAGE + SCALE_BYTES + 1024;
   static constexpr int THREADS = 288;
 };
@@ -161,9 +164,10 @@ __global__ void __launch_bounds__(256) k_sph_slice(DevProb P, const SphCoef* __r
   }
 }
 
-// 2^e as a double (exponent bits for the normal range)
+// 2^e as a double (exponent bits for the normal range, 0 far below it)
 __device__ __forceinline__ double pow2i(int e) {
-  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52)
+                                   : (e < -1022 ? 0.0 : ldexp(1.0, e));
 }
 
 // level sum of one accumulator column: sum_d c_d 2^(-7d), levels paired in
@@ -313,15 +317,15 @@ __global__ void __launch_bounds__(288, 1)
     // ---- epilogue warps ----
     // scale tables of this tile for every l, staged once (the l loop then
     // reads only shared memory and TMEM)
-    double* sA = (double*)(smem + STAGES * C::STAGE);  // [l][128]
-    double* sB = sA + SPH_LMAX * 128;                   // [l][IT][2]
+    int16_t* sA = (int16_t*)(smem + STAGES * C::STAGE);  // [l][128]: eA - 12
+    int16_t* sB = sA + SPH_LMAX * 128;                    // [l][IT][2]: eB
     for (int q = tid; q < L * 128; q += 256) {
       const int l = q >> 7, r = q & 127, J = j0 + r;
-      sA[q] = (J < nv) ? pow2i(exA[(size_t)l * npA + J] - 12) : 0.0;
+      sA[q] = (int16_t)((J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
     }
     for (int q = tid; q < L * 2 * IT; q += 256) {
       const int l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
-      sB[q] = (I < nv) ? pow2i(exB[(size_t)l * 2 * npB + 2 * I + (r & 1)]) : 0.0;
+      sB[q] = (int16_t)((I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
     }
     asm volatile("bar.sync 1, 256;" ::: "memory");  // the epilogue warps only
     const int g = warp & 3, hh = warp >> 2;
@@ -381,7 +385,7 @@ __global__ void __launch_bounds__(288, 1)
         }
         w[u] = (double)(2 * l + 1) * pl;
       }
-      const double fa = sA[l * 128 + 32 * g + lane];
+      const int ea = sA[l * 128 + 32 * g + lane];
       // 4 real columns per I: S re, S im, H re, H im; this thread's HALF I
       // start at column 4 * HALF * hh; read 8 columns (2 I) at a time
 #pragma unroll
@@ -404,9 +408,8 @@ __global__ void __launch_bounds__(288, 1)
 #pragma unroll
         for (int q = 0; q < 2; q++) {
           const int u = 2 * c + q;
-          const double wa = w[u] * fa;
-          const double* sb = sB + (l * IT + hh * HALF + u) * 2;
-          const double sS = wa * sb[0], sH = wa * sb[1];
+          const int16_t* sb = sB + (l * IT + hh * HALF + u) * 2;
+          const double sS = w[u] * pow2i(ea + sb[0]), sH = w[u] * pow2i(ea + sb[1]);
           double v[4];
 #pragma unroll
           for (int m = 0; m < 4; m++) {

@@ -100,86 +100,83 @@ struct Cfg {
 
 // FP64 -> int8 slices.  X: [Kc][npad] complex (k-major planes, the HNS
 // operand layout).  Out: [S][rows][Kp] int8 with Kp = 2*Kcp; for the left
-// operand (isB = 0) rows = npad, row i = [Re | Im]; for the right operand
-// rows = 2*npad, row 2j = [Re | -Im], row 2j+1 = [Im | Re].  ex[row of X] =
-// the power-of-two exponent.  One block of 256 threads per 32 rows.
-__global__ void __launch_bounds__(256) k_slice(const double2* __restrict__ X, int Kc, int Kcp, int npad, int np_out,
-                                               int S, int isB, int8_t* __restrict__ out, int* __restrict__ ex) {
+// operand (isB = 0) rows = np, row i = [Re | Im]; for the right operand
+// rows = 2*np, row 2j = [Re | -Im], row 2j+1 = [Im | Re].  ex[row of X] =
+// the power-of-two exponent of the row's largest component.
+// Row exponents for the slicing, in parallel over rows and K chunks:
+// ex[row] = max over k of ilogb(max(|Re|, |Im|)) + 1 (ex starts at a very
+// negative value, so all-zero rows keep a zero scale).  One thread per row,
+// 64 k per block.
+__global__ void __launch_bounds__(128) k_rowexp(const double2* __restrict__ X, int Kc, int npad,
+                                                int* __restrict__ ex) {
+  const int row = blockIdx.x * 128 + threadIdx.x;
+  const int k0 = blockIdx.y * 64;
+  if (row >= npad) return;
+  double m = 0.0;
+  for (int k = k0; k < min(Kc, k0 + 64); k++) {
+    const double2 v = X[(size_t)k * npad + row];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  if (m > 0.0) atomicMax(&ex[row], ilogb(m) + 1);
+}
+
+// FP64 -> int8 slices with the exponents of k_rowexp, one block per 32 rows
+// x 64 k: every output byte of [0, np) x [0, 2 Kcp) is written (zeros for
+// the padding rows and columns), so the operand buffers need no clearing.
+__global__ void __launch_bounds__(256) k_slice_rows(const double2* __restrict__ X, int Kc, int Kcp, int npad,
+                                                    int np_out, int S, int isB, const int* __restrict__ ex,
+                                                    int8_t* __restrict__ out) {
   __shared__ double2 tile[64][33];
-  __shared__ double red[8][32];
-  __shared__ int rexp[32];
-  const int r0 = blockIdx.x * 32;
+  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
   const int tid = threadIdx.x;
   const int Kp = 2 * Kcp;
-  // rows of one slice plane in the output (the tensor map's row extent)
   const size_t rows = isB ? 2 * (size_t)np_out : (size_t)np_out;
-  {
-    const int row = tid & 31, part = tid >> 5;
-    double m = 0.0;
-    for (int k = part; k < Kc; k += 8) {
-      double2 v = X[(size_t)k * npad + r0 + row];
-      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
-    }
-    red[part][row] = m;
-    __syncthreads();
-    if (tid < 32) {
-      double mm = 0.0;
-      for (int q = 0; q < 8; q++) mm = fmax(mm, red[q][tid]);
-      int e = (mm > 0.0) ? ilogb(mm) + 1 : 0;
-      rexp[tid] = e;
-      ex[r0 + tid] = e;
-    }
-    __syncthreads();
+  for (int q = tid; q < 64 * 32; q += 256) {
+    const int kk = q >> 5, r = q & 31;
+    const int k = k0 + kk, row = r0 + r;
+    tile[kk][r] = (k < Kc && row < npad) ? X[(size_t)k * npad + row] : make_double2(0.0, 0.0);
   }
+  __syncthreads();
   const int rr = tid >> 3;       // row within the block
   const int kq = (tid & 7) * 8;  // 8 consecutive k
-  const int e = rexp[rr];
-  for (int k0 = 0; k0 < Kcp; k0 += 64) {
-    for (int q = tid; q < 64 * 32; q += 256) {
-      int kk = q >> 5, r = q & 31;
-      int k = k0 + kk;
-      tile[kk][r] = (k < Kc) ? X[(size_t)k * npad + r0 + r] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
+  const int row = r0 + rr;
+  if (row >= np_out) return;
+  const int e = ex[row];
+  uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
 #pragma unroll
-    for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
+  for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
-      double2 v = tile[kq + t][rr];
-      double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
-#pragma unroll
-      for (int p = 0; p < L1G_MAX_SLICES; p++) {
-        if (p < S) {
-          double ar = rint(tr), ai = rint(ti);
-          tr = (tr - ar) * 128.0;
-          ti = (ti - ai) * 128.0;
-          pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
-          pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
-        }
-      }
-    }
-    const int col = k0 + kq;
-    const size_t row = (size_t)(r0 + rr);
+  for (int t = 0; t < 8; t++) {
+    const double2 v = tile[kq + t][rr];
+    double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
 #pragma unroll
     for (int p = 0; p < L1G_MAX_SLICES; p++) {
-      if (p >= S) break;
-      int8_t* base = out + (size_t)p * rows * Kp;
-      if (!isB) {
-        *(uint64_t*)(base + row * Kp + col) = pre[p];
-        *(uint64_t*)(base + row * Kp + Kcp + col) = pim[p];
-      } else {
-        // negate 8 packed int8 lanes: -x per byte (values within [-64, 64])
-        uint64_t nim = 0;
-#pragma unroll
-        for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
-        *(uint64_t*)(base + (2 * row) * Kp + col) = pre[p];
-        *(uint64_t*)(base + (2 * row) * Kp + Kcp + col) = nim;
-        *(uint64_t*)(base + (2 * row + 1) * Kp + col) = pim[p];
-        *(uint64_t*)(base + (2 * row + 1) * Kp + Kcp + col) = pre[p];
+      if (p < S) {
+        const double ar = rint(tr), ai = rint(ti);
+        tr = (tr - ar) * 128.0;
+        ti = (ti - ai) * 128.0;
+        pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
+        pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
       }
     }
-    __syncthreads();
+  }
+  const int col = k0 + kq;
+#pragma unroll
+  for (int p = 0; p < L1G_MAX_SLICES; p++) {
+    if (p >= S) break;
+    int8_t* base = out + (size_t)p * rows * Kp;
+    if (!isB) {
+      *(uint64_t*)(base + (size_t)row * Kp + col) = pre[p];
+      *(uint64_t*)(base + (size_t)row * Kp + Kcp + col) = pim[p];
+    } else {
+      uint64_t nim = 0;
+#pragma unroll
+      for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
+      *(uint64_t*)(base + (2 * (size_t)row) * Kp + col) = pre[p];
+      *(uint64_t*)(base + (2 * (size_t)row) * Kp + Kcp + col) = nim;
+      *(uint64_t*)(base + (2 * (size_t)row + 1) * Kp + col) = pim[p];
+      *(uint64_t*)(base + (2 * (size_t)row + 1) * Kp + Kcp + col) = pre[p];
+    }
   }
 }
 
@@ -361,16 +358,20 @@ static PFN_cuTensorMapEncodeTiled_v12000 l1g_encode_fn() {
   return fn;
 }
 
-static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t rows, uint64_t S, uint32_t box_rows) {
+// 3-D map over [S][rows][kp] int8 slice planes; a box is all S slices of
+// box_rows rows and `inner` bytes of K (64 with 64-byte swizzle, 32 with
+// 32-byte swizzle)
+static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t rows, uint64_t S, uint32_t box_rows,
+                       uint32_t inner = 64) {
   auto enc = l1g_encode_fn();
   if (!enc) return LAPW1GPU_ERR_CUDA;
   cuuint64_t dims[3] = {kp, rows, S};
   cuuint64_t strides[2] = {kp, kp * rows};
-  cuuint32_t box[3] = {64, box_rows, (cuuint32_t)S};
+  cuuint32_t box[3] = {inner, box_rows, (cuuint32_t)S};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, inner == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
@@ -387,16 +388,17 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
   int* exA = (int*)c->sbuf(set, "splitExA", sizeof(int) * np);
   int* exB = (int*)c->sbuf(set, "splitExB", sizeof(int) * np);
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
-  // rows in [npad, np) and the K padding stay zero
-  if (cudaMemsetAsync(A, 0, (size_t)S * np * Kp, s) != cudaSuccess ||
-      cudaMemsetAsync(B, 0, (size_t)S * 2 * np * Kp, s) != cudaSuccess ||
-      cudaMemsetAsync(exA, 0, sizeof(int) * np, s) != cudaSuccess ||
-      cudaMemsetAsync(exB, 0, sizeof(int) * np, s) != cudaSuccess)
+  // row exponents (0x80808080 bytes: a very negative start for atomicMax),
+  // then the slices of every row and column of the padded operands
+  if (cudaMemsetAsync(exA, 0x80, sizeof(int) * np, s) != cudaSuccess ||
+      cudaMemsetAsync(exB, 0x80, sizeof(int) * np, s) != cudaSuccess)
     return LAPW1GPU_ERR_CUDA;
-  // slice the real rows; the row count of X is npad (a multiple of 64, so of 32)
-  split::k_slice<<<npad / 32, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, S, 0, A, exA);
-  split::k_slice<<<npad / 32, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, S, 1, B, exB);
-  *nlaunch += 2;
+  const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
+  split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
+  split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
+  split::k_slice_rows<<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, S, 0, exA, A);
+  split::k_slice_rows<<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, S, 1, exB, B);
+  *nlaunch += 4;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;

@@ -33,7 +33,7 @@ EXPORTS = [
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
-    "lapw1gpu_set_tuning", "lapw1gpu_autotune",
+    "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices",
 ]
 
 _lib = None
@@ -68,6 +68,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_init.argtypes = [C.c_int, C.POINTER(vp)]
     lib.lapw1gpu_finalize.argtypes = [vp]
     lib.lapw1gpu_set_precision.argtypes = [vp, C.c_int, C.c_int]
+    lib.lapw1gpu_set_slices.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_kpoint_upload.argtypes = [vp, C.POINTER(CProblem), C.POINTER(vp)]
     lib.lapw1gpu_kpoint_free.argtypes = [vp]
     lib.lapw1gpu_kpoint_run.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(CStats)]
@@ -139,7 +140,7 @@ class KPoint:
 class Context:
     """A lapw1gpu context on one CUDA device."""
 
-    def __init__(self, device: int = 0, prec: int = PREC_FP64, slices: int = 6):
+    def __init__(self, device: int = 0, prec: int = PREC_FP64, slices: int = 5):
         self.lib = load()
         h = C.c_void_p()
         _check("lapw1gpu_init", self.lib.lapw1gpu_init(device, C.byref(h)))
@@ -147,9 +148,13 @@ class Context:
         self.device = device
         self.set_precision(prec, slices)
 
-    def set_precision(self, prec: int, slices: int = 6):
+    def set_precision(self, prec: int, slices: int = 5):
         _check("lapw1gpu_set_precision", self.lib.lapw1gpu_set_precision(self.h, prec, slices))
         self.prec, self.slices = prec, slices
+
+    def set_slices(self, slices_sph: int, slices_hns: int):
+        """split precision with separate slice counts (lapw1gpu_set_slices)"""
+        _check("lapw1gpu_set_slices", self.lib.lapw1gpu_set_slices(self.h, slices_sph, slices_hns))
 
     @property
     def stream_handle(self) -> int:

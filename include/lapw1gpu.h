@@ -159,8 +159,14 @@ typedef struct lapw1gpu_context lapw1gpu_context;
  * host thread and device. */
 int lapw1gpu_init(int device, lapw1gpu_context** ctx);
 int lapw1gpu_finalize(lapw1gpu_context* ctx);
-/* select the muffin-tin contraction arithmetic (LAPW1GPU_PREC_*) */
+/* select the muffin-tin contraction arithmetic (LAPW1GPU_PREC_*); with
+ * LAPW1GPU_PREC_SPLIT both the spherical part and HNS use `slices` int8
+ * slices (2..8; the spherical part runs on tensor cores for 4..7) */
 int lapw1gpu_set_precision(lapw1gpu_context* ctx, int prec, int slices);
+/* split precision with separate slice counts for the spherical part and
+ * for HNS (the non-spherical part is one to two orders of magnitude
+ * smaller, so it tolerates one slice fewer at the same eigenvalue error) */
+int lapw1gpu_set_slices(lapw1gpu_context* ctx, int slices_sph, int slices_hns);
 
 /* One k-point's inputs resident in device memory (uploaded once; the
  * benchmark's resident-input path and the k-point batch driver use it). */

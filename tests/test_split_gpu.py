@@ -54,18 +54,46 @@ def test_split_c1(sctx, slices):
     assert err["S"] <= TOL_H[slices] and err["H"] <= TOL_H[slices], err
 
 
+# SECLR4 solves inside the energy window EL..EU of case.in1 (seclr4.F:150-155);
+# the window here is [-10, 10] Ry
+EWIN = (-10.0, 10.0)
+
+
+def _window_eigs(hs, hsd):
+    w = sl.eigh(*hermitian_from_packed(hs, hsd), eigvals_only=True)
+    return w
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("slices", [5, 6, 7])
-def test_split_eigenvalues(sctx, slices):
-    """Generalized eigenvalues of the split-path H,S within 1e-6 Ry of the
-    FP64 oracle's (S = 5 is the fewest slices that meet the bound here)."""
+@pytest.mark.parametrize("case", ["lo6", "c0"])
+def test_split_eigenvalues(sctx, slices, case):
+    """Generalized eigenvalues of the split-path H,S inside the energy window
+    within 1e-6 Ry of the FP64 oracle's (S = 5 is the default)."""
     sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
-    p = synth.small_case("lo", rkmax=6.0)
+    p = synth.small_case("lo", rkmax=6.0) if case == "lo6" else synth.config("c0")[0]
     hs, hsd = sctx.setup(p)
     hs_o, hsd_o = O.setup(p)
-    w = sl.eigh(*hermitian_from_packed(hs, hsd), eigvals_only=True)
-    wo = sl.eigh(*hermitian_from_packed(hs_o, hsd_o), eigvals_only=True)
-    assert np.max(np.abs(w - wo)) <= 1e-6, np.max(np.abs(w - wo))
+    w, wo = _window_eigs(hs, hsd), _window_eigs(hs_o, hsd_o)
+    win = (wo > EWIN[0]) & (wo < EWIN[1])
+    assert win.sum() >= 0.9 * len(wo)
+    assert np.max(np.abs(w - wo)[win]) <= 1e-6, np.max(np.abs(w - wo)[win])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["lo6", "c0"])
+def test_mixed_slices_eigenvalues(sctx, case):
+    """Spherical part with 5 slices, HNS with 4: window eigenvalues within
+    1e-6 Ry of the FP64 oracle's."""
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    sctx.set_slices(5, 4)
+    p = synth.small_case("lo", rkmax=6.0) if case == "lo6" else synth.config("c0")[0]
+    hs, hsd = sctx.setup(p)
+    hs_o, hsd_o = O.setup(p)
+    w, wo = _window_eigs(hs, hsd), _window_eigs(hs_o, hsd_o)
+    win = (wo > EWIN[0]) & (wo < EWIN[1])
+    assert np.max(np.abs(w - wo)[win]) <= 1e-6, np.max(np.abs(w - wo)[win])
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
 
 
 @pytest.mark.gpu
