@@ -8,7 +8,8 @@ GPU the workload is the 40-atom 2x2x2 ABO3 supercell (RKmax 7, ~4950 basis
 functions, one LO per atom for l<=2, one general k).  With N GPUs each rank
 sets up its own k-point of the same cell (k-points are independent: weak
 scaling, no collective on the data path).  Prints ONE JSON line (rank 0).
-The default arithmetic is the split-precision path (5 int8 slices; the
+The default arithmetic is the split-precision path (5 int8 slices for the
+spherical part, 4 for HNS; the
 plain FP64 GPU path on the same k-point is timed beside it in
 `fp64_path`, with the split path's per-matrix error against it), after the
 autotuner has picked the tile/schedule parameters (untimed).  `batch` is a
@@ -225,11 +226,12 @@ def _rel_err(torch, a, b, n):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--prec", choices=["fp64", "split"], default="split")
     ap.add_argument("--slices", type=int, default=5)
-    ap.add_argument("--slices-hns", type=int, default=None, help="int8 slices of HNS (default: --slices)")
+    ap.add_argument("--slices-hns", type=int, default=4,
+                    help="int8 slices of HNS (the non-spherical part is 1-2 orders smaller than the spherical one)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
@@ -383,26 +385,42 @@ def main():
     # phase product, 4 per type to add PHASE * t into S and H
     f_sph = 2.0 * (6.0 * p.ltop * p.nat + 4.0 * p.ndf + 4.0 * p.nat) * pairs
     # HNS: complex rank-K update of the lower triangle, K = 2 NDF (lmax_ns+1)^2
-    f_hns = 8.0 * (2.0 * p.ndf * nsl2) * (n * (n + 1) / 2.0)
+    K_hns = 2.0 * p.ndf * nsl2
+    f_hns = 8.0 * K_hns * (n * (n + 1) / 2.0)
     split = args.prec == "split"
-    sph_name = "k_sph_tc spherical (K-b)" if split and tuning.get("sph_tc", 0) and 4 <= args.slices <= 7 \
-        else "k_spherical (K-b)"
-    kern = {sph_name: (f_sph, avg["ms_spherical"]), "HNS update (K-ns)": (f_hns, avg["ms_hns"])}
-    dom = max(kern, key=lambda k: kern[k][1])
-    fl, t_ms = kern[dom]
+    sph_tc = split and bool(tuning.get("sph_tc", 0)) and 4 <= args.slices <= 7
     fp64_peak = fp64_peak_tflops(torch, device)
-    on_tensor = split and (dom.startswith("HNS") or dom.startswith("k_sph_tc"))
-    if on_tensor:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
-        bound, peak = "tensor", 2.0 * peaks.get("bf16_tflops", 1590.0)
-        peak_src = ("2 x measured dense bf16 (the int8 tcgen05 rate), MEASURED_PEAKS.json; achieved counts "
-                    "FP64-equivalent flops, so frac understates the int8 slice-product rate by the products per MAC")
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+    int8_peak = 2.0 * peaks.get("bf16_tflops", 1590.0)  # dense int8 tcgen05 rate = 2 x dense bf16
+    # algorithmic work of each main kernel: FP64 flops, or int8 slice-product
+    # ops (2 per MAC; S(S+1)/2 products per real MAC of the complex product)
+    prods = lambda S: S * (S + 1) / 2.0
+    kern = {}
+    if sph_tc:
+        # per pair and l: 4 real outputs (S, H re/im) x 2 K_c real MACs, K_c = 2 NDF
+        ops = 2.0 * pairs * p.ltop * 4.0 * (2.0 * 2 * p.ndf) * prods(args.slices)
+        kern["k_sph_tc (K-b, tcgen05)"] = ("tensor", ops, avg.get("ms_sph_main", 0.0), f_sph)
     else:
-        bound, peak = "fp64", fp64_peak
+        kern["k_spherical (K-b, FP64)"] = ("fp64", f_sph, avg.get("ms_sph_main", 0.0), f_sph)
+    if split:
+        # per lower-triangle element: 2 real outputs x 2 K real MACs
+        ops = 2.0 * (n * (n + 1) / 2.0) * 4.0 * K_hns * prods(slices_hns)
+        kern["k_split_gemm (K-ns, tcgen05)"] = ("tensor", ops, avg.get("ms_hns_main", 0.0), f_hns)
+    else:
+        kern["HNS update (K-ns, FP64: k_hns_gemm + ZGEMM panels)"] = ("fp64", f_hns, avg.get("ms_hns_main", 0.0),
+                                                                     f_hns)
+    dom = max(kern, key=lambda k: kern[k][2])
+    bound, work, t_ms, f64eq = kern[dom]
+    if bound == "tensor":
+        unit, peak = "TOP/s", int8_peak
+        peak_src = ("2 x measured dense bf16 TFLOP/s (MEASURED_PEAKS.json) = the dense int8 tcgen05 rate; "
+                    "achieved counts the int8 slice-product ops the kernel must execute")
+    else:
+        unit, peak = "TFLOP/s", fp64_peak
         peak_src = ("measured here: cuBLAS DGEMM 8192^3, best of 5 (MEASURED_PEAKS.json has no FP64 figure); "
                     "FP64 FMA pipe, not tensor cores or HBM")
-    achieved = fl / (t_ms * 1e-3) / 1e12
+    achieved = work / (t_ms * 1e-3) / 1e12 if t_ms > 0 else None
     traffic = None
     tj = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tj):
@@ -431,12 +449,17 @@ def main():
         "stage_ms": {k: v for k, v in avg.items() if k.startswith("ms_")},
         "tuning": tuning,
         "roofline": {"kernel": dom, "bound": bound,
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "peak_source": peak_src, "flops_per_launch": fl, "ms_per_launch": t_ms,
-                     "fp64_peak_tflops": fp64_peak,
-                     "kernels": {k: {"flops": f, "ms": t, "tflops": f / (t * 1e-3) / 1e12,
-                                     "frac_fp64": f / (t * 1e-3) / 1e12 / fp64_peak} for k, (f, t) in kern.items()}},
+                     "achieved": achieved, "peak": peak, "unit": unit,
+                     "frac": achieved / peak if (peak and achieved) else None, "traffic": traffic,
+                     "peak_source": peak_src, "work_per_launch": work, "ms_per_launch": t_ms,
+                     "fp64_equiv_tflops": f64eq / (t_ms * 1e-3) / 1e12 if t_ms > 0 else None,
+                     "fp64_peak_tflops": fp64_peak, "int8_peak_tops": int8_peak,
+                     "kernels": {k: {"bound": b, "work": w, "ms": t,
+                                     "achieved": w / (t * 1e-3) / 1e12 if t > 0 else None,
+                                     "frac": (w / (t * 1e-3) / 1e12) / (int8_peak if b == "tensor" else fp64_peak)
+                                     if t > 0 else None,
+                                     "fp64_equiv_tflops": f / (t * 1e-3) / 1e12 if t > 0 else None}
+                                 for k, (b, w, t, f) in kern.items()}},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks,

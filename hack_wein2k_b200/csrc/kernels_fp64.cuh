@@ -665,36 +665,50 @@ __global__ void __launch_bounds__(256) k_hns_tmul(int npad, int nsl2, const int*
 }
 
 // LO rows: A2 += TUU21 conj(CLM), B2 += TUD21 conj(CLM),
-// C2 = TUU12 conj(ALM) + TDU12 conj(BLM) + TUU22 conj(CLM)  (hns.F:391-433)
-__global__ void k_hns_lo_ops(DevProb P, const double2* __restrict__ tns, double2* __restrict__ Lop,
-                             const double2* __restrict__ Rop, const double2* __restrict__ Clo,
-                             double2* __restrict__ C2lo) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;  // LO row index
+// C2 = TUU12 conj(ALM) + TDU12 conj(BLM) + TUU22 conj(CLM)  (hns.F:391-433).
+// One thread per (LO row, atom, la): block (32 la, 8 rows), the rows' ALM,
+// BLM, CLM staged in shared memory.
+__global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __restrict__ tns,
+                                                    double2* __restrict__ Lop, const double2* __restrict__ Rop,
+                                                    const double2* __restrict__ Clo, double2* __restrict__ C2lo) {
+  __shared__ double2 sX[8][3][L1G_NSL2];
+  const int la = threadIdx.x, cy = threadIdx.y;
+  const int c = blockIdx.x * 8 + cy;  // LO row index
   const int a = blockIdx.y;
-  if (c >= P.nlo) return;
   const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
-  const size_t npad = P.npad, i = P.nv + c;
-  const double2* T = tns + (size_t)P.atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  const double2* RA = Rop + ((size_t)(a * 2 + 0) * nsl2) * npad + i;
-  const double2* RB = Rop + ((size_t)(a * 2 + 1) * nsl2) * npad + i;
-  const double2* CL = Clo + (size_t)a * nsl2 * P.nlo + c;
-  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2) * npad + i;
-  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2) * npad + i;
-  for (int la = 0; la < nsl2; la++) {
-    double2 da = cmk(0, 0), db = cmk(0, 0), dc = cmk(0, 0);
-    for (int b = 0; b < nsl2; b++) {
-      const double2 A = RA[b * npad], B = RB[b * npad], Cc = CL[(size_t)b * P.nlo];
-#define TT(blk) T[((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b]
-      const double2 tuu21 = TT(2), tud21 = TT(5), tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
-#undef TT
-      da = cadd(da, cmul(tuu21, cconj(Cc)));
-      db = cadd(db, cmul(tud21, cconj(Cc)));
-      dc = cadd(dc, cadd(cadd(cmul(tuu12, cconj(A)), cmul(tdu12, cconj(B))), cmul(tuu22, cconj(Cc))));
+  const size_t npad = P.npad;
+  for (int q = threadIdx.y * 32 + threadIdx.x; q < 8 * 3 * nsl2; q += 256) {
+    const int r = q / (3 * nsl2), w = (q / nsl2) % 3, b = q % nsl2;
+    const int cc = blockIdx.x * 8 + r;
+    double2 v = cmk(0.0, 0.0);
+    if (cc < P.nlo) {
+      const size_t i = P.nv + cc;
+      if (w < 2)
+        v = Rop[((size_t)(a * 2 + w) * nsl2 + b) * npad + i];
+      else
+        v = Clo[((size_t)a * nsl2 + b) * P.nlo + cc];
     }
-    LA[la * npad] = cadd(LA[la * npad], da);
-    LB[la * npad] = cadd(LB[la * npad], db);
-    C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc;
+    sX[r][w][b] = v;
   }
+  __syncthreads();
+  if (c >= P.nlo || la >= nsl2) return;
+  const double2* T = tns + (size_t)P.atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  double2 da = cmk(0, 0), db = cmk(0, 0), dc = cmk(0, 0);
+  for (int b = 0; b < nsl2; b++) {
+    const double2 A = sX[cy][0][b], B = sX[cy][1][b], Cc = sX[cy][2][b];
+#define TT(blk) __ldg(T + ((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b)
+    const double2 tuu21 = TT(2), tud21 = TT(5), tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
+#undef TT
+    da = cadd(da, cmul(tuu21, cconj(Cc)));
+    db = cadd(db, cmul(tud21, cconj(Cc)));
+    dc = cadd(dc, cadd(cadd(cmul(tuu12, cconj(A)), cmul(tdu12, cconj(B))), cmul(tuu22, cconj(Cc))));
+  }
+  const size_t i = P.nv + c;
+  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2 + la) * npad + i;
+  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2 + la) * npad + i;
+  *LA = cadd(*LA, da);
+  *LB = cadd(*LB, db);
+  C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc;
 }
 
 // HS(i,j) += sum_k Lop[k][i] * Rop[k][j] on the lower triangle i >= j

@@ -34,13 +34,30 @@ struct DevBuf {
 }  // namespace
 
 #define L1G_MAX_SETS 4  // concurrent k-point chains in a batch (scratch sets)
+#define L1G_MAX_GROUPS 16
+
+// Column groups of HS: the spherical contraction and the HNS update run
+// group by group, each group followed by an event, so that a caller can
+// copy finished columns of HS while later groups run.  With fixed set, the
+// caller chose the boundaries (multiples of every stage's tile width);
+// otherwise (HNS only) the HNS stage picks them.  groups = 0: one pass.
+struct HnsPipe {
+  int groups = 0;
+  bool fixed = false;
+  int col[L1G_MAX_GROUPS + 1] = {};  // group g covers columns [col[g], col[g+1])
+  cudaEvent_t ev[L1G_MAX_GROUPS] = {};   // HNS of group g done
+  bool recorded[L1G_MAX_GROUPS] = {};
+  cudaEvent_t sev[L1G_MAX_GROUPS] = {};  // S (upper triangle) of group g final
+  bool srec[L1G_MAX_GROUPS] = {};
+};
 
 struct lapw1gpu_context {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side[L1G_MAX_SETS] = {};  // streams of scratch sets 1.. in a batch
-  cudaEvent_t ev[12] = {};
+  cudaEvent_t ev[16] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels
   cudaEvent_t fork = nullptr, join[L1G_MAX_SETS] = {};
+  cudaEvent_t hns_ev[L1G_MAX_GROUPS] = {}, sph_ev[L1G_MAX_GROUPS] = {};
   int* d_status = nullptr;
   int last_status = 0;
   int prec = LAPW1GPU_PREC_FP64;
@@ -111,8 +128,6 @@ struct lapw1gpu_context {
   }
 };
 
-#include "split_tc.cuh"
-#include "sph_tc.cuh"
 
 struct lapw1gpu_kpoint {
   lapw1gpu_context* ctx = nullptr;
@@ -169,6 +184,9 @@ static const int2* kp_tiles(lapw1gpu_kpoint* k, const std::string& key, int* cou
   *count = (int)t.size();
   return d;
 }
+
+#include "split_tc.cuh"
+#include "sph_tc.cuh"
 
 namespace {
 
@@ -249,6 +267,8 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
   cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+  for (auto& e : c->hns_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  for (auto& e : c->sph_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (int i = 1; i < L1G_MAX_SETS; i++) {
     cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming);
@@ -276,6 +296,8 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   if (c->d_status) cudaFree(c->d_status);
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaEventDestroy(c->fork);
+  for (auto& e : c->hns_ev) cudaEventDestroy(e);
+  for (auto& e : c->sph_ev) cudaEventDestroy(e);
   for (int i = 1; i < L1G_MAX_SETS; i++) {
     cudaEventDestroy(c->join[i]);
     cudaStreamDestroy(c->side[i]);
@@ -591,7 +613,7 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
   k_hns_tmul<<<dim3(P.npad / TMUL_I, P.ndf), 256, TMUL_SMEM, s>>>(P.npad, nsl2, P.atype, tns, Rop, Lop);
   *nl += 2;
   if (P.nlo > 0) {
-    k_hns_lo_ops<<<dim3((P.nlo + 127) / 128, P.ndf), 128, 0, s>>>(P, tns, Lop, Rop, Clo, C2lo);
+    k_hns_lo_ops<<<dim3((P.nlo + 7) / 8, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo, C2lo);
     *nl += 1;
   }
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
@@ -611,19 +633,30 @@ static const int2* tiles_hns_diag(lapw1gpu_kpoint* k, int n, int B, int* count) 
   });
 }
 
-static int hns_panels_zgemm(cublasHandle_t h, int n, int npad, int K, int B, const double2* Lop, const double2* Rop,
-                            double2* hs, int ld) {
+// (hp: after the panels of each column group, its event; groups whose
+// columns reach the LO block are left for the caller to record)
+static int hns_panels_zgemm(cublasHandle_t h, int n, int nv, int npad, int K, int B, const double2* Lop,
+                            const double2* Rop, double2* hs, int ld, cudaStream_t s, HnsPipe* hp) {
   if (!h) return LAPW1GPU_ERR_CUDA;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  if (hp && hp->groups > 0 && !hp->fixed) {  // groups of whole panels
+    const int np = (n + B - 1) / B, G = std::min(hp->groups, np);
+    hp->groups = G;
+    for (int g = 0; g <= G; g++) hp->col[g] = std::min(n, (int)((long)np * g / G) * B);
+  }
+  int g = 0;
   for (int c0 = 0; c0 < n; c0 += B) {
     const int w = std::min(B, n - c0);
     const int r0 = c0 + w, m = n - r0;
-    if (m <= 0) continue;
     // HS(r0:n, c0:c0+w) += L(r0:n, :) R(c0:c0+w, :)^T ; L, R column-major npad x K
-    if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, m, w, K, &one, (const cuDoubleComplex*)(Lop + r0), npad,
-                    (const cuDoubleComplex*)(Rop + c0), npad, &one, (cuDoubleComplex*)(hs + (size_t)c0 * ld + r0),
-                    ld) != CUBLAS_STATUS_SUCCESS)
+    if (m > 0 && cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, m, w, K, &one, (const cuDoubleComplex*)(Lop + r0), npad,
+                             (const cuDoubleComplex*)(Rop + c0), npad, &one,
+                             (cuDoubleComplex*)(hs + (size_t)c0 * ld + r0), ld) != CUBLAS_STATUS_SUCCESS)
       return LAPW1GPU_ERR_CUDA;
+    if (hp && g < hp->groups && r0 >= hp->col[g + 1]) {
+      if (hp->col[g + 1] <= nv && cudaEventRecord(hp->ev[g], s) == cudaSuccess) hp->recorded[g] = true;
+      g++;
+    }
   }
   return LAPW1GPU_OK;
 }
@@ -634,7 +667,8 @@ static int hns_panels_zgemm(cublasHandle_t h, int n, int npad, int K, int B, con
 // one CTA per (128 J, IT I) tile of the triangle.
 template <int S, bool PAIR>
 static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
-                         const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
+                         const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
+                         const cudaEvent_t* ev, HnsPipe* sp) {
   using Cf = sphtc::Cfg<S>;
   const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
   const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;  // Kp: whole 64-byte K blocks
@@ -646,9 +680,9 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
   const int sl_smem = Kc * 33 * (int)sizeof(double2);
   if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
-  if (!c->smem((const void*)sphtc::k_sph_slice, sl_smem)) return LAPW1GPU_ERR_CUDA;
-  sphtc::k_sph_slice<<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, S, A, exA);
-  sphtc::k_sph_slice<<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, S, B, exB);
+  if (!c->smem((const void*)sphtc::k_sph_slice<S>, sl_smem)) return LAPW1GPU_ERR_CUDA;
+  sphtc::k_sph_slice<S><<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, A, exA);
+  sphtc::k_sph_slice<S><<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, B, exB);
   *nl += 2;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, 64) ||
@@ -667,9 +701,31 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
                             });
   if (!dt) return LAPW1GPU_ERR_NOMEM;
   if (!c->smem((const void*)sphtc::k_sph_tc<S, PAIR>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
-  sphtc::k_sph_tc<S, PAIR><<<ntile, Cf::THREADS, Cf::SMEM, s>>>(ta, tb, P, dt, Kp / 64, npA, npB, exA, exB, tab,
-                                                                k->tab, hs, ld, hsdiag, c->d_status);
-  *nl += 1;
+  if (ev && cudaEventRecord(ev[0], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
+  // tiles are ordered by the I tile (column of S); per I tile bi the J tiles
+  // bj with bj 128 <= bi IT + IT - 1, so a column group is a contiguous range
+  const int nbj = npA / 128, nbi = npB / Cf::IT;
+  auto first_tile = [&](int bi) {  // tiles before I tile bi
+    long t = 0;
+    for (int b = 0; b < bi; b++) t += std::min(nbj, (b * Cf::IT + Cf::IT - 1) / 128 + 1);
+    return t;
+  };
+  const int G = sp ? sp->groups : 1;
+  for (int g = 0; g < G; g++) {
+    const int b0 = sp ? std::min(nbi, sp->col[g] / Cf::IT) : 0;
+    const int b1 = sp ? (g == G - 1 ? nbi : std::min(nbi, sp->col[g + 1] / Cf::IT)) : nbi;
+    const long t0 = first_tile(b0), t1 = (g == G - 1) ? ntile : first_tile(b1);
+    if (t1 > t0) {
+      sphtc::k_sph_tc<S, PAIR><<<(unsigned)(t1 - t0), Cf::THREADS, Cf::SMEM, s>>>(
+          ta, tb, P, dt + t0, Kp / 64, npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag, c->d_status);
+      *nl += 1;
+    }
+    if (sp && sp->col[g + 1] <= k->nv) {
+      if (cudaEventRecord(sp->sev[g], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
+      sp->srec[g] = true;
+    }
+  }
+  if (ev && cudaEventRecord(ev[1], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
@@ -685,13 +741,14 @@ static bool sph_pair_ok(int S, int Kp) {
 static bool sph_tc_supported(int S) { return S >= 4 && S <= 7; }
 
 static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
-                           const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl) {
+                           const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
+                           const cudaEvent_t* ev, HnsPipe* sp) {
   const int Kp = 2 * round_up(2 * k->ndf, 32);
   const bool pair = sph_pair_ok(c->slices, Kp);
 #define SPH_CASE(SS)                                                                        \
   case SS:                                                                                  \
-    return pair ? sph_tc_launch<SS, true>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl)   \
-                : sph_tc_launch<SS, false>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl);
+    return pair ? sph_tc_launch<SS, true>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp)   \
+                : sph_tc_launch<SS, false>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp);
   switch (c->slices) {
     SPH_CASE(4)
     SPH_CASE(5)
@@ -719,14 +776,19 @@ static double alg_flops(const lapw1gpu_kpoint* k) {
 // is limited to launches: every buffer and tile list already exists when
 // the same k-point ran once before, so the sequence can be captured.
 static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, double2* d_hs, int ldhs,
-                           double2* d_hsdiag, cudaStream_t s, int set, const cudaEvent_t* ev, int* nlaunch) {
+                           double2* d_hsdiag, cudaStream_t s, int set, const cudaEvent_t* ev, int* nlaunch,
+                           HnsPipe* hp = nullptr) {
   DevProb P = k->P;
   const int n = k->n, nv = k->nv, ltop = k->ltop, ndf = k->ndf, nat = k->nat;
   P.al = (double*)c->sbuf(set, "al", sizeof(double) * (size_t)nat * ltop * k->nvpad);
   P.bl = (double*)c->sbuf(set, "bl", sizeof(double) * (size_t)nat * ltop * k->nvpad);
   P.phase = (double2*)c->sbuf(set, "phase", sizeof(double2) * (size_t)ndf * k->npad);
   if (!P.al || !P.bl || !P.phase) return LAPW1GPU_ERR_NOMEM;
-  if (ev) CK(cudaEventRecord(ev[0], s));
+  if (ev) {
+    // main-kernel events start equal, so a stage that does not run reads 0
+    for (int q = 12; q < 16; q++) CK(cudaEventRecord(ev[q], s));
+    CK(cudaEventRecord(ev[0], s));
+  }
   int nl = 0;  // kernels launched by this run
 
   // ---- K-a: matching coefficients and phases (always needed) ----
@@ -747,16 +809,35 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     k_table<<<(unsigned)((ntab + 127) / 128), 128, 0, s>>>(P, k->tab, k->d_warp, tab);
     nl++;
     k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
+    // column groups of the spherical contraction (the caller's boundaries)
+    HnsPipe* sp = (hp && hp->fixed && hp->groups > 0) ? hp : nullptr;
     if (c->prec == LAPW1GPU_PREC_SPLIT && c->sph_tc && sph_tc_supported(c->slices)) {
-      int rc = sph_tc_dispatch(c, k, set, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl);
+      int rc = sph_tc_dispatch(c, k, set, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl, ev ? ev + 12 : nullptr, sp);
       if (rc) return rc;
     } else {
       int ntiles = 0;
       const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
       if (!tl) return LAPW1GPU_ERR_NOMEM;
       if (!c->smem((const void*)k_spherical, SPH_DYN_SMEM)) return LAPW1GPU_ERR_CUDA;
-      nl++;
-      k_spherical<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, tab, k->tab, d_hs, ldhs, d_hsdiag);
+      if (ev) CK(cudaEventRecord(ev[12], s));
+      // tiles are ordered by the I tile (column of S), bi (bi + 1) / 2 before tile row bi
+      const int nbi = (nv + SPH_T - 1) / SPH_T;
+      const int G = sp ? sp->groups : 1;
+      for (int g = 0; g < G; g++) {
+        const int b0 = sp ? std::min(nbi, sp->col[g] / SPH_T) : 0;
+        const int b1 = sp ? (g == G - 1 ? nbi : std::min(nbi, sp->col[g + 1] / SPH_T)) : nbi;
+        const long t0 = (long)b0 * (b0 + 1) / 2, t1 = (long)b1 * (b1 + 1) / 2;
+        if (t1 > t0) {
+          nl++;
+          k_spherical<<<(unsigned)(t1 - t0), SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl + t0, coef, tab, k->tab, d_hs,
+                                                                             ldhs, d_hsdiag);
+        }
+        if (sp && sp->col[g + 1] <= nv) {
+          CK(cudaEventRecord(sp->sev[g], s));
+          sp->srec[g] = true;
+        }
+      }
+      if (ev) CK(cudaEventRecord(ev[13], s));
     }
     CK(cudaGetLastError());
     if (ev) CK(cudaEventRecord(ev[2], s));
@@ -766,6 +847,12 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
       k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag);
     }
     CK(cudaGetLastError());
+    if (sp)  // groups whose columns reach the LO columns are final after k_lo
+      for (int g = 0; g < sp->groups; g++)
+        if (!sp->srec[g]) {
+          CK(cudaEventRecord(sp->sev[g], s));
+          sp->srec[g] = true;
+        }
     if (ev) CK(cudaEventRecord(ev[3], s));
   } else if (ev) {
     CK(cudaEventRecord(ev[2], s));
@@ -785,14 +872,17 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
     if (rc) return rc;
     if (c->prec == LAPW1GPU_PREC_SPLIT)
-      rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl);
+      rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl, hp,
+                          ev ? ev + 14 : nullptr);
     else {
       int ntiles = 0;
       const int2* tl = tiles_hns_diag(k, n, c->hns_diag_b, &ntiles);
       if (!tl) return LAPW1GPU_ERR_NOMEM;
       nl++;
+      if (ev) CK(cudaEventRecord(ev[14], s));
       k_hns_gemm<<<ntiles, 256, 0, s>>>(n, k->npad, K, tl, Lop, Rop, d_hs, ldhs);
-      rc = hns_panels_zgemm(c->handle(set, s), n, k->npad, K, c->hns_diag_b, Lop, Rop, d_hs, ldhs);
+      rc = hns_panels_zgemm(c->handle(set, s), n, nv, k->npad, K, c->hns_diag_b, Lop, Rop, d_hs, ldhs, s, hp);
+      if (ev && !rc) CK(cudaEventRecord(ev[15], s));
     }
     if (rc) return rc;
     if (k->nlo > 0) {
@@ -810,6 +900,12 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
       k_add_lower<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, T, d_hs, ldhs);
     }
     CK(cudaGetLastError());
+    if (hp)  // the groups whose columns reach the LO block end here
+      for (int g = 0; g < hp->groups; g++)
+        if (!hp->recorded[g]) {
+          CK(cudaEventRecord(hp->ev[g], s));
+          hp->recorded[g] = true;
+        }
   }
   if (ev) CK(cudaEventRecord(ev[4], s));
 
@@ -853,6 +949,13 @@ static void fill_stats(lapw1gpu_context* c, const lapw1gpu_kpoint* k, int nl, la
   st->ms_total = tot;
   st->flops_fp64_equiv = alg_flops(k);
   st->kernel_launches = nl;
+  // main contraction kernels: events 12-13 and 14-15 (absent stages read 0)
+  float a = 0.f, b = 0.f;
+  if (cudaEventQuery(c->ev[13]) == cudaSuccess && cudaEventElapsedTime(&a, c->ev[12], c->ev[13]) == cudaSuccess)
+    st->ms_sph_main = a;
+  if (cudaEventQuery(c->ev[15]) == cudaSuccess && cudaEventElapsedTime(&b, c->ev[14], c->ev[15]) == cudaSuccess)
+    st->ms_hns_main = b;
+  cudaGetLastError();
 }
 
 extern "C" {
@@ -1043,6 +1146,30 @@ int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, in
   return LAPW1GPU_OK;
 }
 
+// Column widths of one tile of the spherical and HNS contractions under
+// the context's settings (group boundaries must be multiples of both).
+static int sph_granule(const lapw1gpu_context* c) {
+  if (c->prec == LAPW1GPU_PREC_SPLIT && c->sph_tc && sph_tc_supported(c->slices)) switch (c->slices) {
+      case 4: return sphtc::Cfg<4>::IT;
+      case 5: return sphtc::Cfg<5>::IT;
+      case 6: return sphtc::Cfg<6>::IT;
+      default: return sphtc::Cfg<7>::IT;
+    }
+  return SPH_T;
+}
+static int hns_granule(const lapw1gpu_context* c) {
+  if (c->prec != LAPW1GPU_PREC_SPLIT) return c->hns_diag_b;
+  switch (c->slices_hns) {
+    case 2: return split::Cfg<2>::JT;
+    case 3: return split::Cfg<3>::JT;
+    case 4: return split::Cfg<4>::JT;
+    case 5: return split::Cfg<5>::JT;
+    case 6: return split::Cfg<6>::JT;
+    case 7: return split::Cfg<7>::JT;
+    default: return split::Cfg<8>::JT;
+  }
+}
+
 // Host-buffer form.  When HAMILT runs together with HNS/HORB, the copy of
 // S back to the host overlaps them: S (the strict upper triangle) and
 // HSDIAG are final once HAMILT is done, and the later stages only touch the
@@ -1078,11 +1205,65 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
   CK(cudaEventRecord(e1, s));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
   int nl = 0;
-  rc = kpoint_run_impl(c, k, stages, d_hs, n, d_hd, s, 0, c->ev, &nl);
+  const bool overlap = (stages & 1) && (stages & 6);
+  // HNS in column groups, so that the lower triangle follows group by group
+  // (not with HORB, which adds to every column after HNS)
+  HnsPipe hp;
+  const bool pipe = overlap && (stages & 2) && !k->nohns && !((stages & 4) && !k->orbs.empty());
+  if (pipe) {
+    // about 8 groups of columns, boundaries on a multiple of both tile widths
+    const int a = sph_granule(c), b = hns_granule(c);
+    int gcd = a, r = b;
+    while (r) {
+      const int t = gcd % r;
+      gcd = r;
+      r = t;
+    }
+    const long gran = (long)a / gcd * b;
+    int G = 0;
+    hp.col[0] = 0;
+    for (int g = 1; g < 8; g++) {
+      const int cb = (int)(((long)n * g / 8) / gran * gran);
+      if (cb > hp.col[G] && cb < n) hp.col[++G] = cb;
+    }
+    hp.col[++G] = n;
+    hp.groups = G;
+    hp.fixed = true;
+  }
+  for (int g = 0; g < L1G_MAX_GROUPS; g++) {
+    hp.ev[g] = c->hns_ev[g];
+    hp.sev[g] = c->sph_ev[g];
+  }
+  rc = kpoint_run_impl(c, k, stages, d_hs, n, d_hd, s, 0, c->ev, &nl, pipe ? &hp : nullptr);
   if (rc == LAPW1GPU_OK) {
     CK(cudaEventRecord(e2, s));
-    const bool overlap = (stages & 1) && (stages & 6);
-    if (overlap) {
+    bool grouped = pipe && hp.groups > 0 && hp.col[hp.groups] == n;
+    for (int g = 0; grouped && g < hp.groups; g++) grouped = hp.recorded[g] && hp.srec[g];
+    if (grouped) {
+      // S above each group's columns as soon as the group's spherical tiles
+      // (and, for the last groups, the LO columns) are done, HSDIAG after
+      // HAMILT, then the rest of each group's columns after its HNS update
+      for (int g = 0; g < hp.groups; g++) {
+        const int a = hp.col[g], w = hp.col[g + 1] - a;
+        CK(cudaStreamWaitEvent(cs, hp.sev[g], 0));
+        if (a > 0 && w > 0 &&
+            cudaMemcpy2DAsync(hs + (size_t)a * ldhs, z * ldhs, d_hs + (size_t)a * n, z * n, z * a, w,
+                              cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+          rc = LAPW1GPU_ERR_CUDA;
+      }
+      CK(cudaStreamWaitEvent(cs, c->ev[3], 0));
+      if (cudaMemcpyAsync(hsdiag, d_hd, z * n, cudaMemcpyDeviceToHost, cs) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+      for (int g = 0; g < hp.groups; g++) {
+        const int a = hp.col[g], w = hp.col[g + 1] - a;
+        if (w <= 0) continue;
+        CK(cudaStreamWaitEvent(cs, hp.ev[g], 0));
+        if (cudaMemcpy2DAsync(hs + (size_t)a * ldhs + a, z * ldhs, d_hs + (size_t)a * n + a, z * n, z * (n - a), w,
+                              cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+          rc = LAPW1GPU_ERR_CUDA;
+      }
+      CK(cudaEventRecord(ecp, cs));
+      CK(cudaStreamWaitEvent(s, ecp, 0));
+    } else if (overlap) {
       // c->ev[3] marks the end of HAMILT (+ LO columns) on s
       CK(cudaStreamWaitEvent(cs, c->ev[3], 0));
       for (int c0 = L1G_D2H_PANEL; c0 < n; c0 += L1G_D2H_PANEL) {
@@ -1094,11 +1275,11 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
       if (cudaMemcpyAsync(hsdiag, d_hd, z * n, cudaMemcpyDeviceToHost, cs) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
       CK(cudaEventRecord(ecp, cs));
     }
-    if (!overlap) {
+    if (!grouped && !overlap) {
       if (cudaMemcpy2DAsync(hs, z * ldhs, d_hs, z * n, z * n, n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaMemcpyAsync(hsdiag, d_hd, z * n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
         rc = LAPW1GPU_ERR_CUDA;
-    } else {
+    } else if (!grouped) {
       for (int c0 = 0; c0 < n; c0 += L1G_D2H_PANEL) {
         const int w = std::min(L1G_D2H_PANEL, n - c0);
         // rows [c0, n) of the panel (the first panel: all rows)

@@ -42,6 +42,7 @@ using split::tma_load_3d;
 template <int S>
 struct Cfg {
   static constexpr int N = ((512 / (2 * S)) / 16) * 16;  // real columns per accumulator buffer
+  static_assert(S * N <= 256, "one MMA per A slice needs (S - p) N <= 256 columns");
   static constexpr int IT = N / 4;                        // I per tile
   // one pipeline stage: all S slices of a 64-byte K block of A (128 rows)
   // and of B (N rows)
@@ -63,8 +64,9 @@ struct Cfg {
 // [Re v | Im v] and 2c+1 = [-Im v | Re v], so that a real dot product with
 // [Re u | Im u] gives Re and Im of u conj(v).  out: [S][L][rows][Kp] int8,
 // Kp = 2 Kcp; ex: [L][complex rows] exponents.  32 complex rows per block.
-__global__ void __launch_bounds__(256) k_sph_slice(DevProb P, const SphCoef* __restrict__ coef, int isB, int Kcp,
-                                                   int ncrow, int S, int8_t* __restrict__ out, int* __restrict__ ex) {
+template <int S>
+__global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* __restrict__ coef, int isB, int Kcp,
+                                                      int ncrow, int8_t* __restrict__ out, int* __restrict__ ex) {
   extern __shared__ double2 tile[];  // [Kc][33]
   __shared__ double red[8][32];
   __shared__ int rexp[32];
@@ -125,28 +127,25 @@ __global__ void __launch_bounds__(256) k_sph_slice(DevProb P, const SphCoef* __r
   for (int k0 = 0; k0 < Kcp; k0 += 64) {
     const int col = k0 + kq;
     if (col >= Kcp || rc >= ncrow) continue;
-    uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
+    uint64_t pre[S], pim[S];
 #pragma unroll
-    for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
+    for (int p = 0; p < S; p++) pre[p] = pim[p] = 0;
 #pragma unroll
     for (int t = 0; t < 8; t++) {
       const int k = col + t;
       const double2 v = (k < Kc) ? tile[k * 33 + rr] : make_double2(0.0, 0.0);
       double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
 #pragma unroll
-      for (int p = 0; p < L1G_MAX_SLICES; p++) {
-        if (p < S) {
-          const double ar = rint(tr), ai = rint(ti);
-          tr = (tr - ar) * 128.0;
-          ti = (ti - ai) * 128.0;
-          pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
-          pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
-        }
+      for (int p = 0; p < S; p++) {
+        const double ar = rint(tr), ai = rint(ti);
+        tr = (tr - ar) * 128.0;
+        ti = (ti - ai) * 128.0;
+        pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
+        pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
       }
     }
 #pragma unroll
-    for (int p = 0; p < L1G_MAX_SLICES; p++) {
-      if (p >= S) break;
+    for (int p = 0; p < S; p++) {
       int8_t* base = out + (size_t)p * plane + (size_t)l * nrow_real * Kp;
       if (!isB) {
         *(uint64_t*)(base + (size_t)rc * Kp + col) = pre[p];
@@ -241,7 +240,6 @@ __global__ void __launch_bounds__(288, 1)
 
   if (warp == 8) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_i8(128, N);
       const int nit = L * nkb;
       int issued = 0;
       bool ok = true;
@@ -267,23 +265,25 @@ __global__ void __launch_bounds__(288, 1)
         tc_fence_after();
         const uint32_t a0 = smem_u32(smem + st * C::STAGE);
         const uint32_t b0 = a0 + C::A_BYTES;
+        // The S slices of B lie one after another in shared memory (one
+        // (S N)-row K-major tile) and the level accumulators N columns
+        // apart in TMEM, so A slice p times B slices 0..S-1-p is ONE MMA
+        // of width (S-p) N whose columns land on levels p..S-1.
 #pragma unroll
         for (int p = 0; p < S; p++)
 #pragma unroll
-          for (int q = 0; q < S - p; q++)
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
-              const uint64_t bd = desc_sw64(b0 + q * N * 64 + h * 32);
-              const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
-              const uint32_t d = tmem + (uint32_t)(buf * S * N + (p + q) * N);
-              asm volatile(
-                  "{\n\t.reg .pred pa;\n\t"
-                  "setp.ne.b32 pa, %4, 0;\n\t"
-                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
-                  "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                  : "memory");
-            }
+          for (int h = 0; h < 2; h++) {
+            const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
+            const uint64_t bd = desc_sw64(b0 + h * 32);
+            const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
+            const uint32_t d = tmem + (uint32_t)(buf * S * N + p * N);
+            asm volatile(
+                "{\n\t.reg .pred pa;\n\t"
+                "setp.ne.b32 pa, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
+                "l"(ad), "l"(bd), "r"(idesc_i8(128, (S - p) * N)), "r"(acc)
+                : "memory");
+          }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          smem_u32(&empty[st]))
                      : "memory");

@@ -123,9 +123,10 @@ __global__ void __launch_bounds__(128) k_rowexp(const double2* __restrict__ X, i
 // FP64 -> int8 slices with the exponents of k_rowexp, one block per 32 rows
 // x 64 k: every output byte of [0, np) x [0, 2 Kcp) is written (zeros for
 // the padding rows and columns), so the operand buffers need no clearing.
-__global__ void __launch_bounds__(256) k_slice_rows(const double2* __restrict__ X, int Kc, int Kcp, int npad,
-                                                    int np_out, int S, int isB, const int* __restrict__ ex,
-                                                    int8_t* __restrict__ out) {
+template <int S>
+__global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict__ X, int Kc, int Kcp, int npad,
+                                                       int np_out, int isB, const int* __restrict__ ex,
+                                                       int8_t* __restrict__ out) {
   __shared__ double2 tile[64][33];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
   const int tid = threadIdx.x;
@@ -142,28 +143,25 @@ __global__ void __launch_bounds__(256) k_slice_rows(const double2* __restrict__ 
   const int row = r0 + rr;
   if (row >= np_out) return;
   const int e = ex[row];
-  uint64_t pre[L1G_MAX_SLICES], pim[L1G_MAX_SLICES];
+  uint64_t pre[S], pim[S];
 #pragma unroll
-  for (int p = 0; p < L1G_MAX_SLICES; p++) pre[p] = pim[p] = 0;
+  for (int p = 0; p < S; p++) pre[p] = pim[p] = 0;
 #pragma unroll
   for (int t = 0; t < 8; t++) {
     const double2 v = tile[kq + t][rr];
     double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
 #pragma unroll
-    for (int p = 0; p < L1G_MAX_SLICES; p++) {
-      if (p < S) {
-        const double ar = rint(tr), ai = rint(ti);
-        tr = (tr - ar) * 128.0;
-        ti = (ti - ai) * 128.0;
-        pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
-        pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
-      }
+    for (int p = 0; p < S; p++) {
+      const double ar = rint(tr), ai = rint(ti);
+      tr = (tr - ar) * 128.0;
+      ti = (ti - ai) * 128.0;
+      pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
+      pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
     }
   }
   const int col = k0 + kq;
 #pragma unroll
-  for (int p = 0; p < L1G_MAX_SLICES; p++) {
-    if (p >= S) break;
+  for (int p = 0; p < S; p++) {
     int8_t* base = out + (size_t)p * rows * Kp;
     if (!isB) {
       *(uint64_t*)(base + (size_t)row * Kp + col) = pre[p];
@@ -218,7 +216,6 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t tmem = tmem_slot;
 
   if (tid == 0) {
-    constexpr uint32_t idesc = idesc_i8(128, N);
     int issued = 0;  // k blocks whose TMA was issued
     bool ok = true;
     auto load = [&](int kb) {
@@ -239,21 +236,29 @@ __global__ void __launch_bounds__(128, 1)
       tc_fence_after();
       const uint32_t a0 = smem_u32(smem + st * C::STAGE);
       const uint32_t b0 = a0 + C::A_BYTES;
+      // B's S slices are one (S N)-row K-major tile and the level
+      // accumulators lie N columns apart, so A slice p times B slices
+      // q0..q0+cnt-1 is one MMA of width cnt N (at most 256 columns)
+      // landing on levels p+q0..p+q0+cnt-1.
+      constexpr int QC = (256 / N) < S ? (256 / N) : S;  // B slices per MMA
 #pragma unroll
       for (int p = 0; p < S; p++)
 #pragma unroll
-        for (int q = 0; q < S - p; q++)
+        for (int q0 = 0; q0 < S - p; q0 += QC)
 #pragma unroll
           for (int h = 0; h < 2; h++) {
+            const int cnt = (S - p - q0) < QC ? (S - p - q0) : QC;
             const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
-            const uint64_t bd = desc_sw64(b0 + q * N * 64 + h * 32);
+            const uint64_t bd = desc_sw64(b0 + q0 * N * 64 + h * 32);
+            // the first MMA into each level initialises it: level p+q0 first
+            // appears with p = 0 (q0 = its index) at kb = 0, h = 0
             const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
-            const uint32_t d = tmem + (uint32_t)((p + q) * N);
+            const uint32_t d = tmem + (uint32_t)((p + q0) * N);
             asm volatile(
                 "{\n\t.reg .pred pa;\n\t"
                 "setp.ne.b32 pa, %4, 0;\n\t"
                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
-                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                "l"(ad), "l"(bd), "r"(idesc_i8(128, cnt * N)), "r"(acc)
                 : "memory");
           }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -378,7 +383,7 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
 template <int S>
 static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                              const double2* Lop, const double2* Rop, double2* hs, int ld, cudaStream_t s,
-                             int* nlaunch) {
+                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev) {
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
@@ -396,44 +401,66 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
   const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
   split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
   split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
-  split::k_slice_rows<<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, S, 0, exA, A);
-  split::k_slice_rows<<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, S, 1, exB, B);
+  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, exA, A);
+  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, exB, B);
   *nlaunch += 4;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;
   // grouped order: W row tiles of L stay in L2 while every column tile of R
   // that meets them streams past once, so R is read from DRAM once per
-  // group instead of once per row tile (W is a tunable, 16 by default)
+  // group instead of once per row tile (W is a tunable, 16 by default).
+  // With hp, one launch per column group (hp->groups), each followed by its
+  // event unless its columns reach the LO block (recorded by the caller).
   const int W = c->split_group;
-  int ntile = 0;
-  const int2* dt = kp_tiles(k, "split:" + std::to_string(n) + ":" + std::to_string(Cf::JT) + ":" + std::to_string(W),
-                            &ntile, [&](std::vector<int2>& t) {
-                              const int nbi = (n + 127) / 128, nbj = (n + Cf::JT - 1) / Cf::JT;
-                              for (int g0 = 0; g0 < nbi; g0 += W)
-                                for (int bj = 0; bj < nbj; bj++)
-                                  for (int bi = g0; bi < std::min(nbi, g0 + W); bi++)
-                                    if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
-                            });
-  if (!dt) return LAPW1GPU_ERR_NOMEM;
+  const int nbi = (n + 127) / 128, nbj = (n + Cf::JT - 1) / Cf::JT;
+  int G = 1;
+  if (hp && hp->groups > 0 && hp->fixed) {
+    G = hp->groups;  // the caller's boundaries, multiples of JT
+  } else if (hp && hp->groups > 0) {
+    G = std::min(hp->groups, nbj);
+    hp->groups = G;
+    for (int g = 0; g <= G; g++) hp->col[g] = std::min(n, (int)((long)nbj * g / G) * Cf::JT);
+  }
   if (!c->smem((const void*)split::k_split_gemm<S>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
-  split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, exA, exB, hs, ld,
-                                                                 c->d_status);
-  *nlaunch += 1;
+  if (ev && cudaEventRecord(ev[0], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
+  for (int g = 0; g < G; g++) {
+    const int bj0 = hp && hp->groups > 0 ? std::min(nbj, hp->col[g] / Cf::JT) : 0;
+    const int bj1 = hp && hp->groups > 0 ? (g == G - 1 ? nbj : std::min(nbj, hp->col[g + 1] / Cf::JT)) : nbj;
+    int ntile = 0;
+    const int2* dt = kp_tiles(k,
+                              "split:" + std::to_string(n) + ":" + std::to_string(Cf::JT) + ":" + std::to_string(W) +
+                                  ":" + std::to_string(bj0) + ":" + std::to_string(bj1),
+                              &ntile, [&](std::vector<int2>& t) {
+                                for (int g0 = 0; g0 < nbi; g0 += W)
+                                  for (int bj = bj0; bj < bj1; bj++)
+                                    for (int bi = g0; bi < std::min(nbi, g0 + W); bi++)
+                                      if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
+                              });
+    if (!dt) return LAPW1GPU_ERR_NOMEM;
+    split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, exA, exB, hs, ld,
+                                                                   c->d_status);
+    *nlaunch += 1;
+    if (hp && hp->groups > 0 && hp->col[g + 1] <= k->nv) {
+      if (cudaEventRecord(hp->ev[g], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
+      hp->recorded[g] = true;
+    }
+  }
+  if (ev && cudaEventRecord(ev[1], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
 static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                           const double2* Lop, const double2* Rop, double2* hs, int ld, int slices, cudaStream_t s,
-                          int* nlaunch) {
+                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev) {
   switch (slices) {
-    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
-    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch);
+    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }

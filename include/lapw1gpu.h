@@ -150,6 +150,10 @@ typedef struct lapw1gpu_stats {
   double ms_d2h;        /* device->host copy of HS/HSDIAG              */
   double flops_fp64_equiv; /* algorithmic FP64 flops of K-b + K-ns     */
   double kernel_launches;  /* kernels this library launched in the run */
+  double ms_sph_main;   /* the spherical contraction kernel alone (k_spherical
+                           or k_sph_tc), inside ms_spherical               */
+  double ms_hns_main;   /* the HNS update alone (k_hns_gemm + ZGEMM panels, or
+                           the tcgen05 slice products), inside ms_hns      */
 } lapw1gpu_stats;
 
 typedef struct lapw1gpu_context lapw1gpu_context;
