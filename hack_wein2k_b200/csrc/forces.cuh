@@ -3,7 +3,8 @@
 // E = sum_n f_n eps_n of the generalized problem H c = eps S c that SECLR4
 // solves from the packed state: H from conj of the lower triangle, S the
 // transpose of the conj of the upper one (ZHCGST factors S**T), so that
-// H(I,J) = conj(HS(I,J)) and S(I,J) = conj(HS(J,I)) for I > J.  Hellmann-Feynman for that problem gives
+// H(I,J) = conj(HS(I,J)) and S(I,J) = conj(HS(J,I)) for I > J.
+// Hellmann-Feynman for that problem gives
 //   dE/dr = sum_n f_n c_n^H (dH/dr - eps_n dS/dr) c_n.
 // Atom positions r_a (POS, lattice coordinates) enter the setup only through
 // the structure-factor phases exp(2 pi i KZZ . r_a): every contribution of
@@ -25,13 +26,11 @@
 //                 is symmetric in (I, J) and the lower-triangle sum is half
 //                 the full one, which factors as
 //                   -Im sum_n f_n sum_k [Y0 conj(Zc) - Yc conj(Z0)],
-//                 Y = conj(X)^T (G c), Z = T Y.  For the (ALM, BLM) rows
-//                 Y = R^H (G c) and Z = L^T (G c) (library ZGEMMs; L carries
-//                 the TUU21/TUD21 terms of the LO rows); for the CLM rows
-//                 Y = CLM^H (G c) over the LO rows and Z = T_C Y over all
-//                 rows (k_force_hns_zc): the full matrix needs the CLM row
-//                 of T applied to plane-wave rows too, which the lower
-//                 triangle never uses
+//                 Y = conj(X)^T (G c), Z = T Y.  Y = R^H (G c) for the
+//                 (ALM, BLM) rows and CLM^H (G c) over the LO rows (library
+//                 ZGEMMs); Z = T Y per atom (k_force_hns_z, k_force_hns_zc):
+//                 for the CLM rows this is the CLM row of T applied to
+//                 plane-wave rows too, which the lower triangle never uses
 #pragma once
 #include "kernels_fp64.cuh"
 
@@ -387,6 +386,33 @@ __global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int
   const double2 v = C[(size_t)b * ldc + i];
   Cf[(size_t)b * n + i] = cscale(v, f[b]);
   Ce[(size_t)b * n + i] = cscale(v, f[b] * eps[b]);
+}
+
+// Z_AB[a][(ro, lm)][col] = sum_(r,b) M[(ro,lm)][(r,b)] Y[a][(r,b)][col]
+//                          + T_(ro,C)[lm][b] Y_C[a][b][col]
+// (M = [[TUU, TDU], [TUD, TDD]], T_(A,C) = TUU21, T_(B,C) = TUD21): the
+// product L^T (G c) through the small T of each atom instead of a second
+// N x K GEMM, because L = M conj(R) (+ the CLM terms of the LO rows).
+// Y, Z: [col][K]; Yc: [col][Kc] (null when there are no LO rows)
+__global__ void k_force_hns_z(int nsl2, int K, int Kc, const int* __restrict__ atype, const double2* __restrict__ tns,
+                              const double2* __restrict__ Y, const double2* __restrict__ Yc,
+                              double2* __restrict__ Z) {
+  const int col = blockIdx.x, a = blockIdx.y, ko = threadIdx.x;
+  if (ko >= 2 * nsl2) return;
+  const int ro = ko / nsl2, la = ko % nsl2;
+  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  const double2* y = Y + (size_t)col * K + (size_t)a * 2 * nsl2;
+  const int bA = ro == 0 ? 0 : 3, bB = ro == 0 ? 1 : 4, bC = ro == 0 ? 2 : 5;  // TUU TDU TUU21 / TUD TDD TUD21
+  double2 z = cmk(0.0, 0.0);
+  for (int b = 0; b < nsl2; b++) {
+    z = cadd(z, cmul(T[((size_t)bA * L1G_NSL2 + la) * L1G_NSL2 + b], y[b]));
+    z = cadd(z, cmul(T[((size_t)bB * L1G_NSL2 + la) * L1G_NSL2 + b], y[nsl2 + b]));
+  }
+  if (Yc) {
+    const double2* yc = Yc + (size_t)col * Kc + (size_t)a * nsl2;
+    for (int b = 0; b < nsl2; b++) z = cadd(z, cmul(T[((size_t)bC * L1G_NSL2 + la) * L1G_NSL2 + b], yc[b]));
+  }
+  Z[(size_t)col * K + (size_t)a * 2 * nsl2 + ko] = z;
 }
 
 // Z_C[a][lm][col] = sum_(r,b) T_(C,r)[lm][b] Y[a][(r,b)][col] + TUU22 Y_C:

@@ -1455,22 +1455,25 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     if (rc) return rc;
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
     CK(cudaGetLastError());
-    // Y = R^H (G c), Z = L^T (G c): K x 4nb, rows of R and L beyond n unused
+    // Y = R^H (G c): K x 4nb (rows of R beyond n unused); Yc = CLM^H (G c)
+    // over the LO rows; Z = T (Y; Yc) per atom
     if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
-                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS ||
-        cublasZgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Lop, k->npad,
-                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Z, K) != CUBLAS_STATUS_SUCCESS)
+                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS)
       return LAPW1GPU_ERR_CUDA;
-    k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
-    CK(cudaGetLastError());
+    double2* Yc = nullptr;
+    double2* Zc = nullptr;
     if (nlo > 0) {
-      // CLM rows: Yc = CLM^H (G c) over the LO rows, Zc = T_C (Y; Yc)
-      double2* Yc = (double2*)c->buf("frc_yc", sizeof(double2) * (size_t)4 * nb * Kc);
-      double2* Zc = (double2*)c->buf("frc_zc", sizeof(double2) * (size_t)4 * nb * Kc);
+      Yc = (double2*)c->buf("frc_yc", sizeof(double2) * (size_t)4 * nb * Kc);
+      Zc = (double2*)c->buf("frc_zc", sizeof(double2) * (size_t)4 * nb * Kc);
       if (!Yc || !Zc) return LAPW1GPU_ERR_NOMEM;
       if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
                       (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc, Kc) != CUBLAS_STATUS_SUCCESS)
         return LAPW1GPU_ERR_CUDA;
+    }
+    k_force_hns_z<<<dim3(4 * nb, ndf), 64, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Z);
+    k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
+    CK(cudaGetLastError());
+    if (nlo > 0) {
       k_force_hns_zc<<<dim3(4 * nb, ndf), 32, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Zc);
       k_force_hns_reduce<<<ndf, 256, 0, s>>>(nsl2, Kc, nb, Yc, Zc, d_occ, d_grad);
       CK(cudaGetLastError());
