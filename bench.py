@@ -223,6 +223,113 @@ def _rel_err(torch, a, b, n):
     return out
 
 
+def north_star(args):
+    """The 100-atom configurations: c4 (16 k-points, RKmax 8, N ~ 12700) as
+    one captured batch, split precision (spherical/HNS slices) against the
+    plain FP64 GPU path, plus the adjoint forces of 400 bands (c3 for
+    accuracy, c4 k-point 0 for time).  One JSON line, rank 0 only."""
+    import torch
+    from hack_wein2k_b200 import forces as FO
+    from hack_wein2k_b200 import lapw1gpu, synth
+    from hack_wein2k_b200.seclr import hermitian_from_packed_device, solve
+    rank, world, local = _env_rank()
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = lapw1gpu.Context(local)
+    s_sph, s_hns = args.slices, args.slices_hns
+
+    def use(prec):
+        if prec == "fp64":
+            ctx.set_precision(lapw1gpu.PREC_FP64)
+        else:
+            ctx.set_precision(lapw1gpu.PREC_SPLIT, s_sph)
+            ctx.set_slices(s_sph, s_hns)
+
+    def window_err(w, w0, lo=-10.0, hi=10.0):
+        win = (w0 > lo) & (w0 < hi)
+        return float(np.abs(w - w0)[win].max()) if win.any() else None
+
+    out = {"metric": "c4 k-batched setup ms/k-point, split vs plain FP64 GPU; c3/c4 adjoint forces",
+           "unit": "ms/k-point", "higher_is_better": False, "data": "synthetic (seeded)",
+           "slices": [s_sph, s_hns]}
+    # ---- c4 batch ----
+    ps = synth.config("c4")
+    hs = [torch.empty((q.n, q.n), dtype=torch.complex128, device=dev) for q in ps]
+    hd = [torch.empty(q.n, dtype=torch.complex128, device=dev) for q in ps]
+    res = {}
+    for prec in ("fp64", "split"):
+        use(prec)
+        kps = [ctx.upload(q) for q in ps]
+        ctx.autotune(kps[0], hs[0].data_ptr(), ps[0].n, hd[0].data_ptr())
+        a = (kps, [t.data_ptr() for t in hs], [q.n for q in ps], [t.data_ptr() for t in hd])
+        ctx.setup_batch(*a)
+        ms = min(ctx.setup_batch(*a)["ms_total"] for _ in range(2))
+        res[prec] = {"ms_per_batch": ms, "ms_per_kpoint": ms / len(ps)}
+        if prec == "fp64":
+            ref, refd = hs[0].clone(), hd[0].clone()
+        else:
+            err = {}
+            low = torch.tril(torch.ones(ps[0].n, ps[0].n, dtype=torch.bool, device=dev))
+            a0, b0 = hs[0].transpose(0, 1), ref.transpose(0, 1)  # [row][col]
+            for name, m in (("H", low), ("S", ~low)):
+                err[name] = ((a0 - b0).abs() * m).max().item() / ((b0.abs() * m).max().item())
+            res[prec]["rel_error_vs_fp64_k0"] = err
+        for k in kps:
+            k.free()
+    out["c4"] = {"workload": f"c4: 100-atom cell 20^3 bohr, RKmax 8, 16 k-points, N {min(q.n for q in ps)}.."
+                             f"{max(q.n for q in ps)}, one CUDA graph per batch", **res,
+                 "setup_speedup": res["fp64"]["ms_per_kpoint"] / res["split"]["ms_per_kpoint"]}
+    # ---- c4 k-point 0: forces of 400 bands (eigenvectors of the split setup) ----
+    p4 = ps[0]
+    use("split")
+    kp = ctx.upload(p4)
+    kp.run(hs[0].data_ptr(), p4.n, hd[0].data_ptr(), stats=True)
+    H, S = hermitian_from_packed_device(hs[0], hd[0])
+    del hs, hd
+    torch.cuda.empty_cache()
+    w, X = solve(H, S, nmax=400)
+    del H, S
+    occ = torch.ones(400, dtype=torch.float64, device=dev)
+    FO.gradient(ctx, kp, X, occ, w)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    FO.gradient(ctx, kp, X, occ, w)
+    e1.record()
+    torch.cuda.synchronize()
+    f_ms = e0.elapsed_time(e1)
+    kp.free()
+    del X
+    torch.cuda.empty_cache()
+    out["c4"]["forces_ms_per_kpoint_400_bands"] = f_ms
+    out["c4"]["setup_plus_forces_speedup"] = ((res["fp64"]["ms_per_kpoint"] + f_ms) /
+                                             (res["split"]["ms_per_kpoint"] + f_ms))
+    # ---- c3: accuracy of the split path (eigenvalues, forces) ----
+    p3 = synth.config("c3")[0]
+    acc = {}
+    for prec in ("fp64", "split"):
+        use(prec)
+        kp = ctx.upload(p3)
+        h3 = torch.zeros((p3.n, p3.n), dtype=torch.complex128, device=dev)
+        d3 = torch.zeros(p3.n, dtype=torch.complex128, device=dev)
+        torch.cuda.synchronize()
+        st = kp.run(h3.data_ptr(), p3.n, d3.data_ptr(), stats=True)
+        H, S = hermitian_from_packed_device(h3, d3)
+        w, X = solve(H, S, nmax=400)
+        g = FO.gradient(ctx, kp, X, torch.ones(400, dtype=torch.float64, device=dev), w)
+        acc[prec] = (w.cpu().numpy(), FO.cartesian_forces(p3, g.cpu().numpy()), st["ms_total"])
+        kp.free()
+        del H, S, X, h3, d3
+    out["c3"] = {"workload": "c3: 100-atom cell 20^3 bohr, RKmax 6, N %d, 400 bands" % p3.n,
+                 "eig_err_window_ry": window_err(acc["split"][0], acc["fp64"][0]),
+                 "force_err_ry_bohr": float(np.abs(acc["split"][1] - acc["fp64"][1]).max()),
+                 "max_force_ry_bohr": float(np.abs(acc["fp64"][1]).max())}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,9 +342,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
+    ap.add_argument("--north-star", action="store_true",
+                    help="instead: the 100-atom c4 batch (split vs FP64) and c3/c4 adjoint forces, one JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.north_star:
+        return north_star(args)
 
     import torch
     from hack_wein2k_b200 import lapw1gpu, synth

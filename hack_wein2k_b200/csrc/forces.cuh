@@ -16,8 +16,10 @@
 // Diagonal elements do not depend on the positions (D = 0).  Radial
 // functions, rotations (ROTIJ, ROTLOC) and the warped potential are held
 // fixed: the result is the gradient of the setup as a function of POS.
-//   k_force_sph   PW x PW pairs: the spherical sums of k_spherical plus the
-//                 step-function term 3 V BESR of each atom type (k_table)
+//   k_force_sph   PW x PW pairs: the spherical sums of k_spherical; the
+//                 step-function term 3 V BESR of each atom (k_table) depends
+//                 on the pair only through dK, so the pairs are binned by dK
+//                 and k_force_step sums the bins per atom
 //   k_force_lo    local-orbital columns, per equivalent atom (k_lo's terms)
 //   k_force_hns_reduce  the HNS update through its factors.  HNS adds
 //                 A(I,J) = X_J^T T conj(X_I) with X = (ALM, BLM, CLM) per atom
@@ -39,7 +41,8 @@
 
 __global__ void __launch_bounds__(SPH_THREADS, 1)
     k_force_sph(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef, TabDesc T,
-                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, double* __restrict__ F) {
+                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, double* __restrict__ F,
+                double* __restrict__ bins) {
   extern __shared__ double2 sm2[];
   double2* sJ = sm2;
   double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
@@ -53,7 +56,7 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
   const int nv = P.nv, ltop = P.ltop, nat = P.nat;
 
   double w[4][SPH_LMAX];
-  double dx[4][3], slen[4], x2[4];
+  double dx[4][3];
   double2 rj[4], re[4];  // rho(J,I) and rhoE(J,I) of the owned pairs
   bool act[4];
 #pragma unroll
@@ -65,12 +68,9 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
       act[q] = (J < nv && I < nv && J < I);
       double x = 0.0;
       dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
-      slen[q] = 1.0;
-      x2[q] = 0.0;
       rj[q] = re[q] = cmk(0.0, 0.0);
       if (act[q]) {
         x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
-        x2[q] = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
         double den = P.rk[I] * P.rk[J];
         if (den > 1.0e-8) x = x / den;
         const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
@@ -78,13 +78,14 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
         dx[q][0] = FRC_2PI * d0;
         dx[q][1] = FRC_2PI * d1;
         dx[q][2] = FRC_2PI * d2;
-        // |dK| as k_table forms it (the step function's argument)
-        const double g0 = T.bk[0] * d0 + T.bk[1] * d1 + T.bk[2] * d2;
-        const double g1 = T.bk[3] * d0 + T.bk[4] * d1 + T.bk[5] * d2;
-        const double g2 = T.bk[6] * d0 + T.bk[7] * d1 + T.bk[8] * d2;
-        slen[q] = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
         rj[q] = rho[(size_t)I * ldr + J];
         re[q] = rhoe[(size_t)I * ldr + J];
+        // the step-function term depends on the pair only through dK =
+        // KZZ_I - KZZ_J: bin x2 rho - rhoE by dK (k_force_step finishes it)
+        const size_t b = (((size_t)(d2 + T.d3) * (2 * T.d2 + 1)) + (d1 + T.d2)) * (2 * T.d1 + 1) + (d0 + T.d1);
+        const double x2q = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
+        atomicAdd(&bins[2 * b], x2q * rj[q].x - re[q].x);
+        atomicAdd(&bins[2 * b + 1], x2q * rj[q].y - re[q].y);
       }
       const bool top = !(fabs(x) < 0.9999999);
       double pm2 = 1.0, pm1 = x;
@@ -170,19 +171,6 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
             }
         }
       }
-      // interstitial step function of this type (hamilt.F:297-326)
-      const double v3 = 3.0 * P.v[jn], rt = P.rmt[jn];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        if (act[q]) {
-          const double h = slen[q] * rt;
-          double sn, cs;
-          sincos(h, &sn, &cs);
-          const double besr = (h * cs - sn) * (1.0 / (h * h * h));
-          tS[q] += v3 * besr;
-          tH[q] += x2[q] * (v3 * besr);
-        }
-      }
       const int ae = P.afirst[jn], me = P.mult[jn];
       for (int e = 0; e < me; e++) {
         double fr[3] = {0.0, 0.0, 0.0};
@@ -242,6 +230,48 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
       }
     t0 += ntc;
   }
+}
+
+// Step-function part of the spherical force: with B(dK) = sum over pairs
+// J < I with KZZ_I - KZZ_J = dK of (x2 rho(J,I) - rhoE(J,I)) (binned by
+// k_force_sph), atom a of type t gets
+//   dE/dr_a,c += sum_dK -2 (3 V_t) BESR(|dK| R_t) Im(exp(2 pi i dK.r_a) B(dK)) 2 pi dK_c
+// (the 3 V BESR term of k_table for that atom).  One block per atom.
+__global__ void __launch_bounds__(256) k_force_step(DevProb P, TabDesc T, const double* __restrict__ bins,
+                                                    double* __restrict__ F) {
+  __shared__ double red[3][256];
+  const int a = blockIdx.x, jn = P.atype[a];
+  const double v3 = 3.0 * P.v[jn], rt = P.rmt[jn];
+  const double* r = P.pos + 3 * a;
+  const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1, nz = 2 * T.d3 + 1;
+  const long nb = (long)nx * ny * nz;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (long q = threadIdx.x; q < nb; q += blockDim.x) {
+    const double bx = bins[2 * q], by = bins[2 * q + 1];
+    if (bx == 0.0 && by == 0.0) continue;
+    const int d0 = (int)(q % nx) - T.d1, d1 = (int)((q / nx) % ny) - T.d2, d2 = (int)(q / ((long)nx * ny)) - T.d3;
+    const double g0 = T.bk[0] * d0 + T.bk[1] * d1 + T.bk[2] * d2;
+    const double g1 = T.bk[3] * d0 + T.bk[4] * d1 + T.bk[5] * d2;
+    const double g2 = T.bk[6] * d0 + T.bk[7] * d1 + T.bk[8] * d2;
+    const double h = sqrt(g0 * g0 + g1 * g1 + g2 * g2) * rt;
+    double sn, cs;
+    sincos(h, &sn, &cs);
+    const double besr = (h * cs - sn) * (1.0 / (h * h * h));
+    const double2 ph = cexp2pi(r[0] * d0 + r[1] * d1 + r[2] * d2);
+    const double im = ph.x * by + ph.y * bx;  // Im(exp(2 pi i dK.r) B)
+    const double gq = -2.0 * v3 * besr * im * FRC_2PI;
+    acc[0] = fma(gq, (double)d0, acc[0]);
+    acc[1] = fma(gq, (double)d1, acc[1]);
+    acc[2] = fma(gq, (double)d2, acc[2]);
+  }
+  for (int c = 0; c < 3; c++) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 3; c++) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) atomicAdd(&F[a * 3 + threadIdx.x], red[threadIdx.x][0]);
 }
 
 // local-orbital columns: k_lo's terms per equivalent atom, reduced per warp

@@ -1424,17 +1424,25 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
   k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, Cf, Ce);
   CK(cudaGetLastError());
-  // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)): column-major n x n
-  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Cf, n,
-                  (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
-      cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, nb, &one, (const cuDoubleComplex*)Ce, n,
-                  (const cuDoubleComplex*)C, ldc, &zero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
+  // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)), column-major n x n, and rhoE:
+  // Hermitian, and only J < I is read, so the library forms the upper
+  // triangle alone (half the flops of a full product)
+  const double rzero = 0.0;
+  if (cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Cf, n,
+                   (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
+      cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Ce, n,
+                   (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
     return LAPW1GPU_ERR_CUDA;
   int ntiles = 0;
   const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
   if (!c->smem((const void*)k_force_sph, SPH_DYN_SMEM)) return LAPW1GPU_ERR_CUDA;
-  k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, d_grad);
+  const size_t nbox = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
+  double* bins = (double*)c->buf("frc_bins", sizeof(double) * 2 * nbox);
+  if (!bins) return LAPW1GPU_ERR_NOMEM;
+  CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
+  k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, d_grad, bins);
+  k_force_step<<<ndf, 256, 0, s>>>(P, k->tab, bins, d_grad);
   CK(cudaGetLastError());
   if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, d_grad);
   CK(cudaGetLastError());
