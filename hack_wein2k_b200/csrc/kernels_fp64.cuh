@@ -611,16 +611,19 @@ __global__ void k_hns_alm(DevProb P, const LoRange* __restrict__ lor, int nlor, 
 }
 
 #define TMUL_I 64
+#define TMUL_CH 4  // 64-row chunks per block: M is staged once for all of them
 #define TMUL_SMEM ((2 * L1G_NSL2) * (2 * L1G_NSL2) * 16 + (2 * L1G_NSL2) * TMUL_I * 16)
 // L[(a, r_out, la)][i] = sum_{(r, b)} M[(r_out, la)][(r, b)] conj(R[(a, r, b)][i])
-__global__ void __launch_bounds__(256) k_hns_tmul(int npad, int nsl2, const int* __restrict__ atype,
+// One block per (atom, TMUL_CH x 64 rows); the next chunk of R is fetched
+// into registers while the current one is multiplied.
+__global__ void __launch_bounds__(256, 2) k_hns_tmul(int npad, int nsl2, const int* __restrict__ atype,
                                                   const double2* __restrict__ tns, const double2* __restrict__ Rop,
                                                   double2* __restrict__ Lop) {
   extern __shared__ double2 tm[];
   const int K = 2 * nsl2;
   double2* sM = tm;          // [K][K]
   double2* sR = tm + K * K;  // [K][TMUL_I]
-  const int a = blockIdx.y, i0 = blockIdx.x * TMUL_I;
+  const int a = blockIdx.y;
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
   for (int idx = tid; idx < K * K; idx += 256) {
@@ -630,36 +633,55 @@ __global__ void __launch_bounds__(256) k_hns_tmul(int npad, int nsl2, const int*
     sM[idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
   }
   const double2* R = Rop + (size_t)a * K * npad;
-  for (int idx = tid; idx < K * TMUL_I; idx += 256) {
-    const int k = idx / TMUL_I, ii = idx % TMUL_I;
-    sR[idx] = R[(size_t)k * npad + i0 + ii];
-  }
-  __syncthreads();
-  constexpr int PR = (2 * L1G_NSL2 + 7) / 8;  // output rows per thread
-  double2 acc[PR][2];
+  double2* L = Lop + (size_t)a * K * npad;
+  constexpr int PF = (2 * L1G_NSL2 * TMUL_I + 255) / 256;  // R values per thread per chunk
+  double2 pre[PF];
+  auto fetch = [&](int i0) {
 #pragma unroll
-  for (int p = 0; p < PR; p++) acc[p][0] = acc[p][1] = cmk(0.0, 0.0);
-  for (int k = 0; k < K; k++) {
-    const double2 x0 = sR[k * TMUL_I + tx], x1 = sR[k * TMUL_I + tx + 32];
+    for (int q = 0; q < PF; q++) {
+      const int idx = tid + 256 * q;
+      pre[q] = (idx < K * TMUL_I && i0 < npad) ? R[(size_t)(idx / TMUL_I) * npad + i0 + idx % TMUL_I]
+                                               : make_double2(0.0, 0.0);
+    }
+  };
+  const int c0 = blockIdx.x * TMUL_CH;
+  fetch(c0 * TMUL_I);
+  constexpr int PR = (2 * L1G_NSL2 + 7) / 8;  // output rows per thread
+  for (int ch = c0; ch < c0 + TMUL_CH; ch++) {
+    const int i0 = ch * TMUL_I;
+    if (i0 >= npad) break;  // uniform across the block
+    __syncthreads();       // the previous chunk's sR reads are done
+#pragma unroll
+    for (int q = 0; q < PF; q++) {
+      const int idx = tid + 256 * q;
+      if (idx < K * TMUL_I) sR[idx] = pre[q];
+    }
+    __syncthreads();
+    if (ch + 1 < c0 + TMUL_CH) fetch(i0 + TMUL_I);
+    double2 acc[PR][2];
+#pragma unroll
+    for (int p = 0; p < PR; p++) acc[p][0] = acc[p][1] = cmk(0.0, 0.0);
+    for (int k = 0; k < K; k++) {
+      const double2 x0 = sR[k * TMUL_I + tx], x1 = sR[k * TMUL_I + tx + 32];
+#pragma unroll
+      for (int p = 0; p < PR; p++) {
+        const int row = ty + 8 * p;
+        if (row < K) {
+          const double2 m = sM[row * K + k];
+          acc[p][0].x = fma(m.x, x0.x, fma(m.y, x0.y, acc[p][0].x));
+          acc[p][0].y = fma(m.y, x0.x, fma(-m.x, x0.y, acc[p][0].y));
+          acc[p][1].x = fma(m.x, x1.x, fma(m.y, x1.y, acc[p][1].x));
+          acc[p][1].y = fma(m.y, x1.x, fma(-m.x, x1.y, acc[p][1].y));
+        }
+      }
+    }
 #pragma unroll
     for (int p = 0; p < PR; p++) {
       const int row = ty + 8 * p;
       if (row < K) {
-        const double2 m = sM[row * K + k];
-        acc[p][0].x = fma(m.x, x0.x, fma(m.y, x0.y, acc[p][0].x));
-        acc[p][0].y = fma(m.y, x0.x, fma(-m.x, x0.y, acc[p][0].y));
-        acc[p][1].x = fma(m.x, x1.x, fma(m.y, x1.y, acc[p][1].x));
-        acc[p][1].y = fma(m.y, x1.x, fma(-m.x, x1.y, acc[p][1].y));
+        L[(size_t)row * npad + i0 + tx] = acc[p][0];
+        L[(size_t)row * npad + i0 + tx + 32] = acc[p][1];
       }
-    }
-  }
-  double2* L = Lop + (size_t)a * K * npad;
-#pragma unroll
-  for (int p = 0; p < PR; p++) {
-    const int row = ty + 8 * p;
-    if (row < K) {
-      L[(size_t)row * npad + i0 + tx] = acc[p][0];
-      L[(size_t)row * npad + i0 + tx + 32] = acc[p][1];
     }
   }
 }

@@ -105,3 +105,20 @@ def run_sharded(sizes: Sequence[int], worker: Callable[[int], object], rank: int
     for loc, _ in gathered:
         out.update(loc)
     return dict(sorted(out.items()))
+
+
+def allreduce_forces(local, group=None):
+    """Band-energy gradients summed over the k-points of every rank.
+
+    `local` is this rank's sum over its own k-points of w_k dE_k/dPOS (a
+    float64 tensor [NDF, 3]; the k weights w_k of the BZ integration applied
+    by the caller).  One all-reduce of 3 NDF doubles (NCCL between GPUs,
+    gloo on CPU) gives every rank the total; with one rank it is returned
+    unchanged.  This is the only collective of a force run: the setups and
+    the per-k adjoints share nothing."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return local
+    out = local.clone()
+    dist.all_reduce(out, op=dist.ReduceOp.SUM, group=group)
+    return out

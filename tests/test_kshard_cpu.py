@@ -87,3 +87,39 @@ def test_two_gloo_ranks_gather_all_kpoints():
 def test_failed_kpoint_is_reported_on_every_rank():
     res = _spawn(fail_k=3)
     assert all(r[1] == "err" and "k-point 3" in r[2] for r in res)
+
+
+def _force_rank(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    sizes = [40, 55, 47, 61, 52]
+    weights = [0.1, 0.3, 0.2, 0.25, 0.15]
+    local = torch.zeros(4, 3, dtype=torch.float64)
+    for k in kshard.assign_kpoints(sizes, world)[rank]:
+        g = torch.arange(12, dtype=torch.float64).reshape(4, 3) * (k + 1) - k  # stands in for dE_k/dPOS
+        local += weights[k] * g
+    q.put((rank, kshard.allreduce_forces(local).tolist()))
+    dist.destroy_process_group()
+
+
+def test_force_sum_over_ranks_equals_serial_sum():
+    """Every rank gets the k-weighted force sum over all k-points (one
+    all-reduce), equal to the serial sum."""
+    import torch
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_force_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    weights = [0.1, 0.3, 0.2, 0.25, 0.15]
+    ref = sum(w * (torch.arange(12, dtype=torch.float64).reshape(4, 3) * (k + 1) - k) for k, w in enumerate(weights))
+    for _, out in res:
+        assert np.allclose(np.array(out), ref.numpy(), rtol=0, atol=1e-12)

@@ -82,6 +82,20 @@ def test_split_eigenvalues(sctx, slices, case):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["lo6", "c0"])
+def test_fp64_eigenvalues(ctx, case):
+    """The plain FP64 GPU path: window eigenvalues within 1e-8 Ry of the
+    oracle's (host LAPACK solve of both)."""
+    ctx.set_precision(lapw1gpu.PREC_FP64)
+    p = synth.small_case("lo", rkmax=6.0) if case == "lo6" else synth.config("c0")[0]
+    hs, hsd = ctx.setup(p)
+    hs_o, hsd_o = O.setup(p)
+    w, wo = _window_eigs(hs, hsd), _window_eigs(hs_o, hsd_o)
+    win = (wo > EWIN[0]) & (wo < EWIN[1])
+    assert np.max(np.abs(w - wo)[win]) <= 1e-8, np.max(np.abs(w - wo)[win])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["lo6", "c0"])
 def test_mixed_slices_eigenvalues(sctx, case):
     """Spherical part with 5 slices, HNS with 4: window eigenvalues within
     1e-6 Ry of the FP64 oracle's."""
