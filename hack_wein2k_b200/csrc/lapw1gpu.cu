@@ -672,7 +672,9 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
                          const cudaEvent_t* ev, HnsPipe* sp) {
   using Cf = sphtc::Cfg<S>;
   const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
-  const int Kcp = round_up(Kc, 32), Kp = 2 * Kcp;  // Kp: whole 64-byte K blocks
+  // Kp: whole 32-byte MMA steps; the tensor map's K extent is Kp, so the
+  // last 64-byte TMA block of an odd step count reads zero fill past it
+  const int Kcp = round_up(Kc, 16), Kp = 2 * Kcp;
   const int npA = round_up(nv, 128), npB = round_up(nv, Cf::IT);
   int8_t* A = (int8_t*)c->sbuf(set, "sphA", (size_t)S * L * npA * Kp);
   int8_t* B = (int8_t*)c->sbuf(set, "sphB", (size_t)S * L * 4 * npB * Kp);
@@ -718,7 +720,8 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
     const long t0 = first_tile(b0), t1 = (g == G - 1) ? ntile : first_tile(b1);
     if (t1 > t0) {
       sphtc::k_sph_tc<S, PAIR><<<(unsigned)(t1 - t0), Cf::THREADS, Cf::SMEM, s>>>(
-          ta, tb, P, dt + t0, Kp / 64, npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag, c->d_status);
+          ta, tb, P, dt + t0, (Kp + 63) / 64, (Kp % 64) != 0, npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag,
+          c->d_status);
       *nl += 1;
     }
     if (sp && sp->col[g + 1] <= k->nv) {
@@ -744,7 +747,7 @@ static bool sph_tc_supported(int S) { return S >= 4 && S <= 7; }
 static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
                            const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
                            const cudaEvent_t* ev, HnsPipe* sp) {
-  const int Kp = 2 * round_up(2 * k->ndf, 32);
+  const int Kp = 2 * round_up(2 * k->ndf, 16);
   const bool pair = sph_pair_ok(c->slices, Kp);
 #define SPH_CASE(SS)                                                                        \
   case SS:                                                                                  \

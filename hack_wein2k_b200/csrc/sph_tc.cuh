@@ -22,7 +22,8 @@
 // gathered from the Theta/WARP table and HS is written as k_spherical does.
 //
 // Warp roles: warps 0-7 epilogue (warp w reads TMEM lanes 32 (w%4).. and
-// the I half w/4 of the tile), warp 8 lane 0 issues TMA and MMA.  Every
+// the I half w/4 of the tile), warp 8 lane 0 issues the MMAs, warp 9 lane 0
+// the TMA loads (a full ring ahead of the MMAs, whatever they wait on).  Every
 // mbarrier wait is bounded; a timeout sets a status bit and ends the CTA's
 // work cleanly (copies drained, MMAs complete, TMEM freed).
 #pragma once
@@ -30,9 +31,11 @@
 namespace sphtc {
 
 using split::desc_sw64;
+using split::i2d_exact;
 using split::idesc_i8;
 using split::mbar_expect_tx;
 using split::mbar_init;
+using split::mbar_try_wait;
 using split::mbar_wait;
 using split::smem_u32;
 using split::tc_fence_after;
@@ -54,7 +57,7 @@ struct Cfg {
   static constexpr int STAGES_FIT = (227 * 1024 - SCALE_BYTES - 1024) / STAGE;
   static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
   static constexpr int SMEM = STAGES * STAGE + SCALE_BYTES + 1024;
-  static constexpr int THREADS = 288;
+  static constexpr int THREADS = 320;
 };
 
 // Operand rows of one l, built from AL/BL, phases and the per-(type, l)
@@ -179,16 +182,16 @@ __device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
     for (int d = 0; d < S; d += 2) {
       if (d + 1 < S) {
         const int pr = (int)r[d] * 128 + (int)r[d + 1];
-        v = fma((double)pr, w * 0.0078125, v);
+        v = fma(i2d_exact((uint32_t)pr), w * 0.0078125, v);
       } else {
-        v = fma((double)(int)r[d], w, v);
+        v = fma(i2d_exact(r[d]), w, v);
       }
       w *= 6.103515625e-05;  // 2^-14
     }
   } else {
 #pragma unroll
     for (int d = 0; d < S; d++) {
-      v = fma((double)(int)r[d], w, v);
+      v = fma(i2d_exact(r[d]), w, v);
       w *= 0.0078125;
     }
   }
@@ -196,9 +199,9 @@ __device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
 }
 
 template <int S, bool PAIR>
-__global__ void __launch_bounds__(288, 1)
+__global__ void __launch_bounds__(320, 1)
     k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
-             const int2* __restrict__ tiles, int nkb, int npA, int npB, const int* __restrict__ exA,
+             const int2* __restrict__ tiles, int nkb, int khalf, int npA, int npB, const int* __restrict__ exA,
              const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs,
              int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
   using C = Cfg<S>;
@@ -238,21 +241,45 @@ __global__ void __launch_bounds__(288, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
-  if (warp == 8) {
+  if (warp == 9) {
+    // ---- TMA producer ----
     if (lane == 0) {
       const int nit = L * nkb;
       int issued = 0;
       bool ok = true;
-      auto load = [&](int it) {
+      for (int it = 0; it < nit; it++) {
         const int st = it % STAGES, l = it / nkb, kb = it % nkb;
+        if (it >= STAGES) {  // the MMAs of it - STAGES have released the stage
+          const uint32_t par = ((it - STAGES) / STAGES) & 1;
+          long long t0 = clock64();
+          while (!mbar_try_wait(&empty[st], par)) {
+            if (*(volatile int*)&abort_flag || clock64() - t0 > (1LL << 31)) {
+              ok = false;
+              break;
+            }
+          }
+          if (!ok) break;
+        }
         uint8_t* a = smem + st * C::STAGE;
         uint8_t* b = a + C::A_BYTES;
         mbar_expect_tx(&full[st], C::STAGE);
         tma_load_3d(a, &tmA, &full[st], kb * 64, l * npA + j0, 0);
         tma_load_3d(b, &tmB, &full[st], kb * 64, l * 4 * npB + 4 * i0, 0);
-      };
-      for (int it = 0; it < STAGES - 1 && it < nit; it++) load(issued++);
-      for (int it = 0; it < nit && ok; it++) {
+        issued = it + 1;
+      }
+      if (!ok) atomicOr(status, L1G_STATUS_TIMEOUT);
+      // the copies in flight land before the CTA's shared memory is released
+      // (the MMA issuer may stop early; consumed stages return at once)
+      for (int it = issued - STAGES > 0 ? issued - STAGES : 0; it < issued; it++)
+        mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
+    }
+    __syncwarp();
+  } else if (warp == 8) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      const int nit = L * nkb;
+      bool ok = true;
+      for (int it = 0; it < nit; it++) {
         const int st = it % STAGES, l = it / nkb, kb = it % nkb, buf = l & 1;
         if (kb == 0 && l >= 2 && !mbar_wait(&tempty[buf], ((l - 2) >> 1) & 1)) {
           ok = false;
@@ -268,11 +295,15 @@ __global__ void __launch_bounds__(288, 1)
         // The S slices of B lie one after another in shared memory (one
         // (S N)-row K-major tile) and the level accumulators N columns
         // apart in TMEM, so A slice p times B slices 0..S-1-p is ONE MMA
-        // of width (S-p) N whose columns land on levels p..S-1.
+        // of width (S-p) N whose columns land on levels p..S-1.  When K is
+        // an odd number of 32-byte steps the last block holds one step
+        // (TMA zero-fills the rest; its MMA half is skipped).
+        const int nh = (khalf && kb == nkb - 1) ? 1 : 2;
 #pragma unroll
         for (int p = 0; p < S; p++)
 #pragma unroll
           for (int h = 0; h < 2; h++) {
+            if (h >= nh) continue;
             const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
             const uint64_t bd = desc_sw64(b0 + h * 32);
             const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
@@ -291,22 +322,10 @@ __global__ void __launch_bounds__(288, 1)
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_u32(&tfull[buf]))
                        : "memory");
-        const int nx = it + STAGES - 1;
-        if (nx < nit) {
-          const int rs = nx % STAGES;
-          if (nx >= STAGES && !mbar_wait(&empty[rs], ((nx - STAGES) / STAGES) & 1)) {
-            ok = false;
-            break;
-          }
-          load(nx);
-          issued = nx + 1;
-        }
       }
       if (!ok) {
         atomicOr(status, L1G_STATUS_TIMEOUT);
-        abort_flag = 1;
-        for (int it = issued - STAGES > 0 ? issued - STAGES : 0; it < issued; it++)
-          mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
+        *(volatile int*)&abort_flag = 1;
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&accbar))

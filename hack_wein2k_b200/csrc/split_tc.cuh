@@ -70,6 +70,13 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
+// int32 -> double, exact: the bits (0x43300000, x + 2^31) are the double
+// 2^52 + 2^31 + x, so one add recovers x (an FP64 add issues at the full
+// FP64 rate, the integer-to-double conversion at a fraction of it)
+__device__ __forceinline__ double i2d_exact(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -318,7 +325,7 @@ __global__ void __launch_bounds__(128, 1)
             : "r"(trow + (uint32_t)(d * N + c * 16)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int q = 0; q < 16; q++) v[q] = fma((double)(int)r[q], w, v[q]);
+        for (int q = 0; q < 16; q++) v[q] = fma(i2d_exact(r[q]), w, v[q]);
         w *= 0.0078125;  // 2^-7
       }
       if (i < n) {
