@@ -222,19 +222,39 @@ __global__ void __launch_bounds__(128, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
-  if (tid == 0) {
+  if (tid == 32) {
+    // TMA producer (warp 1 lane 0): a full ring ahead of the MMAs
     int issued = 0;  // k blocks whose TMA was issued
     bool ok = true;
-    auto load = [&](int kb) {
+    for (int kb = 0; kb < nkb; kb++) {
       const int st = kb % STAGES;
+      if (kb >= STAGES) {  // the MMAs of kb - STAGES have released the stage
+        const uint32_t par = ((kb - STAGES) / STAGES) & 1;
+        long long t0 = clock64();
+        while (!mbar_try_wait(&empty[st], par)) {
+          if (*(volatile int*)&abort_flag || clock64() - t0 > (1LL << 31)) {
+            ok = false;
+            break;
+          }
+        }
+        if (!ok) break;
+      }
       uint8_t* a = smem + st * C::STAGE;
       uint8_t* b = a + C::A_BYTES;
       mbar_expect_tx(&full[st], C::STAGE);
       tma_load_3d(a, &tmA, &full[st], kb * 64, i0, 0);
       tma_load_3d(b, &tmB, &full[st], kb * 64, 2 * j0, 0);
-    };
-    for (int kb = 0; kb < STAGES - 1 && kb < nkb; kb++) load(issued++);
-    for (int kb = 0; kb < nkb && ok; kb++) {
+      issued = kb + 1;
+    }
+    if (!ok) atomicOr(status, L1G_STATUS_TIMEOUT);
+    // the copies in flight land before the CTA may exit (the MMA issuer may
+    // stop early; consumed stages return at once); every wait is bounded
+    for (int kb = issued - STAGES > 0 ? issued - STAGES : 0; kb < issued; kb++)
+      mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+  } else if (tid == 0) {
+    // MMA issuer (warp 0 lane 0)
+    bool ok = true;
+    for (int kb = 0; kb < nkb; kb++) {
       const int st = kb % STAGES;
       if (!mbar_wait(&full[st], (kb / STAGES) & 1)) {
         ok = false;
@@ -271,26 +291,10 @@ __global__ void __launch_bounds__(128, 1)
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&empty[st]))
                    : "memory");
-      const int nk = kb + STAGES - 1;
-      if (nk < nkb) {
-        const int rs = nk % STAGES;
-        if (nk >= STAGES && !mbar_wait(&empty[rs], ((nk - STAGES) / STAGES) & 1)) {
-          ok = false;
-          break;
-        }
-        load(nk);
-        issued = nk + 1;
-      }
     }
     if (!ok) {
       atomicOr(status, L1G_STATUS_TIMEOUT);
-      abort_flag = 1;
-      // drain the copies that can still be in flight (the last STAGES
-      // issued) before the CTA may exit; every wait is bounded
-      for (int kb = issued - STAGES > 0 ? issued - STAGES : 0; kb < issued; kb++) {
-        const int st = kb % STAGES;
-        mbar_wait(&full[st], (kb / STAGES) & 1);
-      }
+      *(volatile int*)&abort_flag = 1;
     }
     // arrives once every MMA issued so far has completed, so TMEM is
     // quiescent when the epilogue (or the abort path) proceeds
@@ -313,19 +317,23 @@ __global__ void __launch_bounds__(128, 1)
       double v[16];
 #pragma unroll
       for (int q = 0; q < 16; q++) v[q] = 0.0;
-      double w = 1.0;
+      // all S levels of these 16 columns in flight at once, one wait
+      uint32_t r[S][16];
 #pragma unroll
-      for (int d = 0; d < S; d++) {
-        uint32_t r[16];
+      for (int d = 0; d < S; d++)
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
             "[%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
+              "=r"(r[d][6]), "=r"(r[d][7]), "=r"(r[d][8]), "=r"(r[d][9]), "=r"(r[d][10]), "=r"(r[d][11]),
+              "=r"(r[d][12]), "=r"(r[d][13]), "=r"(r[d][14]), "=r"(r[d][15])
             : "r"(trow + (uint32_t)(d * N + c * 16)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double w = 1.0;
 #pragma unroll
-        for (int q = 0; q < 16; q++) v[q] = fma(i2d_exact(r[q]), w, v[q]);
+      for (int d = 0; d < S; d++) {
+#pragma unroll
+        for (int q = 0; q < 16; q++) v[q] = fma(i2d_exact(r[d][q]), w, v[q]);
         w *= 0.0078125;  // 2^-7
       }
       if (i < n) {
