@@ -53,6 +53,7 @@ struct HnsPipe {
 
 struct lapw1gpu_context {
   int device = 0;
+  int nsm = 148;  // streaming multiprocessors (persistent grids)
   cudaStream_t stream = nullptr;
   cudaStream_t side[L1G_MAX_SETS] = {};  // streams of scratch sets 1.. in a batch
   cudaEvent_t ev[16] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels
@@ -261,6 +262,7 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
   CK(cudaSetDevice(device));
   lapw1gpu_context* c = new lapw1gpu_context();
   c->device = device;
+  c->nsm = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return LAPW1GPU_ERR_CUDA;
@@ -666,7 +668,7 @@ static int hns_panels_zgemm(cublasHandle_t h, int n, int nv, int npad, int K, in
 
 // Spherical part on tcgen05 (sph_tc.cuh): slice the per-l operands, then
 // one CTA per (128 J, IT I) tile of the triangle.
-template <int S, bool PAIR>
+template <int S, int LS>
 static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
                          const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
                          const cudaEvent_t* ev, HnsPipe* sp) {
@@ -703,7 +705,7 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
                                   if (bj * 128 <= bi * Cf::IT + Cf::IT - 1) t.push_back(make_int2(bj, bi));
                             });
   if (!dt) return LAPW1GPU_ERR_NOMEM;
-  if (!c->smem((const void*)sphtc::k_sph_tc<S, PAIR>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
+  if (!c->smem((const void*)sphtc::k_sph_tc<S, LS>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
   if (ev && cudaEventRecord(ev[0], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   // tiles are ordered by the I tile (column of S); per I tile bi the J tiles
   // bj with bj 128 <= bi IT + IT - 1, so a column group is a contiguous range
@@ -719,9 +721,11 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
     const int b1 = sp ? (g == G - 1 ? nbi : std::min(nbi, sp->col[g + 1] / Cf::IT)) : nbi;
     const long t0 = first_tile(b0), t1 = (g == G - 1) ? ntile : first_tile(b1);
     if (t1 > t0) {
-      sphtc::k_sph_tc<S, PAIR><<<(unsigned)(t1 - t0), Cf::THREADS, Cf::SMEM, s>>>(
-          ta, tb, P, dt + t0, (Kp + 63) / 64, (Kp % 64) != 0, npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag,
-          c->d_status);
+      // persistent: one CTA per SM over the group's tiles
+      const int grid = (int)std::min<long>(t1 - t0, c->nsm);
+      sphtc::k_sph_tc<S, LS><<<grid, Cf::THREADS, Cf::SMEM, s>>>(
+          ta, tb, P, dt + t0, (int)(t1 - t0), (Kp + 63) / 64, (Kp % 64) != 0, npA, npB, exA, exB, tab, k->tab, hs,
+          ld, hsdiag, c->d_status);
       *nl += 1;
     }
     if (sp && sp->col[g + 1] <= k->nv) {
@@ -733,12 +737,17 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
-// Pairing two levels in int32 before the conversion is exact while
-// (d+1) 4096 Kp 128 + (d+2) 4096 Kp < 2^31 for every level d < S-1
-// (|slice| <= 64, level d sums d+1 products per k).
-static bool sph_pair_ok(int S, int Kp) {
-  const double worst = (double)S * 4096.0 * Kp * 128.0 + (double)(S + 1) * 4096.0 * Kp;
-  return worst < 2147483647.0;
+// Exactness of the level sums (|slice| <= 64; level d sums d+1 products of
+// at most 4096 per k): the int32 pairs c_d 128 + c_(d+1) hold while
+// S 4096 Kp 128 + (S+1) 4096 Kp < 2^31, and the int64 combination
+// V = sum_d c_d 2^(7(S-1-d)) converts with one add while |V| < 2^51.
+// Returns the level-sum form of k_sph_tc: 2 int64, 1 int32 pairs, 0 plain.
+static int sph_level_mode(int S, int Kp) {
+  const double pair = (double)S * 4096.0 * Kp * 128.0 + (double)(S + 1) * 4096.0 * Kp;
+  if (pair >= 2147483647.0) return 0;
+  double v = 0.0;
+  for (int d = 0; d < S; d++) v += (double)(d + 1) * 4096.0 * Kp * std::ldexp(1.0, 7 * (S - 1 - d));
+  return v < std::ldexp(1.0, 51) ? 2 : 1;
 }
 
 // true when the split-precision spherical path handles this slice count
@@ -748,11 +757,12 @@ static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, con
                            const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
                            const cudaEvent_t* ev, HnsPipe* sp) {
   const int Kp = 2 * round_up(2 * k->ndf, 16);
-  const bool pair = sph_pair_ok(c->slices, Kp);
-#define SPH_CASE(SS)                                                                        \
-  case SS:                                                                                  \
-    return pair ? sph_tc_launch<SS, true>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp)   \
-                : sph_tc_launch<SS, false>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp);
+  const int mode = sph_level_mode(c->slices, Kp);
+#define SPH_CASE(SS)                                                                               \
+  case SS:                                                                                         \
+    return mode == 2   ? sph_tc_launch<SS, 2>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
+           : mode == 1 ? sph_tc_launch<SS, 1>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
+                       : sph_tc_launch<SS, 0>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp);
   switch (c->slices) {
     SPH_CASE(4)
     SPH_CASE(5)
@@ -764,7 +774,7 @@ static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, con
 #undef SPH_CASE
 }
 
-// algorithmic FP64-equivalent flops of the contractions (see DESIGN.md roofline)
+// algorithmic FP64-equivalent flops of the contractions
 static double alg_flops(const lapw1gpu_kpoint* k) {
   double nv = k->nv, n = k->n;
   // spherical: per pair and atom type 6 FMA per l, 4 FMA per equivalent

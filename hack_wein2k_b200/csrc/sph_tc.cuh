@@ -31,6 +31,8 @@
 namespace sphtc {
 
 using split::desc_sw64;
+using split::digit7;
+using split::digit_scale;
 using split::i2d_exact;
 using split::idesc_i8;
 using split::mbar_expect_tx;
@@ -137,14 +139,12 @@ __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* 
     for (int t = 0; t < 8; t++) {
       const int k = col + t;
       const double2 v = (k < Kc) ? tile[k * 33 + rr] : make_double2(0.0, 0.0);
-      double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
+      double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
 #pragma unroll
       for (int p = 0; p < S; p++) {
-        const double ar = rint(tr), ai = rint(ti);
-        tr = (tr - ar) * 128.0;
-        ti = (ti - ai) * 128.0;
-        pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
-        pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
+        const int ar = digit7(tr), ai = digit7(ti);
+        pre[p] |= (uint64_t)(uint8_t)ar << (8 * t);
+        pim[p] |= (uint64_t)(uint8_t)ai << (8 * t);
       }
     }
 #pragma unroll
@@ -172,12 +172,30 @@ __device__ __forceinline__ double pow2i(int e) {
                                    : (e < -1022 ? 0.0 : ldexp(1.0, e));
 }
 
-// level sum of one accumulator column: sum_d c_d 2^(-7d), levels paired in
-// int32 (c_d 128 + c_(d+1), exact when PAIR holds) before the conversion
-template <int S, bool PAIR>
+// Level sum of one accumulator column, sum_d c_d 2^(-7d), in one of three
+// exact forms (LS, chosen on the host from the bound on |c_d|):
+//   LS = 2: levels paired in int32 (c_d 128 + c_(d+1)), the pairs combined
+//           in int64 into V = sum_d c_d 2^(7(S-1-d)), |V| < 2^51, and V
+//           converted by one add (returns V: the caller's scale carries
+//           2^(-7(S-1)));
+//   LS = 1: pairs in int32, each pair converted and accumulated in FP64;
+//   LS = 0: every level converted and accumulated in FP64.
+template <int S, int LS>
 __device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
+  if (LS == 2) {
+    long long V = 0;
+#pragma unroll
+    for (int d = 0; d < S; d += 2) {
+      if (d + 1 < S)
+        V = V * 16384 + (long long)((int)r[d] * 128 + (int)r[d + 1]);
+      else
+        V = V * 128 + (long long)(int)r[d];
+    }
+    // 1.5 2^52 + V has V in its low mantissa bits for |V| < 2^51
+    return __longlong_as_double(V + 0x4338000000000000LL) - 6755399441055744.0;
+  }
   double v = 0.0, w = 1.0;
-  if (PAIR) {
+  if (LS == 1) {
 #pragma unroll
     for (int d = 0; d < S; d += 2) {
       if (d + 1 < S) {
@@ -198,23 +216,57 @@ __device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
   return v;
 }
 
-template <int S, bool PAIR>
+// S levels x 8 columns of this warp's TMEM lanes into registers (async until
+// tmem_wait)
+template <int S>
+__device__ __forceinline__ void tmem_ld8(uint32_t (&r)[S][8], uint32_t addr, int N) {
+#pragma unroll
+  for (int d = 0; d < S; d++)
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
+                   "=r"(r[d][6]), "=r"(r[d][7])
+                 : "r"(addr + (uint32_t)(d * N)));
+}
+// wait for this thread's TMEM loads; the registers pass through an empty asm
+// so that no use of them is scheduled before the wait
+template <int S>
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[S][8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int d = 0; d < S; d++)
+    asm volatile(""
+                 : "+r"(r[d][0]), "+r"(r[d][1]), "+r"(r[d][2]), "+r"(r[d][3]), "+r"(r[d][4]), "+r"(r[d][5]),
+                   "+r"(r[d][6]), "+r"(r[d][7]));
+}
+
+// bounded wait that also gives up once another role has raised the abort flag
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, const int* flag) {
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (*(volatile const int*)flag || clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+
+// Persistent: CTA b takes tiles b, b + gridDim.x, ... of the list.  The
+// stage ring and the two accumulator buffers run on counters that continue
+// across tiles, so the loads and MMAs of a tile's first l overlap the
+// previous tile's last epilogue, interstitial gather and HS writes.
+template <int S, int LS>
 __global__ void __launch_bounds__(320, 1)
     k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
-             const int2* __restrict__ tiles, int nkb, int khalf, int npA, int npB, const int* __restrict__ exA,
-             const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T, double2* __restrict__ hs,
-             int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
+             const int2* __restrict__ tiles, int ntile, int nkb, int khalf, int npA, int npB,
+             const int* __restrict__ exA, const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T,
+             double2* __restrict__ hs, int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
   using C = Cfg<S>;
   constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = IT / 2;
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar;
+  __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar, ebar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int2 tt = tiles[blockIdx.x];
-  const int j0 = tt.x * 128, i0 = tt.y * IT;
   const int L = P.ltop, nv = P.nv;
+  const int nit = L * nkb;  // pipeline iterations per tile
 
   if (warp == 8) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -232,6 +284,7 @@ __global__ void __launch_bounds__(320, 1)
       mbar_init(&tempty[b], 8);  // one arrival per epilogue warp
     }
     mbar_init(&accbar, 1);
+    mbar_init(&ebar, 256);  // the epilogue threads' barrier (bounded waits)
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -242,86 +295,94 @@ __global__ void __launch_bounds__(320, 1)
   const uint32_t tmem = tmem_slot;
 
   if (warp == 9) {
-    // ---- TMA producer ----
+    // ---- TMA producer: a full ring ahead of the MMAs ----
     if (lane == 0) {
-      const int nit = L * nkb;
-      int issued = 0;
+      long g = 0;  // iterations issued over all tiles
       bool ok = true;
-      for (int it = 0; it < nit; it++) {
-        const int st = it % STAGES, l = it / nkb, kb = it % nkb;
-        if (it >= STAGES) {  // the MMAs of it - STAGES have released the stage
-          const uint32_t par = ((it - STAGES) / STAGES) & 1;
-          long long t0 = clock64();
-          while (!mbar_try_wait(&empty[st], par)) {
-            if (*(volatile int*)&abort_flag || clock64() - t0 > (1LL << 31)) {
-              ok = false;
-              break;
+      for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
+        const int2 tt = tiles[t];
+        const int j0 = tt.x * 128, i0 = tt.y * IT;
+        for (int it = 0; it < nit; it++, g++) {
+          const int st = (int)(g % STAGES);
+          if (g >= STAGES) {  // the MMAs of g - STAGES have released the stage
+            const uint32_t par = (uint32_t)((g - STAGES) / STAGES) & 1;
+            long long t0 = clock64();
+            while (!mbar_try_wait(&empty[st], par)) {
+              if (*(volatile int*)&abort_flag || clock64() - t0 > (1LL << 31)) {
+                ok = false;
+                break;
+              }
             }
+            if (!ok) break;
           }
-          if (!ok) break;
+          const int l = it / nkb, kb = it % nkb;
+          uint8_t* a = smem + st * C::STAGE;
+          uint8_t* b = a + C::A_BYTES;
+          mbar_expect_tx(&full[st], C::STAGE);
+          tma_load_3d(a, &tmA, &full[st], kb * 64, l * npA + j0, 0);
+          tma_load_3d(b, &tmB, &full[st], kb * 64, l * 4 * npB + 4 * i0, 0);
         }
-        uint8_t* a = smem + st * C::STAGE;
-        uint8_t* b = a + C::A_BYTES;
-        mbar_expect_tx(&full[st], C::STAGE);
-        tma_load_3d(a, &tmA, &full[st], kb * 64, l * npA + j0, 0);
-        tma_load_3d(b, &tmB, &full[st], kb * 64, l * 4 * npB + 4 * i0, 0);
-        issued = it + 1;
       }
       if (!ok) atomicOr(status, L1G_STATUS_TIMEOUT);
       // the copies in flight land before the CTA's shared memory is released
       // (the MMA issuer may stop early; consumed stages return at once)
-      for (int it = issued - STAGES > 0 ? issued - STAGES : 0; it < issued; it++)
-        mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
+      for (long q = g - STAGES > 0 ? g - STAGES : 0; q < g; q++)
+        mbar_wait(&full[q % STAGES], (uint32_t)(q / STAGES) & 1);
     }
     __syncwarp();
   } else if (warp == 8) {
     // ---- MMA issuer ----
     if (lane == 0) {
-      const int nit = L * nkb;
+      long g = 0;   // pipeline iterations over all tiles
+      long gl = 0;  // accumulations (tile, l) over all tiles
       bool ok = true;
-      for (int it = 0; it < nit; it++) {
-        const int st = it % STAGES, l = it / nkb, kb = it % nkb, buf = l & 1;
-        if (kb == 0 && l >= 2 && !mbar_wait(&tempty[buf], ((l - 2) >> 1) & 1)) {
-          ok = false;
-          break;
-        }
-        if (!mbar_wait(&full[st], (it / STAGES) & 1)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t a0 = smem_u32(smem + st * C::STAGE);
-        const uint32_t b0 = a0 + C::A_BYTES;
-        // The S slices of B lie one after another in shared memory (one
-        // (S N)-row K-major tile) and the level accumulators N columns
-        // apart in TMEM, so A slice p times B slices 0..S-1-p is ONE MMA
-        // of width (S-p) N whose columns land on levels p..S-1.  When K is
-        // an odd number of 32-byte steps the last block holds one step
-        // (TMA zero-fills the rest; its MMA half is skipped).
-        const int nh = (khalf && kb == nkb - 1) ? 1 : 2;
-#pragma unroll
-        for (int p = 0; p < S; p++)
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            if (h >= nh) continue;
-            const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
-            const uint64_t bd = desc_sw64(b0 + h * 32);
-            const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
-            const uint32_t d = tmem + (uint32_t)(buf * S * N + p * N);
-            asm volatile(
-                "{\n\t.reg .pred pa;\n\t"
-                "setp.ne.b32 pa, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
-                "l"(ad), "l"(bd), "r"(idesc_i8(128, (S - p) * N)), "r"(acc)
-                : "memory");
+      for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
+        for (int it = 0; it < nit; it++, g++) {
+          const int st = (int)(g % STAGES), kb = it % nkb, buf = (int)(gl & 1);
+          if (kb == 0 && gl >= 2 && !wait_or_abort(&tempty[buf], (uint32_t)((gl - 2) >> 1) & 1, &abort_flag)) {
+            ok = false;
+            break;
           }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&empty[st]))
-                     : "memory");
-        if (kb == nkb - 1)
+          if (!wait_or_abort(&full[st], (uint32_t)(g / STAGES) & 1, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + st * C::STAGE);
+          const uint32_t b0 = a0 + C::A_BYTES;
+          // The S slices of B lie one after another in shared memory (one
+          // (S N)-row K-major tile) and the level accumulators N columns
+          // apart in TMEM, so A slice p times B slices 0..S-1-p is ONE MMA
+          // of width (S-p) N whose columns land on levels p..S-1.  When K
+          // is an odd number of 32-byte steps the last block holds one step
+          // (TMA zero-fills the rest; its MMA half is skipped).
+          const int nh = (khalf && kb == nkb - 1) ? 1 : 2;
+#pragma unroll
+          for (int p = 0; p < S; p++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              if (h >= nh) continue;
+              const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
+              const uint64_t bd = desc_sw64(b0 + h * 32);
+              const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
+              const uint32_t d = tmem + (uint32_t)(buf * S * N + p * N);
+              asm volatile(
+                  "{\n\t.reg .pred pa;\n\t"
+                  "setp.ne.b32 pa, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pa;\n\t}" ::"r"(d),
+                  "l"(ad), "l"(bd), "r"(idesc_i8(128, (S - p) * N)), "r"(acc)
+                  : "memory");
+            }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                           smem_u32(&tfull[buf]))
+                           smem_u32(&empty[st]))
                        : "memory");
+          if (kb == nkb - 1) {
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&tfull[buf]))
+                         : "memory");
+            gl++;
+          }
+        }
       }
       if (!ok) {
         atomicOr(status, L1G_STATUS_TIMEOUT);
@@ -334,138 +395,163 @@ __global__ void __launch_bounds__(320, 1)
     __syncwarp();
   } else {
     // ---- epilogue warps ----
-    // scale tables of this tile for every l, staged once (the l loop then
-    // reads only shared memory and TMEM)
     int16_t* sA = (int16_t*)(smem + STAGES * C::STAGE);  // [l][128]: eA - 12
     int16_t* sB = sA + SPH_LMAX * 128;                    // [l][IT][2]: eB
-    for (int q = tid; q < L * 128; q += 256) {
-      const int l = q >> 7, r = q & 127, J = j0 + r;
-      sA[q] = (int16_t)((J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
-    }
-    for (int q = tid; q < L * 2 * IT; q += 256) {
-      const int l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
-      sB[q] = (int16_t)((I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
-    }
-    asm volatile("bar.sync 1, 256;" ::: "memory");  // the epilogue warps only
-    const int g = warp & 3, hh = warp >> 2;
-    const int J = j0 + 32 * g + lane;
-    const bool jin = J < nv;
-    const double xj = jin ? P.xk[J] : 0.0, yj = jin ? P.yk[J] : 0.0, zj = jin ? P.zk[J] : 0.0;
-    const double rj = jin ? P.rk[J] : 0.0;
-    double x[HALF], pm1[HALF], pm2[HALF];
-    double2 aS[HALF], aH[HALF];
-#pragma unroll
-    for (int u = 0; u < HALF; u++) {
-      const int I = i0 + hh * HALF + u;
-      double xx = 0.0;
-      if (jin && I < nv) {
-        xx = P.xk[I] * xj + P.yk[I] * yj + P.zk[I] * zj;
-        const double den = P.rk[I] * rj;
-        if (den > 1.0e-8) xx = xx / den;
-      }
-      x[u] = xx;
-      pm1[u] = xx;   // P_1
-      pm2[u] = 1.0;  // P_0
-      aS[u] = aH[u] = make_double2(0.0, 0.0);
-    }
-    const uint32_t trow = tmem + ((uint32_t)(32 * g) << 16);
+    const int g4 = warp & 3, hh = warp >> 2;
+    const uint32_t trow = tmem + ((uint32_t)(32 * g4) << 16);
+    long gl = 0;  // accumulations consumed over all tiles
     bool ok = true;
-    for (int l = 0; l < L && ok; l++) {
-      const int buf = l & 1;
-      // warp-uniform outcome: the TMEM loads below are .sync.aligned
-      if (!__all_sync(0xffffffffu, mbar_wait(&tfull[buf], (l >> 1) & 1))) {
+    uint32_t ephase = 0;
+    // barrier of the 256 epilogue threads on an mbarrier, every wait bounded
+    // (a warp that gave up leaves the others to time out, not to hang);
+    // warp-uniform outcome
+    auto epi_sync = [&]() -> bool {
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&ebar)) : "memory");
+      const bool r = __all_sync(0xffffffffu, wait_or_abort(&ebar, ephase & 1, &abort_flag));
+      ephase++;
+      return r;
+    };
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+      const int2 tt = tiles[t];
+      const int j0 = tt.x * 128, i0 = tt.y * IT;
+      // scale tables of this tile for every l, written once the previous
+      // tile's readers are past the first barrier
+      if (!epi_sync()) {
         ok = false;
-        if (lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
         break;
       }
-      if (*(volatile int*)&abort_flag) {
+      for (int q = tid; q < L * 128; q += 256) {
+        const int l = q >> 7, r = q & 127, J = j0 + r;
+        sA[q] = (int16_t)((J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
+      }
+      for (int q = tid; q < L * 2 * IT; q += 256) {
+        const int l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
+        sB[q] = (int16_t)((I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
+      }
+      if (!epi_sync()) {
         ok = false;
         break;
       }
-      tc_fence_after();
-      // Legendre weights of this l (hamilt.F:250-281 recursion, UTOP branch)
-      double w[HALF];
-#pragma unroll
-      for (int u = 0; u < HALF; u++) {
-        double pl;
-        if (l == 0)
-          pl = 1.0;
-        else if (l == 1)
-          pl = x[u];
-        else {
-          if (fabs(x[u]) < 0.9999999) {
-            const double pplx = x[u] * pm1[u];
-            pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2[u]);
-          } else {
-            pl = x[u] * pm1[u];
-          }
-          pm2[u] = pm1[u];
-          pm1[u] = pl;
-        }
-        w[u] = (double)(2 * l + 1) * pl;
-      }
-      const int ea = sA[l * 128 + 32 * g + lane];
-      // 4 real columns per I: S re, S im, H re, H im; this thread's HALF I
-      // start at column 4 * HALF * hh; read 8 columns (2 I) at a time
-#pragma unroll
-      for (int c = 0; c < HALF / 2; c++) {
-        uint32_t r[S][8];
-#pragma unroll
-        for (int d = 0; d < S; d++)
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-              : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
-                "=r"(r[d][6]), "=r"(r[d][7])
-              : "r"(trow + (uint32_t)(buf * S * N + d * N + 4 * HALF * hh + 8 * c)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (c == HALF / 2 - 1) {
-          // all columns of this buffer read: hand it back to the MMA issuer
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf])) : "memory");
-        }
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const int u = 2 * c + q;
-          const int16_t* sb = sB + (l * IT + hh * HALF + u) * 2;
-          const double sS = w[u] * pow2i(ea + sb[0]), sH = w[u] * pow2i(ea + sb[1]);
-          double v[4];
-#pragma unroll
-          for (int m = 0; m < 4; m++) {
-            uint32_t rr[S];
-#pragma unroll
-            for (int d = 0; d < S; d++) rr[d] = r[d][4 * q + m];
-            v[m] = level_sum<S, PAIR>(rr);
-          }
-          aS[u].x = fma(v[0], sS, aS[u].x);
-          aS[u].y = fma(v[1], sS, aS[u].y);
-          aH[u].x = fma(v[2], sH, aH[u].x);
-          aH[u].y = fma(v[3], sH, aH[u].y);
-        }
-      }
-    }
-    // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
-    if (ok && jin) {
-      const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
-      const int k1 = P.kzz[3 * J], k2 = P.kzz[3 * J + 1], k3 = P.kzz[3 * J + 2];
+      const int J = j0 + 32 * g4 + lane;
+      const bool jin = J < nv;
+      const double xj = jin ? P.xk[J] : 0.0, yj = jin ? P.yk[J] : 0.0, zj = jin ? P.zk[J] : 0.0;
+      const double rj = jin ? P.rk[J] : 0.0;
+      double x[HALF], pm1[HALF], pm2[HALF];
+      double2 aS[HALF], aH[HALF];
 #pragma unroll
       for (int u = 0; u < HALF; u++) {
         const int I = i0 + hh * HALF + u;
-        if (I >= nv || J > I) continue;
-        const double x2 = xj * P.xk[I] + yj * P.yk[I] + zj * P.zk[I];
-        const int d1 = k1 - P.kzz[3 * I] + T.d1, d2 = k2 - P.kzz[3 * I + 1] + T.d2, d3 = k3 - P.kzz[3 * I + 2] + T.d3;
-        const size_t ci = ((size_t)d3 * ny + d2) * nx + d1;
-        const double2 th = tab[2 * ci], wp = tab[2 * ci + 1];
-        const double2 s = cadd(th, aS[u]);
-        const double2 h = cadd(cadd(cscale(th, x2), wp), aH[u]);
-        if (J == I) {
-          hs[(size_t)I * ld + I] = h;
-          hsdiag[I] = s;
-        } else {
-          hs[(size_t)I * ld + J] = s;  // S upper: HS(J,I)
-          hs[(size_t)J * ld + I] = h;  // H lower: HS(I,J)
+        double xx = 0.0;
+        if (jin && I < nv) {
+          xx = P.xk[I] * xj + P.yk[I] * yj + P.zk[I] * zj;
+          const double den = P.rk[I] * rj;
+          if (den > 1.0e-8) xx = xx / den;
+        }
+        x[u] = xx;
+        pm1[u] = xx;   // P_1
+        pm2[u] = 1.0;  // P_0
+        aS[u] = aH[u] = make_double2(0.0, 0.0);
+      }
+      for (int l = 0; l < L; l++, gl++) {
+        const int buf = (int)(gl & 1);
+        // warp-uniform outcome: the TMEM loads below are .sync.aligned
+        if (!__all_sync(0xffffffffu, wait_or_abort(&tfull[buf], (uint32_t)(gl >> 1) & 1, &abort_flag))) {
+          ok = false;
+          if (lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
+          break;
+        }
+        if (__any_sync(0xffffffffu, *(volatile int*)&abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int ea = sA[l * 128 + 32 * g4 + lane] + (LS == 2 ? -7 * (S - 1) : 0);
+        // 4 real columns per I: S re, S im, H re, H im; this thread's HALF I
+        // start at column 4 * HALF * hh; 8 columns (2 I) per chunk, the next
+        // chunk's TMEM loads in flight while this one is accumulated
+        constexpr int NC = HALF / 2;
+        const uint32_t tcol = trow + (uint32_t)(buf * S * N + 4 * HALF * hh);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          uint32_t r[S][8];
+          tmem_ld8<S>(r, tcol + 8 * c, N);
+          tmem_wait<S>(r);
+          double v[8];
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+            uint32_t rr[S];
+#pragma unroll
+            for (int d = 0; d < S; d++) rr[d] = r[d][m];
+            v[m] = level_sum<S, LS>(rr);
+          }
+          if (c + 1 == NC) {
+            // all columns of this buffer read: hand it back to the MMA issuer
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+              asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf])) : "memory");
+          }
+#pragma unroll
+          for (int q = 0; q < 2; q++) {
+            const int u = 2 * c + q;
+            // Legendre weight (hamilt.F:250-281 recursion, UTOP branch)
+            double pl;
+            if (l == 0)
+              pl = 1.0;
+            else if (l == 1)
+              pl = x[u];
+            else {
+              if (fabs(x[u]) < 0.9999999) {
+                const double pplx = x[u] * pm1[u];
+                pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2[u]);
+              } else {
+                pl = x[u] * pm1[u];
+              }
+              pm2[u] = pm1[u];
+              pm1[u] = pl;
+            }
+            const double wl = (double)(2 * l + 1) * pl;
+            const int16_t* sb = sB + (l * IT + hh * HALF + u) * 2;
+            const double sS = wl * pow2i(ea + sb[0]), sH = wl * pow2i(ea + sb[1]);
+            aS[u].x = fma(v[4 * q + 0], sS, aS[u].x);
+            aS[u].y = fma(v[4 * q + 1], sS, aS[u].y);
+            aH[u].x = fma(v[4 * q + 2], sH, aH[u].x);
+            aH[u].y = fma(v[4 * q + 3], sH, aH[u].y);
+          }
         }
       }
+      if (!ok) {
+        *(volatile int*)&abort_flag = 1;
+        break;
+      }
+      // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
+      if (jin) {
+        const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
+        const int k1 = P.kzz[3 * J], k2 = P.kzz[3 * J + 1], k3 = P.kzz[3 * J + 2];
+#pragma unroll
+        for (int u = 0; u < HALF; u++) {
+          const int I = i0 + hh * HALF + u;
+          if (I >= nv || J > I) continue;
+          const double x2 = xj * P.xk[I] + yj * P.yk[I] + zj * P.zk[I];
+          const int d1 = k1 - P.kzz[3 * I] + T.d1, d2 = k2 - P.kzz[3 * I + 1] + T.d2,
+                    d3 = k3 - P.kzz[3 * I + 2] + T.d3;
+          const size_t ci = ((size_t)d3 * ny + d2) * nx + d1;
+          const double2 th = tab[2 * ci], wp = tab[2 * ci + 1];
+          const double2 s = cadd(th, aS[u]);
+          const double2 h = cadd(cadd(cscale(th, x2), wp), aH[u]);
+          if (J == I) {
+            hs[(size_t)I * ld + I] = h;
+            hsdiag[I] = s;
+          } else {
+            hs[(size_t)I * ld + J] = s;  // S upper: HS(J,I)
+            hs[(size_t)J * ld + I] = h;  // H lower: HS(I,J)
+          }
+        }
+      }
+    }
+    if (!ok) {
+      *(volatile int*)&abort_flag = 1;
+      if (lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
     }
   }
   // every MMA issued has completed before TMEM is freed

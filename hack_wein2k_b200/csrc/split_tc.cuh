@@ -77,6 +77,22 @@ __device__ __forceinline__ double i2d_exact(uint32_t x) {
   return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
 }
 
+// x 2^(6 - e): the first int8 digit's scale for a row of exponent e (one
+// multiply by the exact power of two in the normal range, ldexp outside it)
+__device__ __forceinline__ double digit_scale(double x, int e) {
+  const int k = 6 - e;
+  return (k >= -1022 && k <= 1023) ? x * __longlong_as_double((long long)(k + 1023) << 52) : ldexp(x, k);
+}
+// One int8 digit of the slicing: t rounded to the nearest integer (ties to
+// even, as rint) by adding 1.5 2^52, whose low mantissa bits then hold the
+// integer; t becomes the exact remainder scaled by 2^7 for the next digit.
+__device__ __forceinline__ int digit7(double& t) {
+  const double sh = t + 6755399441055744.0;
+  const int d = __double2loint(sh);
+  t = (t - (sh - 6755399441055744.0)) * 128.0;
+  return d;
+}
+
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -156,14 +172,12 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
 #pragma unroll
   for (int t = 0; t < 8; t++) {
     const double2 v = tile[kq + t][rr];
-    double tr = ldexp(v.x, -e) * 64.0, ti = ldexp(v.y, -e) * 64.0;
+    double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
 #pragma unroll
     for (int p = 0; p < S; p++) {
-      const double ar = rint(tr), ai = rint(ti);
-      tr = (tr - ar) * 128.0;
-      ti = (ti - ai) * 128.0;
-      pre[p] |= (uint64_t)(uint8_t)(int8_t)(int)ar << (8 * t);
-      pim[p] |= (uint64_t)(uint8_t)(int8_t)(int)ai << (8 * t);
+      const int ar = digit7(tr), ai = digit7(ti);
+      pre[p] |= (uint64_t)(uint8_t)ar << (8 * t);
+      pim[p] |= (uint64_t)(uint8_t)ai << (8 * t);
     }
   }
   const int col = k0 + kq;
