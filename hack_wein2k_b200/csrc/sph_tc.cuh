@@ -21,9 +21,10 @@
 // overlaps the MMAs of l+1.  After the last l the interstitial terms are
 // gathered from the Theta/WARP table and HS is written as k_spherical does.
 //
-// Warp roles: warps 0-7 epilogue (warp w reads TMEM lanes 32 (w%4).. and
-// the I half w/4 of the tile), warp 8 lane 0 issues the MMAs, warp 9 lane 0
-// the TMA loads (a full ring ahead of the MMAs, whatever they wait on).  Every
+// Warp roles: warps 0..4 EG-1 epilogue (warp w reads TMEM lanes 32 (w%4)..
+// and the I group w/4 of 4 I), warp 4 EG lane 0 issues the MMAs, warp
+// 4 EG + 1 lane 0 the TMA loads (a full ring ahead of the MMAs, whatever
+// they wait on).  Every
 // mbarrier wait is bounded; a timeout sets a status bit and ends the CTA's
 // work cleanly (copies drained, MMAs complete, TMEM freed).
 #pragma once
@@ -46,9 +47,16 @@ using split::tma_load_3d;
 
 template <int S>
 struct Cfg {
-  static constexpr int N = ((512 / (2 * S)) / 16) * 16;  // real columns per accumulator buffer
+  // real columns per level of one accumulator buffer: 4 per I, at most 48
+  // (12 I: three epilogue warp groups of 4 I)
+  static constexpr int NMAX = ((512 / (2 * S)) / 16) * 16;
+  static constexpr int N = NMAX > 48 ? 48 : NMAX;
   static_assert(S * N <= 256, "one MMA per A slice needs (S - p) N <= 256 columns");
-  static constexpr int IT = N / 4;                        // I per tile
+  static constexpr int IT = N / 4;   // I per tile
+  static constexpr int IPT = 4;      // I per epilogue thread
+  static constexpr int EG = IT / IPT;  // epilogue warp groups (4 warps each: the 4 TMEM lane quarters)
+  static_assert(EG * IPT == IT, "I per tile must be a multiple of 4");
+  static constexpr int EPI = 128 * EG;  // epilogue threads
   // one pipeline stage: all S slices of a 64-byte K block of A (128 rows)
   // and of B (N rows)
   static constexpr int A_BYTES = S * 128 * 64;
@@ -59,7 +67,7 @@ struct Cfg {
   static constexpr int STAGES_FIT = (227 * 1024 - SCALE_BYTES - 1024) / STAGE;
   static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
   static constexpr int SMEM = STAGES * STAGE + SCALE_BYTES + 1024;
-  static constexpr int THREADS = 320;
+  static constexpr int THREADS = EPI + 64;  // + the MMA warp and the TMA warp
 };
 
 // Operand rows of one l, built from AL/BL, phases and the per-(type, l)
@@ -216,29 +224,24 @@ __device__ __forceinline__ double level_sum(const uint32_t (&r)[S]) {
   return v;
 }
 
-// S levels x 8 columns of this warp's TMEM lanes into registers (async until
-// tmem_wait)
+// S levels x 4 columns of this warp's TMEM lanes into registers (async until
+// tmem_wait4)
 template <int S>
-__device__ __forceinline__ void tmem_ld8(uint32_t (&r)[S][8], uint32_t addr, int N) {
+__device__ __forceinline__ void tmem_ld4(uint32_t (&r)[S][4], uint32_t addr, int N) {
 #pragma unroll
   for (int d = 0; d < S; d++)
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
-                   "=r"(r[d][6]), "=r"(r[d][7])
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3])
                  : "r"(addr + (uint32_t)(d * N)));
 }
 // wait for this thread's TMEM loads; the registers pass through an empty asm
 // so that no use of them is scheduled before the wait
 template <int S>
-__device__ __forceinline__ void tmem_wait(uint32_t (&r)[S][8]) {
+__device__ __forceinline__ void tmem_wait4(uint32_t (&r)[S][4]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int d = 0; d < S; d++)
-    asm volatile(""
-                 : "+r"(r[d][0]), "+r"(r[d][1]), "+r"(r[d][2]), "+r"(r[d][3]), "+r"(r[d][4]), "+r"(r[d][5]),
-                   "+r"(r[d][6]), "+r"(r[d][7]));
+  for (int d = 0; d < S; d++) asm volatile("" : "+r"(r[d][0]), "+r"(r[d][1]), "+r"(r[d][2]), "+r"(r[d][3]));
 }
-
 // bounded wait that also gives up once another role has raised the abort flag
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, const int* flag) {
   long long t0 = clock64();
@@ -252,13 +255,14 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, co
 // across tiles, so the loads and MMAs of a tile's first l overlap the
 // previous tile's last epilogue, interstitial gather and HS writes.
 template <int S, int LS>
-__global__ void __launch_bounds__(320, 1)
+__global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
     k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
              const int2* __restrict__ tiles, int ntile, int nkb, int khalf, int npA, int npB,
              const int* __restrict__ exA, const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T,
              double2* __restrict__ hs, int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
   using C = Cfg<S>;
-  constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = IT / 2;
+  constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = C::IPT, EPI = C::EPI;
+  constexpr int MMA_WARP = 4 * C::EG, TMA_WARP = 4 * C::EG + 1;
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar, ebar;
   __shared__ uint32_t tmem_slot;
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(320, 1)
   const int L = P.ltop, nv = P.nv;
   const int nit = L * nkb;  // pipeline iterations per tile
 
-  if (warp == 8) {
+  if (warp == MMA_WARP) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
                  "r"(512)
                  : "memory");
@@ -281,10 +285,10 @@ __global__ void __launch_bounds__(320, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 8);  // one arrival per epilogue warp
+      mbar_init(&tempty[b], 4 * C::EG);  // one arrival per epilogue warp
     }
     mbar_init(&accbar, 1);
-    mbar_init(&ebar, 256);  // the epilogue threads' barrier (bounded waits)
+    mbar_init(&ebar, EPI);  // the epilogue threads' barrier (bounded waits)
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(320, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
-  if (warp == 9) {
+  if (warp == TMA_WARP) {
     // ---- TMA producer: a full ring ahead of the MMAs ----
     if (lane == 0) {
       long g = 0;  // iterations issued over all tiles
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(320, 1)
         mbar_wait(&full[q % STAGES], (uint32_t)(q / STAGES) & 1);
     }
     __syncwarp();
-  } else if (warp == 8) {
+  } else if (warp == MMA_WARP) {
     // ---- MMA issuer ----
     if (lane == 0) {
       long g = 0;   // pipeline iterations over all tiles
@@ -402,7 +406,7 @@ __global__ void __launch_bounds__(320, 1)
     long gl = 0;  // accumulations consumed over all tiles
     bool ok = true;
     uint32_t ephase = 0;
-    // barrier of the 256 epilogue threads on an mbarrier, every wait bounded
+    // barrier of the epilogue threads on an mbarrier, every wait bounded
     // (a warp that gave up leaves the others to time out, not to hang);
     // warp-uniform outcome
     auto epi_sync = [&]() -> bool {
@@ -420,11 +424,11 @@ __global__ void __launch_bounds__(320, 1)
         ok = false;
         break;
       }
-      for (int q = tid; q < L * 128; q += 256) {
+      for (int q = tid; q < L * 128; q += EPI) {
         const int l = q >> 7, r = q & 127, J = j0 + r;
         sA[q] = (int16_t)((J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
       }
-      for (int q = tid; q < L * 2 * IT; q += 256) {
+      for (int q = tid; q < L * 2 * IT; q += EPI) {
         const int l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
         sB[q] = (int16_t)((I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
       }
@@ -466,58 +470,53 @@ __global__ void __launch_bounds__(320, 1)
         }
         tc_fence_after();
         const int ea = sA[l * 128 + 32 * g4 + lane] + (LS == 2 ? -7 * (S - 1) : 0);
+        const double cl = (l >= 2) ? (double)(l - 1) / (double)l : 0.0, fl = (double)(2 * l + 1);
         // 4 real columns per I: S re, S im, H re, H im; this thread's HALF I
-        // start at column 4 * HALF * hh; 8 columns (2 I) per chunk, the next
-        // chunk's TMEM loads in flight while this one is accumulated
-        constexpr int NC = HALF / 2;
+        // start at column 4 HALF hh; one I (4 columns x S levels) per load
         const uint32_t tcol = trow + (uint32_t)(buf * S * N + 4 * HALF * hh);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          uint32_t r[S][8];
-          tmem_ld8<S>(r, tcol + 8 * c, N);
-          tmem_wait<S>(r);
-          double v[8];
-#pragma unroll
-          for (int m = 0; m < 8; m++) {
-            uint32_t rr[S];
-#pragma unroll
-            for (int d = 0; d < S; d++) rr[d] = r[d][m];
-            v[m] = level_sum<S, LS>(rr);
-          }
-          if (c + 1 == NC) {
+        for (int u = 0; u < HALF; u++) {
+          uint32_t r[S][4];
+          tmem_ld4<S>(r, tcol + 4 * u, N);
+          tmem_wait4<S>(r);
+          if (u == HALF - 1) {
             // all columns of this buffer read: hand it back to the MMA issuer
             tc_fence_before();
             __syncwarp();
             if (lane == 0)
               asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf])) : "memory");
           }
+          double v[4];
 #pragma unroll
-          for (int q = 0; q < 2; q++) {
-            const int u = 2 * c + q;
-            // Legendre weight (hamilt.F:250-281 recursion, UTOP branch)
-            double pl;
-            if (l == 0)
-              pl = 1.0;
-            else if (l == 1)
-              pl = x[u];
-            else {
-              if (fabs(x[u]) < 0.9999999) {
-                const double pplx = x[u] * pm1[u];
-                pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2[u]);
-              } else {
-                pl = x[u] * pm1[u];
-              }
-              pm2[u] = pm1[u];
-              pm1[u] = pl;
-            }
-            const double wl = (double)(2 * l + 1) * pl;
-            const int16_t* sb = sB + (l * IT + hh * HALF + u) * 2;
-            const double sS = wl * pow2i(ea + sb[0]), sH = wl * pow2i(ea + sb[1]);
-            aS[u].x = fma(v[4 * q + 0], sS, aS[u].x);
-            aS[u].y = fma(v[4 * q + 1], sS, aS[u].y);
-            aH[u].x = fma(v[4 * q + 2], sH, aH[u].x);
-            aH[u].y = fma(v[4 * q + 3], sH, aH[u].y);
+          for (int m = 0; m < 4; m++) {
+            uint32_t rr[S];
+#pragma unroll
+            for (int d = 0; d < S; d++) rr[d] = r[d][m];
+            v[m] = level_sum<S, LS>(rr);
           }
+          // Legendre weight (hamilt.F:250-281 recursion, UTOP branch)
+          double pl;
+          if (l == 0)
+            pl = 1.0;
+          else if (l == 1)
+            pl = x[u];
+          else {
+            if (fabs(x[u]) < 0.9999999) {
+              const double pplx = x[u] * pm1[u];
+              pl = pplx + cl * (pplx - pm2[u]);
+            } else {
+              pl = x[u] * pm1[u];
+            }
+            pm2[u] = pm1[u];
+            pm1[u] = pl;
+          }
+          const double wl = fl * pl;
+          const int16_t* sb = sB + (l * IT + hh * HALF + u) * 2;
+          const double sS = wl * pow2i(ea + sb[0]), sH = wl * pow2i(ea + sb[1]);
+          aS[u].x = fma(v[0], sS, aS[u].x);
+          aS[u].y = fma(v[1], sS, aS[u].y);
+          aH[u].x = fma(v[2], sH, aH[u].x);
+          aH[u].y = fma(v[3], sH, aH[u].y);
         }
       }
       if (!ok) {
@@ -555,10 +554,10 @@ __global__ void __launch_bounds__(320, 1)
     }
   }
   // every MMA issued has completed before TMEM is freed
-  if (warp == 8) mbar_wait(&accbar, 0);
+  if (warp == MMA_WARP) mbar_wait(&accbar, 0);
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == MMA_WARP) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
