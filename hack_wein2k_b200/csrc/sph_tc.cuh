@@ -415,6 +415,25 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
       ephase++;
       return r;
     };
+    // this thread's share of a tile's scale tables, fetched into registers
+    // one tile ahead (behind the previous tile's interstitial part)
+    constexpr int QA = (SPH_LMAX * 128 + EPI - 1) / EPI, QB = (SPH_LMAX * 2 * IT + EPI - 1) / EPI;
+    int16_t pa[QA], pb[QB];
+    auto fetch = [&](int t) {
+      const int2 tt = tiles[t];
+      const int j0 = tt.x * 128, i0 = tt.y * IT;
+#pragma unroll
+      for (int k = 0; k < QA; k++) {
+        const int q = tid + k * EPI, l = q >> 7, J = j0 + (q & 127);
+        pa[k] = (int16_t)((q < L * 128 && J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
+      }
+#pragma unroll
+      for (int k = 0; k < QB; k++) {
+        const int q = tid + k * EPI, l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
+        pb[k] = (int16_t)((q < L * 2 * IT && I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
+      }
+    };
+    if (blockIdx.x < ntile) fetch(blockIdx.x);
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
       const int2 tt = tiles[t];
       const int j0 = tt.x * 128, i0 = tt.y * IT;
@@ -424,14 +443,12 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
         ok = false;
         break;
       }
-      for (int q = tid; q < L * 128; q += EPI) {
-        const int l = q >> 7, r = q & 127, J = j0 + r;
-        sA[q] = (int16_t)((J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
-      }
-      for (int q = tid; q < L * 2 * IT; q += EPI) {
-        const int l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
-        sB[q] = (int16_t)((I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
-      }
+#pragma unroll
+      for (int k = 0; k < QA; k++)
+        if (tid + k * EPI < L * 128) sA[tid + k * EPI] = pa[k];
+#pragma unroll
+      for (int k = 0; k < QB; k++)
+        if (tid + k * EPI < L * 2 * IT) sB[tid + k * EPI] = pb[k];
       if (!epi_sync()) {
         ok = false;
         break;
@@ -523,21 +540,31 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
         *(volatile int*)&abort_flag = 1;
         break;
       }
-      // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164)
+      if (t + (int)gridDim.x < ntile) fetch(t + gridDim.x);
+      // interstitial + write (hamilt.F:289-345, 459-466, calkpt.F:164): every
+      // load of the HALF pairs first (the HS stores might alias them), then
+      // the stores; I past NV reads a valid row and stores nothing
       if (jin) {
         const int nx = 2 * T.d1 + 1, ny = 2 * T.d2 + 1;
         const int k1 = P.kzz[3 * J], k2 = P.kzz[3 * J + 1], k3 = P.kzz[3 * J + 2];
+        double2 th[HALF], wp[HALF];
+        double x2[HALF];
+#pragma unroll
+        for (int u = 0; u < HALF; u++) {
+          const int I = min(i0 + hh * HALF + u, nv - 1);
+          x2[u] = xj * P.xk[I] + yj * P.yk[I] + zj * P.zk[I];
+          const int d1 = k1 - P.kzz[3 * I] + T.d1, d2 = k2 - P.kzz[3 * I + 1] + T.d2,
+                    d3 = k3 - P.kzz[3 * I + 2] + T.d3;
+          const size_t ci = ((size_t)d3 * ny + d2) * nx + d1;
+          th[u] = tab[2 * ci];
+          wp[u] = tab[2 * ci + 1];
+        }
 #pragma unroll
         for (int u = 0; u < HALF; u++) {
           const int I = i0 + hh * HALF + u;
           if (I >= nv || J > I) continue;
-          const double x2 = xj * P.xk[I] + yj * P.yk[I] + zj * P.zk[I];
-          const int d1 = k1 - P.kzz[3 * I] + T.d1, d2 = k2 - P.kzz[3 * I + 1] + T.d2,
-                    d3 = k3 - P.kzz[3 * I + 2] + T.d3;
-          const size_t ci = ((size_t)d3 * ny + d2) * nx + d1;
-          const double2 th = tab[2 * ci], wp = tab[2 * ci + 1];
-          const double2 s = cadd(th, aS[u]);
-          const double2 h = cadd(cadd(cscale(th, x2), wp), aH[u]);
+          const double2 s = cadd(th[u], aS[u]);
+          const double2 h = cadd(cadd(cscale(th[u], x2[u]), wp[u]), aH[u]);
           if (J == I) {
             hs[(size_t)I * ld + I] = h;
             hsdiag[I] = s;
