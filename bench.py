@@ -342,6 +342,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the library's default tuning (profiling runs: timings under a profiler mislead the autotuner)")
     ap.add_argument("--north-star", action="store_true",
                     help="instead: the 100-atom c4 batch (split vs FP64) and c3/c4 adjoint forces, one JSON line")
     args = ap.parse_args()
@@ -382,7 +384,10 @@ def main():
     d_hs = torch.empty((n, n, 2), dtype=torch.float64, device=device)  # column-major view: [col][row]
     d_hd = torch.empty((n, 2), dtype=torch.float64, device=device)
     torch.cuda.synchronize()
-    tuning = ctx.autotune(kp, d_hs.data_ptr(), n, d_hd.data_ptr())  # untimed: picks tile/schedule parameters
+    if args.no_autotune:
+        tuning = ctx.tuning()
+    else:
+        tuning = ctx.autotune(kp, d_hs.data_ptr(), n, d_hd.data_ptr())  # untimed: picks tile/schedule parameters
 
     def step(stats=True):
         return kp.run(d_hs.data_ptr(), n, d_hd.data_ptr(), stages=7, stats=stats)

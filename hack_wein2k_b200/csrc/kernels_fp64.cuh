@@ -610,77 +610,73 @@ __global__ void k_hns_alm(DevProb P, const LoRange* __restrict__ lor, int nlor, 
   }
 }
 
-#define TMUL_I 64
-#define TMUL_CH 4  // 64-row chunks per block: M is staged once for all of them
+#define TMUL_I 64        // columns (basis rows i) per work item
+#define TMUL_ROWS 10     // rows of L per thread (one warp: 10 rows x 64 columns)
+#define TMUL_WARPS 5     // 5 x 10 >= 2 NSL2 = 50 rows
 #define TMUL_SMEM ((2 * L1G_NSL2) * (2 * L1G_NSL2) * 16 + (2 * L1G_NSL2) * TMUL_I * 16)
 // L[(a, r_out, la)][i] = sum_{(r, b)} M[(r_out, la)][(r, b)] conj(R[(a, r, b)][i])
-// One block per (atom, TMUL_CH x 64 rows); the next chunk of R is fetched
-// into registers while the current one is multiplied.
-__global__ void __launch_bounds__(256, 2) k_hns_tmul(int npad, int nsl2, const int* __restrict__ atype,
-                                                  const double2* __restrict__ tns, const double2* __restrict__ Rop,
-                                                  double2* __restrict__ Lop) {
+// A work item is (atom, 64 columns i); block b takes the contiguous items
+// [b per, (b+1) per) (one atom for most of them: M is staged again only
+// when the atom changes).  Thread (warp w, lane): rows 10 w .. 10 w + 9 and
+// columns lane, lane + 32 of the item, 20 complex accumulators; per k two
+// R values (conflict-free rows of smem) and ten broadcast M values.
+__global__ void __launch_bounds__(32 * TMUL_WARPS, 2) k_hns_tmul(int npad, int nsl2, int ndf, int per,
+                                                              const int* __restrict__ atype,
+                                                              const double2* __restrict__ tns,
+                                                              const double2* __restrict__ Rop,
+                                                              double2* __restrict__ Lop) {
   extern __shared__ double2 tm[];
   const int K = 2 * nsl2;
   double2* sM = tm;          // [K][K]
   double2* sR = tm + K * K;  // [K][TMUL_I]
-  const int a = blockIdx.y;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  for (int idx = tid; idx < K * K; idx += 256) {
-    const int row = idx / K, col = idx % K;
-    const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
-    const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
-    sM[idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
-  }
-  const double2* R = Rop + (size_t)a * K * npad;
-  double2* L = Lop + (size_t)a * K * npad;
-  constexpr int PF = (2 * L1G_NSL2 * TMUL_I + 255) / 256;  // R values per thread per chunk
-  double2 pre[PF];
-  auto fetch = [&](int i0) {
-#pragma unroll
-    for (int q = 0; q < PF; q++) {
-      const int idx = tid + 256 * q;
-      pre[q] = (idx < K * TMUL_I && i0 < npad) ? R[(size_t)(idx / TMUL_I) * npad + i0 + idx % TMUL_I]
-                                               : make_double2(0.0, 0.0);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nch = (npad + TMUL_I - 1) / TMUL_I, nitem = nch * ndf;
+  const int it0 = blockIdx.x * per, it1 = min(nitem, it0 + per);
+  int staged = -1;
+  for (int item = it0; item < it1; item++) {
+    const int a = item / nch, i0 = (item % nch) * TMUL_I;
+    __syncthreads();  // the previous item's smem reads are done
+    if (a != staged) {
+      const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+      for (int idx = tid; idx < K * K; idx += 32 * TMUL_WARPS) {
+        const int row = idx / K, col = idx % K;
+        const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
+        const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
+        sM[idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
+      }
+      staged = a;
     }
-  };
-  const int c0 = blockIdx.x * TMUL_CH;
-  fetch(c0 * TMUL_I);
-  constexpr int PR = (2 * L1G_NSL2 + 7) / 8;  // output rows per thread
-  for (int ch = c0; ch < c0 + TMUL_CH; ch++) {
-    const int i0 = ch * TMUL_I;
-    if (i0 >= npad) break;  // uniform across the block
-    __syncthreads();       // the previous chunk's sR reads are done
-#pragma unroll
-    for (int q = 0; q < PF; q++) {
-      const int idx = tid + 256 * q;
-      if (idx < K * TMUL_I) sR[idx] = pre[q];
+    const double2* R = Rop + (size_t)a * K * npad;
+    for (int idx = tid; idx < K * TMUL_I; idx += 32 * TMUL_WARPS) {
+      const int k = idx / TMUL_I, c = idx % TMUL_I;
+      sR[idx] = (i0 + c < npad) ? R[(size_t)k * npad + i0 + c] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    if (ch + 1 < c0 + TMUL_CH) fetch(i0 + TMUL_I);
-    double2 acc[PR][2];
+    const int r0 = w * TMUL_ROWS;
+    if (r0 < K) {  // warp-uniform
+      double2 acc[TMUL_ROWS][2];
 #pragma unroll
-    for (int p = 0; p < PR; p++) acc[p][0] = acc[p][1] = cmk(0.0, 0.0);
-    for (int k = 0; k < K; k++) {
-      const double2 x0 = sR[k * TMUL_I + tx], x1 = sR[k * TMUL_I + tx + 32];
+      for (int r = 0; r < TMUL_ROWS; r++) acc[r][0] = acc[r][1] = cmk(0.0, 0.0);
+#pragma unroll 2
+      for (int k = 0; k < K; k++) {
+        const double2 x0 = sR[k * TMUL_I + lane], x1 = sR[k * TMUL_I + lane + 32];
 #pragma unroll
-      for (int p = 0; p < PR; p++) {
-        const int row = ty + 8 * p;
-        if (row < K) {
-          const double2 m = sM[row * K + k];
-          acc[p][0].x = fma(m.x, x0.x, fma(m.y, x0.y, acc[p][0].x));
-          acc[p][0].y = fma(m.y, x0.x, fma(-m.x, x0.y, acc[p][0].y));
-          acc[p][1].x = fma(m.x, x1.x, fma(m.y, x1.y, acc[p][1].x));
-          acc[p][1].y = fma(m.y, x1.x, fma(-m.x, x1.y, acc[p][1].y));
+        for (int r = 0; r < TMUL_ROWS; r++) {
+          const double2 m = sM[min(r0 + r, K - 1) * K + k];  // rows past K: computed, not stored
+          acc[r][0].x = fma(m.x, x0.x, fma(m.y, x0.y, acc[r][0].x));
+          acc[r][0].y = fma(m.y, x0.x, fma(-m.x, x0.y, acc[r][0].y));
+          acc[r][1].x = fma(m.x, x1.x, fma(m.y, x1.y, acc[r][1].x));
+          acc[r][1].y = fma(m.y, x1.x, fma(-m.x, x1.y, acc[r][1].y));
         }
       }
-    }
+      double2* L = Lop + (size_t)a * K * npad;
 #pragma unroll
-    for (int p = 0; p < PR; p++) {
-      const int row = ty + 8 * p;
-      if (row < K) {
-        L[(size_t)row * npad + i0 + tx] = acc[p][0];
-        L[(size_t)row * npad + i0 + tx + 32] = acc[p][1];
+      for (int r = 0; r < TMUL_ROWS; r++) {
+        const int row = r0 + r;
+        if (row < K) {
+          if (i0 + lane < npad) L[(size_t)row * npad + i0 + lane] = acc[r][0];
+          if (i0 + lane + 32 < npad) L[(size_t)row * npad + i0 + lane + 32] = acc[r][1];
+        }
       }
     }
   }

@@ -612,8 +612,14 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
   if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
         : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
     return LAPW1GPU_ERR_CUDA;
-  k_hns_tmul<<<dim3((P.npad / TMUL_I + TMUL_CH - 1) / TMUL_CH, P.ndf), 256, TMUL_SMEM, s>>>(P.npad, nsl2, P.atype,
-                                                                                           tns, Rop, Lop);
+  {
+    // two blocks per SM over the (atom, 64-column) items, contiguous ranges
+    const int nitem = (P.npad + TMUL_I - 1) / TMUL_I * P.ndf;
+    const int nblk = std::max(1, std::min(nitem, 2 * (c ? c->nsm : 148)));
+    const int per = (nitem + nblk - 1) / nblk;
+    k_hns_tmul<<<(nitem + per - 1) / per, 32 * TMUL_WARPS, TMUL_SMEM, s>>>(P.npad, nsl2, P.ndf, per, P.atype, tns,
+                                                                         Rop, Lop);
+  }
   *nl += 2;
   if (P.nlo > 0) {
     k_hns_lo_ops<<<dim3((P.nlo + 7) / 8, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo, C2lo);

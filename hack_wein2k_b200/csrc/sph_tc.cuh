@@ -174,10 +174,11 @@ __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* 
   }
 }
 
-// 2^e as a double (exponent bits for the normal range, 0 far below it)
+// 2^e as a double from its exponent bits: exact for -1022 <= e <= 1023,
+// 0 below that range and infinity above it (no branch)
 __device__ __forceinline__ double pow2i(int e) {
-  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52)
-                                   : (e < -1022 ? 0.0 : ldexp(1.0, e));
+  const double v = __longlong_as_double((long long)(min(max(e, -1023), 1024) + 1023) << 52);
+  return e < -1022 ? 0.0 : v;
 }
 
 // Level sum of one accumulator column, sum_d c_d 2^(-7d), in one of three
