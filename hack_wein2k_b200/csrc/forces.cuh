@@ -41,8 +41,8 @@
 
 __global__ void __launch_bounds__(SPH_THREADS, 1)
     k_force_sph(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef, TabDesc T,
-                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, double* __restrict__ F,
-                double* __restrict__ bins) {
+                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, int rt,
+                double* __restrict__ F, double* __restrict__ bins) {
   extern __shared__ double2 sm2[];
   double2* sJ = sm2;
   double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
@@ -78,8 +78,9 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
         dx[q][0] = FRC_2PI * d0;
         dx[q][1] = FRC_2PI * d1;
         dx[q][2] = FRC_2PI * d2;
-        rj[q] = rho[(size_t)I * ldr + J];
-        re[q] = rhoe[(size_t)I * ldr + J];
+        // rt: the density matrices hold conj(rho(J,I)) at (I, J) instead
+        rj[q] = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
+        re[q] = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
         // the step-function term depends on the pair only through dK =
         // KZZ_I - KZZ_J: bin x2 rho - rhoE by dK (k_force_step finishes it)
         const size_t b = (((size_t)(d2 + T.d3) * (2 * T.d2 + 1)) + (d1 + T.d2)) * (2 * T.d1 + 1) + (d0 + T.d1);
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256) k_force_step(DevProb P, TabDesc T, const 
 
 // local-orbital columns: k_lo's terms per equivalent atom, reduced per warp
 __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const double2* __restrict__ rho,
-                           const double2* __restrict__ rhoe, int ldr, double* __restrict__ F) {
+                           const double2* __restrict__ rhoe, int ldr, int rt, double* __restrict__ F) {
   const LoCol c = cols[blockIdx.y];
   const int nv = P.nv;
   const int I = nv + c.nnlo - 1;
@@ -317,8 +318,8 @@ __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const doub
     dxc[0] = FRC_2PI * (P.kzz[3 * I] - P.kzz[3 * J]);
     dxc[1] = FRC_2PI * (P.kzz[3 * I + 1] - P.kzz[3 * J + 1]);
     dxc[2] = FRC_2PI * (P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
-    rj = rho[(size_t)I * ldr + J];
-    re = rhoe[(size_t)I * ldr + J];
+    rj = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
+    re = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
     if (J < nv) {
       size_t oo = ((size_t)jn * P.ltop + l) * P.nvpad + J;
       alj = P.al[oo];
@@ -408,12 +409,16 @@ __global__ void k_force_gscale(int n, int nb, const int* __restrict__ kzz, const
 }
 
 // occupation- and energy-weighted copies of the eigenvector block
+// Cf = f c, Ce = f eps c per band (cj: their conjugates, for the split
+// path's products C conj(Cf)^T, which take no conjugate themselves)
 __global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int ldc, const double* __restrict__ f,
-                               const double* __restrict__ eps, double2* __restrict__ Cf, double2* __restrict__ Ce) {
+                               const double* __restrict__ eps, int cj, double2* __restrict__ Cf,
+                               double2* __restrict__ Ce) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   if (i >= n) return;
-  const double2 v = C[(size_t)b * ldc + i];
+  double2 v = C[(size_t)b * ldc + i];
+  if (cj) v = cconj(v);
   Cf[(size_t)b * n + i] = cscale(v, f[b]);
   Ce[(size_t)b * n + i] = cscale(v, f[b] * eps[b]);
 }

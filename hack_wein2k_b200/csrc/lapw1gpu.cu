@@ -1442,17 +1442,40 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
   k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
   k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
-  k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, Cf, Ce);
+  const bool split_rho = c->prec == LAPW1GPU_PREC_SPLIT;
+  k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, split_rho ? 1 : 0, Cf, Ce);
   CK(cudaGetLastError());
   // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)), column-major n x n, and rhoE:
-  // Hermitian, and only J < I is read, so the library forms the upper
-  // triangle alone (half the flops of a full product)
-  const double rzero = 0.0;
-  if (cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Cf, n,
-                   (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
-      cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Ce, n,
-                   (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
-    return LAPW1GPU_ERR_CUDA;
+  // Hermitian, and only J < I is read.  FP64: the library forms the upper
+  // triangle alone (half the flops of a full product).  Split precision:
+  // the int8 slice-product kernel of the HNS update forms the lower
+  // triangle of C X^T with X = conj(Cf) (k_force_weight conjugated it), i.e.
+  // conj(rho(J,I)) at (I, J) (rt = 1 below).
+  int rt = 0;
+  if (split_rho) {
+    const double2* Cn = C;
+    if (ldc != n) {  // the operand kernels take one row stride for both sides
+      double2* Cc = (double2*)c->buf("frc_c", sizeof(double2) * (size_t)n * nb);
+      if (!Cc) return LAPW1GPU_ERR_NOMEM;
+      CK(cudaMemcpy2DAsync(Cc, sizeof(double2) * n, C, sizeof(double2) * ldc, sizeof(double2) * n, nb,
+                           cudaMemcpyDeviceToDevice, s));
+      Cn = Cc;
+    }
+    CK(cudaMemsetAsync(rho, 0, sizeof(double2) * (size_t)n * n, s));
+    CK(cudaMemsetAsync(rhoe, 0, sizeof(double2) * (size_t)n * n, s));
+    int nlr = 0;
+    int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices, s, &nlr, nullptr, nullptr);
+    if (!rc) rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices, s, &nlr, nullptr, nullptr);
+    if (rc) return rc;
+    rt = 1;
+  } else {
+    const double rzero = 0.0;
+    if (cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Cf, n,
+                     (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rho, n) != CUBLAS_STATUS_SUCCESS ||
+        cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Ce, n,
+                     (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
+      return LAPW1GPU_ERR_CUDA;
+  }
   int ntiles = 0;
   const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
@@ -1461,10 +1484,10 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   double* bins = (double*)c->buf("frc_bins", sizeof(double) * 2 * nbox);
   if (!bins) return LAPW1GPU_ERR_NOMEM;
   CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
-  k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, d_grad, bins);
+  k_force_sph<<<ntiles, SPH_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, rt, d_grad, bins);
   k_force_step<<<ndf, 256, 0, s>>>(P, k->tab, bins, d_grad);
   CK(cudaGetLastError());
-  if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, d_grad);
+  if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, rt, d_grad);
   CK(cudaGetLastError());
   if (!k->nohns) {
     const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);

@@ -44,6 +44,30 @@ def test_adjoint_matches_oracle_hellmann_feynman(ctx, kind):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", KINDS)
+def test_split_density_matrices_match_fp64(ctx, kind):
+    """In split precision lapw1gpu_forces forms rho and rhoE as int8 slice
+    products (5 slices); for the same eigenvectors the gradient agrees with
+    the FP64 one (ZHERKX density matrices) to 1e-8 of its largest component."""
+    p = synth.small_case(kind)
+    w, _ = FR.eigh(p)
+    nb, _ = FR.gapped_nb(w)
+    dev = torch.device("cuda", ctx.device)
+    occ = _occ(p, nb).to(dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    g64 = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    try:
+        gs = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    kp.free()
+    scale = np.abs(g64).max()
+    assert scale > 0
+    assert np.abs(gs - g64).max() <= 1e-8 * scale, (gs, g64)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["lo", "ins"])
 def test_autograd_matches_band_energy_fd(ctx, kind):
     p = synth.small_case(kind)
