@@ -409,6 +409,26 @@ __global__ void k_force_gscale(int n, int nb, const int* __restrict__ kzz, const
 }
 
 // occupation- and energy-weighted copies of the eigenvector block
+// out[c][r] = in[r][c] (conjugated when cj): in is rows x cols with row
+// stride ldi, out cols x rows with row stride ldo; 32 x 32 tiles through
+// shared memory, both sides coalesced
+__global__ void __launch_bounds__(256) k_force_trans(const double2* __restrict__ in, int ldi, int rows, int cols,
+                                                     int cj, double2* __restrict__ out, int ldo) {
+  __shared__ double2 t[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int y = ty; y < 32; y += 8) {
+    const int r = r0 + y, c = c0 + tx;
+    double2 v = (r < rows && c < cols) ? in[(size_t)r * ldi + c] : cmk(0.0, 0.0);
+    t[y][tx] = cj ? cconj(v) : v;
+  }
+  __syncthreads();
+  for (int y = ty; y < 32; y += 8) {
+    const int c = c0 + y, r = r0 + tx;
+    if (c < cols && r < rows) out[(size_t)c * ldo + r] = t[tx][y];
+  }
+}
+
 // Cf = f c, Ce = f eps c per band (cj: their conjugates, for the split
 // path's products C conj(Cf)^T, which take no conjugate themselves)
 __global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int ldc, const double* __restrict__ f,

@@ -1507,10 +1507,22 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
     CK(cudaGetLastError());
     // Y = R^H (G c): K x 4nb (rows of R beyond n unused); Yc = CLM^H (G c)
-    // over the LO rows; Z = T (Y; Yc) per atom
-    if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
-                    (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS)
+    // over the LO rows; Z = T (Y; Yc) per atom.  Split precision: Y as int8
+    // slice products over the n rows, from k-major copies conj(R)^T, (G c)^T
+    if (split_rho) {
+      double2* Lt = (double2*)c->buf("frc_rt", sizeof(double2) * (size_t)n * K);
+      double2* Gt = (double2*)c->buf("frc_gt", sizeof(double2) * (size_t)n * 4 * nb);
+      if (!Lt || !Gt) return LAPW1GPU_ERR_NOMEM;
+      k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
+      k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
+      CK(cudaMemsetAsync(Y, 0, sizeof(double2) * (size_t)4 * nb * K, s));
+      int nly = 0;
+      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices, s, &nly);
+      if (rc) return rc;
+    } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
+                           (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS) {
       return LAPW1GPU_ERR_CUDA;
+    }
     double2* Yc = nullptr;
     double2* Zc = nullptr;
     if (nlo > 0) {

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
 template <int S>
 __global__ void __launch_bounds__(128, 1)
     k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                 const int2* __restrict__ tiles, int nkb, int n, const int* __restrict__ exA,
+                 const int2* __restrict__ tiles, int nkb, int n, int nr, int rect, const int* __restrict__ exA,
                  const int* __restrict__ exB, double2* __restrict__ hs, int ld, int* __restrict__ status) {
   using C = Cfg<S>;
   constexpr int N = C::N, STAGES = C::STAGES;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
         for (int q = 0; q < 8; q++) {
           const int j = j0 + c * 8 + q;
-          if (j < n && j <= i) {
+          if (j < nr && (rect || j <= i)) {
             const double sc = sa * ldexp(1.0, exB[j]);
             double2* dst = hs + (size_t)j * ld + i;
             double2 o = *dst;
@@ -467,7 +467,7 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
                                       if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
                               });
     if (!dt) return LAPW1GPU_ERR_NOMEM;
-    split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, exA, exB, hs, ld,
+    split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, n, 0, exA, exB, hs, ld,
                                                                    c->d_status);
     *nlaunch += 1;
     if (hp && hp->groups > 0 && hp->col[g + 1] <= k->nv) {
@@ -477,6 +477,64 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
   }
   if (ev && cudaEventRecord(ev[1], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+// Rectangular product out(i, j) += sum_k L(i, k) R(j, k), i < m, j < nr,
+// every tile (no triangle), complex operands in k-major planes: L[k][npadL],
+// R[k][npadR] (npadL >= m, npadR >= nr); out column-major with ld.
+template <int S>
+static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
+                           const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
+                           cudaStream_t s, int* nlaunch) {
+  using Cf = split::Cfg<S>;
+  const int Kcp = (Kc + 63) / 64 * 64;
+  const int Kp = 2 * Kcp;
+  const int npL = (npadL + 127) / 128 * 128, npR = (npadR + 127) / 128 * 128;
+  int8_t* A = (int8_t*)c->sbuf(set, "rectA", (size_t)S * npL * Kp);
+  int8_t* B = (int8_t*)c->sbuf(set, "rectB", (size_t)S * 2 * npR * Kp);
+  int* exA = (int*)c->sbuf(set, "rectExA", sizeof(int) * npL);
+  int* exB = (int*)c->sbuf(set, "rectExB", sizeof(int) * npR);
+  if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
+  if (cudaMemsetAsync(exA, 0x80, sizeof(int) * npL, s) != cudaSuccess ||
+      cudaMemsetAsync(exB, 0x80, sizeof(int) * npR, s) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  split::k_rowexp<<<dim3((npadL + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Lop, Kc, npadL, exA);
+  split::k_rowexp<<<dim3((npadR + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Rop, Kc, npadR, exB);
+  split::k_slice_rows<S><<<dim3(npL / 32, Kcp / 64), 256, 0, s>>>(Lop, Kc, Kcp, npadL, npL, 0, exA, A);
+  split::k_slice_rows<S><<<dim3(npR / 32, Kcp / 64), 256, 0, s>>>(Rop, Kc, Kcp, npadR, npR, 1, exB, B);
+  *nlaunch += 4;
+  CUtensorMap ta, tb;
+  if (l1g_tmap_3d(&ta, A, Kp, npL, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)npR, S, Cf::N))
+    return LAPW1GPU_ERR_CUDA;
+  const int W = c->split_group;
+  const int nbi = (m + 127) / 128, nbj = (nr + Cf::JT - 1) / Cf::JT;
+  int ntile = 0;
+  const int2* dt = kp_tiles(k,
+                            "rect:" + std::to_string(m) + ":" + std::to_string(nr) + ":" + std::to_string(Cf::JT) +
+                                ":" + std::to_string(W),
+                            &ntile, [&](std::vector<int2>& t) {
+                              for (int g0 = 0; g0 < nbi; g0 += W)
+                                for (int bj = 0; bj < nbj; bj++)
+                                  for (int bi = g0; bi < std::min(nbi, g0 + W); bi++) t.push_back(make_int2(bi, bj));
+                            });
+  if (!dt) return LAPW1GPU_ERR_NOMEM;
+  if (!c->smem((const void*)split::k_split_gemm<S>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
+  split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, 1, exA, exB, out, ld,
+                                                                 c->d_status);
+  *nlaunch += 1;
+  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+}
+
+static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
+                           const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
+                           int slices, cudaStream_t s, int* nlaunch) {
+  switch (slices) {
+    case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
+    case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
+    case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
+    case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
+    default: return LAPW1GPU_ERR_RANGE;
+  }
 }
 
 static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
