@@ -132,43 +132,29 @@ __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* 
     }
     __syncthreads();
   }
-  const int rr = tid >> 3;       // complex row within the block
-  const int kq = (tid & 7) * 8;  // 8 consecutive k
-  const int rc = rc0 + rr;
-  const int e = rexp[rr];
+  // one element per thread and pass, lanes along k: conflict-free tile
+  // reads (stride 33) and byte stores coalesced along each row
   const size_t plane = (size_t)L * nrow_real * Kp;  // one slice plane
-  for (int k0 = 0; k0 < Kcp; k0 += 64) {
-    const int col = k0 + kq;
-    if (col >= Kcp || rc >= ncrow) continue;
-    uint64_t pre[S], pim[S];
-#pragma unroll
-    for (int p = 0; p < S; p++) pre[p] = pim[p] = 0;
-#pragma unroll
-    for (int t = 0; t < 8; t++) {
-      const int k = col + t;
-      const double2 v = (k < Kc) ? tile[k * 33 + rr] : make_double2(0.0, 0.0);
-      double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
-#pragma unroll
-      for (int p = 0; p < S; p++) {
-        const int ar = digit7(tr), ai = digit7(ti);
-        pre[p] |= (uint64_t)(uint8_t)ar << (8 * t);
-        pim[p] |= (uint64_t)(uint8_t)ai << (8 * t);
-      }
-    }
+  int8_t* lbase = out + (size_t)l * nrow_real * Kp;
+  for (int idx = tid; idx < 32 * Kcp; idx += 256) {
+    const int rr = idx / Kcp, k = idx - rr * Kcp;
+    const int rc = rc0 + rr;
+    if (rc >= ncrow) continue;
+    const int e = rexp[rr];
+    const double2 v = (k < Kc) ? tile[k * 33 + rr] : make_double2(0.0, 0.0);
+    double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
 #pragma unroll
     for (int p = 0; p < S; p++) {
-      int8_t* base = out + (size_t)p * plane + (size_t)l * nrow_real * Kp;
+      const int8_t ar = (int8_t)digit7(tr), ai = (int8_t)digit7(ti);
+      int8_t* base = lbase + (size_t)p * plane;
       if (!isB) {
-        *(uint64_t*)(base + (size_t)rc * Kp + col) = pre[p];
-        *(uint64_t*)(base + (size_t)rc * Kp + Kcp + col) = pim[p];
+        base[(size_t)rc * Kp + k] = ar;
+        base[(size_t)rc * Kp + Kcp + k] = ai;
       } else {
-        uint64_t nim = 0;
-#pragma unroll
-        for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
-        *(uint64_t*)(base + (size_t)(2 * rc) * Kp + col) = pre[p];
-        *(uint64_t*)(base + (size_t)(2 * rc) * Kp + Kcp + col) = pim[p];
-        *(uint64_t*)(base + (size_t)(2 * rc + 1) * Kp + col) = nim;
-        *(uint64_t*)(base + (size_t)(2 * rc + 1) * Kp + Kcp + col) = pre[p];
+        base[(size_t)(2 * rc) * Kp + k] = ar;
+        base[(size_t)(2 * rc) * Kp + Kcp + k] = ai;
+        base[(size_t)(2 * rc + 1) * Kp + k] = (int8_t)(-ai);
+        base[(size_t)(2 * rc + 1) * Kp + Kcp + k] = ar;
       }
     }
   }

@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
                                                        int np_out, int isB, const int* __restrict__ ex,
                                                        int8_t* __restrict__ out) {
   __shared__ double2 tile[64][33];
+  __shared__ int rexp[32];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
   const int tid = threadIdx.x;
   const int Kp = 2 * Kcp;
@@ -160,41 +161,30 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
     const int k = k0 + kk, row = r0 + r;
     tile[kk][r] = (k < Kc && row < npad) ? X[(size_t)k * npad + row] : make_double2(0.0, 0.0);
   }
+  if (tid < 32) rexp[tid] = (r0 + tid < np_out) ? ex[r0 + tid] : 0;
   __syncthreads();
-  const int rr = tid >> 3;       // row within the block
-  const int kq = (tid & 7) * 8;  // 8 consecutive k
-  const int row = r0 + rr;
-  if (row >= np_out) return;
-  const int e = ex[row];
-  uint64_t pre[S], pim[S];
-#pragma unroll
-  for (int p = 0; p < S; p++) pre[p] = pim[p] = 0;
-#pragma unroll
-  for (int t = 0; t < 8; t++) {
-    const double2 v = tile[kq + t][rr];
+  // one element per thread and pass, lanes along k: conflict-free tile
+  // reads (stride 33) and byte stores coalesced along each row
+  for (int idx = tid; idx < 32 * 64; idx += 256) {
+    const int rr = idx >> 6, kk = idx & 63;
+    const int row = r0 + rr, col = k0 + kk;
+    if (row >= np_out || col >= Kcp) continue;
+    const int e = rexp[rr];
+    const double2 v = tile[kk][rr];
     double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
 #pragma unroll
     for (int p = 0; p < S; p++) {
-      const int ar = digit7(tr), ai = digit7(ti);
-      pre[p] |= (uint64_t)(uint8_t)ar << (8 * t);
-      pim[p] |= (uint64_t)(uint8_t)ai << (8 * t);
-    }
-  }
-  const int col = k0 + kq;
-#pragma unroll
-  for (int p = 0; p < S; p++) {
-    int8_t* base = out + (size_t)p * rows * Kp;
-    if (!isB) {
-      *(uint64_t*)(base + (size_t)row * Kp + col) = pre[p];
-      *(uint64_t*)(base + (size_t)row * Kp + Kcp + col) = pim[p];
-    } else {
-      uint64_t nim = 0;
-#pragma unroll
-      for (int t = 0; t < 8; t++) nim |= (uint64_t)(uint8_t)(int8_t)(-(int8_t)(uint8_t)(pim[p] >> (8 * t))) << (8 * t);
-      *(uint64_t*)(base + (2 * (size_t)row) * Kp + col) = pre[p];
-      *(uint64_t*)(base + (2 * (size_t)row) * Kp + Kcp + col) = nim;
-      *(uint64_t*)(base + (2 * (size_t)row + 1) * Kp + col) = pim[p];
-      *(uint64_t*)(base + (2 * (size_t)row + 1) * Kp + Kcp + col) = pre[p];
+      const int8_t ar = (int8_t)digit7(tr), ai = (int8_t)digit7(ti);
+      int8_t* base = out + (size_t)p * rows * Kp;
+      if (!isB) {
+        base[(size_t)row * Kp + col] = ar;
+        base[(size_t)row * Kp + Kcp + col] = ai;
+      } else {
+        base[(2 * (size_t)row) * Kp + col] = ar;
+        base[(2 * (size_t)row) * Kp + Kcp + col] = (int8_t)(-ai);
+        base[(2 * (size_t)row + 1) * Kp + col] = ai;
+        base[(2 * (size_t)row + 1) * Kp + Kcp + col] = ar;
+      }
     }
   }
 }
