@@ -39,7 +39,12 @@
 #define FRC_RED_ATOMS SPH_MAXA
 #define FRC_2PI 6.283185307179586476925287
 
-__global__ void __launch_bounds__(SPH_THREADS, 1)
+// One block per 32 x 32 pair tile, 512 threads: thread (tj = lane, ti =
+// warp) owns the pairs (J = j0 + tj, I = i0 + ti + 16 v), v = 0, 1, with
+// their Legendre weights in registers (16 warps per SM: the FP64 chains of
+// the l sums need the occupancy).
+#define FRC_THREADS 512
+__global__ void __launch_bounds__(FRC_THREADS, 1)
     k_force_sph(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef, TabDesc T,
                 const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, int rt,
                 double* __restrict__ F, double* __restrict__ bins) {
@@ -48,64 +53,62 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
   double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
   double2* sPJ = sI + 2 * SPH_TC * SPH_LMAX * SPH_T;
   double2* sPI = sPJ + SPH_MAXA * SPH_T;
-  __shared__ double red[FRC_RED_ATOMS][3][SPH_THREADS / 32];
+  __shared__ double red[FRC_RED_ATOMS][3][FRC_THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tj = tid & 15, ti = tid >> 4;
+  const int tj = lane, ti = warp;
   const int2 t = tiles[blockIdx.x];
   const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
   const int nv = P.nv, ltop = P.ltop, nat = P.nat;
 
-  double w[4][SPH_LMAX];
-  double dx[4][3];
-  double2 rj[4], re[4];  // rho(J,I) and rhoE(J,I) of the owned pairs
-  bool act[4];
+  double w[2][SPH_LMAX];
+  double dx[2][3];
+  double2 rj[2], re[2];  // rho(J,I) and rhoE(J,I) of the owned pairs
+  bool act[2];
+  const int J = j0 + tj;
 #pragma unroll
-  for (int u = 0; u < 2; u++)
-#pragma unroll
-    for (int v = 0; v < 2; v++) {
-      const int q = u * 2 + v;
-      const int J = j0 + tj + 16 * u, I = i0 + ti + 16 * v;
-      act[q] = (J < nv && I < nv && J < I);
-      double x = 0.0;
-      dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
-      rj[q] = re[q] = cmk(0.0, 0.0);
-      if (act[q]) {
-        x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
-        double den = P.rk[I] * P.rk[J];
-        if (den > 1.0e-8) x = x / den;
-        const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
-                  d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
-        dx[q][0] = FRC_2PI * d0;
-        dx[q][1] = FRC_2PI * d1;
-        dx[q][2] = FRC_2PI * d2;
-        // rt: the density matrices hold conj(rho(J,I)) at (I, J) instead
-        rj[q] = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
-        re[q] = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
-        // the step-function term depends on the pair only through dK =
-        // KZZ_I - KZZ_J: bin x2 rho - rhoE by dK (k_force_step finishes it)
-        const size_t b = (((size_t)(d2 + T.d3) * (2 * T.d2 + 1)) + (d1 + T.d2)) * (2 * T.d1 + 1) + (d0 + T.d1);
-        const double x2q = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
-        atomicAdd(&bins[2 * b], x2q * rj[q].x - re[q].x);
-        atomicAdd(&bins[2 * b + 1], x2q * rj[q].y - re[q].y);
-      }
-      const bool top = !(fabs(x) < 0.9999999);
-      double pm2 = 1.0, pm1 = x;
-      w[q][0] = 1.0;
-      w[q][1] = 3.0 * x;
-#pragma unroll
-      for (int l = 2; l < SPH_LMAX; l++) {
-        double pl;
-        if (!top) {
-          const double pplx = x * pm1;
-          pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2);
-        } else {
-          pl = x * pm1;
-        }
-        pm2 = pm1;
-        pm1 = pl;
-        w[q][l] = (double)(2 * l + 1) * pl;
-      }
+  for (int q = 0; q < 2; q++) {
+    const int I = i0 + ti + 16 * q;
+    act[q] = (J < nv && I < nv && J < I);
+    double x = 0.0;
+    dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
+    rj[q] = re[q] = cmk(0.0, 0.0);
+    if (act[q]) {
+      x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
+      double den = P.rk[I] * P.rk[J];
+      if (den > 1.0e-8) x = x / den;
+      const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
+                d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
+      dx[q][0] = FRC_2PI * d0;
+      dx[q][1] = FRC_2PI * d1;
+      dx[q][2] = FRC_2PI * d2;
+      // rt: the density matrices hold conj(rho(J,I)) at (I, J) instead
+      rj[q] = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
+      re[q] = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
+      // the step-function term depends on the pair only through dK =
+      // KZZ_I - KZZ_J: bin x2 rho - rhoE by dK (k_force_step finishes it)
+      const size_t b = (((size_t)(d2 + T.d3) * (2 * T.d2 + 1)) + (d1 + T.d2)) * (2 * T.d1 + 1) + (d0 + T.d1);
+      const double x2q = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
+      atomicAdd(&bins[2 * b], x2q * rj[q].x - re[q].x);
+      atomicAdd(&bins[2 * b + 1], x2q * rj[q].y - re[q].y);
     }
+    const bool top = !(fabs(x) < 0.9999999);
+    double pm2 = 1.0, pm1 = x;
+    w[q][0] = 1.0;
+    w[q][1] = 3.0 * x;
+#pragma unroll
+    for (int l = 2; l < SPH_LMAX; l++) {
+      double pl;
+      if (!top) {
+        const double pplx = x * pm1;
+        pl = pplx + ((double)(l - 1) / (double)l) * (pplx - pm2);
+      } else {
+        pl = x * pm1;
+      }
+      pm2 = pm1;
+      pm1 = pl;
+      w[q][l] = (double)(2 * l + 1) * pl;
+    }
+  }
 
   for (int t0 = 0; t0 < nat;) {
     int ntc = 0, na = 0;
@@ -114,28 +117,28 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
     if (!staged) ntc = 1;
     const int a0c = P.afirst[t0];
     __syncthreads();
-    for (int idx = tid; idx < ntc * ltop * SPH_T; idx += SPH_THREADS) {
+    for (int idx = tid; idx < ntc * ltop * SPH_T; idx += FRC_THREADS) {
       const int r = idx % SPH_T, l = (idx / SPH_T) % ltop, tc = idx / (SPH_T * ltop);
       const int jn = t0 + tc;
       const size_t ob = ((size_t)jn * ltop + l) * P.nvpad;
-      const int J = j0 + r, I = i0 + r;
+      const int Jr = j0 + r, Ir = i0 + r;
       double aj = 0.0, bj = 0.0, ai = 0.0, bi = 0.0;
-      if (J < nv) {
-        aj = P.al[ob + J];
-        bj = P.bl[ob + J];
+      if (Jr < nv) {
+        aj = P.al[ob + Jr];
+        bj = P.bl[ob + Jr];
       }
-      if (I < nv) {
-        ai = P.al[ob + I];
-        bi = P.bl[ob + I];
+      if (Ir < nv) {
+        ai = P.al[ob + Ir];
+        bi = P.bl[ob + Ir];
       }
       const SphCoef c = coef[jn * ltop + l];
-      const int s = (tc * SPH_LMAX + l) * SPH_T + r;
-      sJ[s] = cmk(aj, bj);
-      sI[2 * s] = cmk(c.vif * ai, c.vif * (c.chn * bi));
-      sI[2 * s + 1] = cmk(c.vif * (c.mAA * ai + c.mAB * bi), c.vif * (c.mBA * ai + c.mBB * bi));
+      const int sx = (tc * SPH_LMAX + l) * SPH_T + r;
+      sJ[sx] = cmk(aj, bj);
+      sI[2 * sx] = cmk(c.vif * ai, c.vif * (c.chn * bi));
+      sI[2 * sx + 1] = cmk(c.vif * (c.mAA * ai + c.mAB * bi), c.vif * (c.mBA * ai + c.mBB * bi));
     }
     if (staged)
-      for (int idx = tid; idx < na * SPH_T; idx += SPH_THREADS) {
+      for (int idx = tid; idx < na * SPH_T; idx += FRC_THREADS) {
         const int r = idx % SPH_T, e = idx / SPH_T;
         const double2* pa = P.phase + (size_t)(a0c + e) * P.npad;
         sPJ[idx] = pa[j0 + r];
@@ -145,77 +148,63 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
     int nred = 0;  // atoms of this chunk reduced through red[]
     for (int tc = 0; tc < ntc; tc++) {
       const int jn = t0 + tc;
-      double tS[4], tH[4];
+      double tS[2], tH[2];
 #pragma unroll
-      for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
+      for (int q = 0; q < 2; q++) tS[q] = tH[q] = 0.0;
 #pragma unroll
       for (int l = 0; l < SPH_LMAX; l++) {
         if (l < ltop) {
-          const int s = (tc * SPH_LMAX + l) * SPH_T;
-          double2 jv[2], is[2], ih[2];
+          const int sx = (tc * SPH_LMAX + l) * SPH_T;
+          const double2 jv = sJ[sx + tj];
 #pragma unroll
-          for (int u = 0; u < 2; u++) jv[u] = sJ[s + tj + 16 * u];
-#pragma unroll
-          for (int v = 0; v < 2; v++) {
-            is[v] = sI[2 * (s + ti + 16 * v)];
-            ih[v] = sI[2 * (s + ti + 16 * v) + 1];
+          for (int q = 0; q < 2; q++) {
+            const double2 is = sI[2 * (sx + ti + 16 * q)], ih = sI[2 * (sx + ti + 16 * q) + 1];
+            const double sv = fma(jv.y, is.y, jv.x * is.x);
+            const double hv = fma(jv.y, ih.y, jv.x * ih.x);
+            tS[q] = fma(w[q][l], sv, tS[q]);
+            tH[q] = fma(w[q][l], hv, tH[q]);
           }
-#pragma unroll
-          for (int u = 0; u < 2; u++)
-#pragma unroll
-            for (int v = 0; v < 2; v++) {
-              const int q = u * 2 + v;
-              const double sv = fma(jv[u].y, is[v].y, jv[u].x * is[v].x);
-              const double hv = fma(jv[u].y, ih[v].y, jv[u].x * ih[v].x);
-              tS[q] = fma(w[q][l], sv, tS[q]);
-              tH[q] = fma(w[q][l], hv, tH[q]);
-            }
         }
       }
       const int ae = P.afirst[jn], me = P.mult[jn];
       for (int e = 0; e < me; e++) {
         double fr[3] = {0.0, 0.0, 0.0};
-        double2 fj[2], fi[2];
+        double2 fj, fi[2];
         if (staged) {
           const int b = (ae - a0c + e) * SPH_T;
+          fj = sPJ[b + tj];
 #pragma unroll
-          for (int u = 0; u < 2; u++) fj[u] = sPJ[b + tj + 16 * u];
-#pragma unroll
-          for (int v = 0; v < 2; v++) fi[v] = sPI[b + ti + 16 * v];
+          for (int q = 0; q < 2; q++) fi[q] = sPI[b + ti + 16 * q];
         } else {
           const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
+          fj = pa[j0 + tj];
 #pragma unroll
-          for (int u = 0; u < 2; u++) fj[u] = pa[j0 + tj + 16 * u];
-#pragma unroll
-          for (int v = 0; v < 2; v++) fi[v] = pa[i0 + ti + 16 * v];
+          for (int q = 0; q < 2; q++) fi[q] = pa[i0 + ti + 16 * q];
         }
 #pragma unroll
-        for (int u = 0; u < 2; u++)
-#pragma unroll
-          for (int v = 0; v < 2; v++) {
-            const int q = u * 2 + v;
-            if (!act[q]) continue;
-            // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I))
-            const double cpr = fj[u].x * fi[v].x + fj[u].y * fi[v].y;
-            const double cpi = fj[u].x * fi[v].y - fj[u].y * fi[v].x;
-            const double uim = cpr * rj[q].y + cpi * rj[q].x;  // Im(cP rho(J,I))
-            const double vim = cpr * re[q].y + cpi * re[q].x;  // Im(cP rhoE(J,I))
-            const double g = -2.0 * (tH[q] * uim - tS[q] * vim);
-            fr[0] = fma(g, dx[q][0], fr[0]);
-            fr[1] = fma(g, dx[q][1], fr[1]);
-            fr[2] = fma(g, dx[q][2], fr[2]);
-          }
+        for (int q = 0; q < 2; q++) {
+          if (!act[q]) continue;
+          // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I))
+          const double cpr = fj.x * fi[q].x + fj.y * fi[q].y;
+          const double cpi = fj.x * fi[q].y - fj.y * fi[q].x;
+          const double uim = cpr * rj[q].y + cpi * rj[q].x;  // Im(cP rho(J,I))
+          const double vim = cpr * re[q].y + cpi * re[q].x;  // Im(cP rhoE(J,I))
+          const double g = -2.0 * (tH[q] * uim - tS[q] * vim);
+          fr[0] = fma(g, dx[q][0], fr[0]);
+          fr[1] = fma(g, dx[q][1], fr[1]);
+          fr[2] = fma(g, dx[q][2], fr[2]);
+        }
         // warp partials of this atom
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          double s = fr[c];
+          double sacc = fr[c];
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+          for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
           if (lane == 0) {
             if (staged && nred < FRC_RED_ATOMS)
-              red[nred][c][warp] = s;
+              red[nred][c][warp] = sacc;
             else
-              atomicAdd(&F[(ae + e) * 3 + c], s);
+              atomicAdd(&F[(ae + e) * 3 + c], sacc);
           }
         }
         if (staged) nred++;
@@ -223,11 +212,11 @@ __global__ void __launch_bounds__(SPH_THREADS, 1)
     }
     __syncthreads();
     if (staged)
-      for (int q = tid; q < nred * 3; q += SPH_THREADS) {
+      for (int q = tid; q < nred * 3; q += FRC_THREADS) {
         const int e = q / 3, c = q % 3;
-        double s = 0.0;
-        for (int wq = 0; wq < SPH_THREADS / 32; wq++) s += red[e][c][wq];
-        atomicAdd(&F[(a0c + e) * 3 + c], s);
+        double sacc = 0.0;
+        for (int wq = 0; wq < FRC_THREADS / 32; wq++) sacc += red[e][c][wq];
+        atomicAdd(&F[(a0c + e) * 3 + c], sacc);
       }
     t0 += ntc;
   }
