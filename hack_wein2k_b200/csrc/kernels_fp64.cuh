@@ -686,9 +686,12 @@ __global__ void __launch_bounds__(32 * TMUL_WARPS, 2) k_hns_tmul(int npad, int n
 // C2 = TUU12 conj(ALM) + TDU12 conj(BLM) + TUU22 conj(CLM)  (hns.F:391-433).
 // One thread per (LO row, atom, la): block (32 la, 8 rows), the rows' ALM,
 // BLM, CLM staged in shared memory.
+// cj: Lop holds conj(L) (the library product of the split path), so the
+// LO terms are added conjugated.
 __global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __restrict__ tns,
                                                     double2* __restrict__ Lop, const double2* __restrict__ Rop,
-                                                    const double2* __restrict__ Clo, double2* __restrict__ C2lo) {
+                                                    const double2* __restrict__ Clo, double2* __restrict__ C2lo,
+                                                    int cj) {
   __shared__ double2 sX[8][3][L1G_NSL2];
   const int la = threadIdx.x, cy = threadIdx.y;
   const int c = blockIdx.x * 8 + cy;  // LO row index
@@ -724,9 +727,24 @@ __global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __
   const size_t i = P.nv + c;
   double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2 + la) * npad + i;
   double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2 + la) * npad + i;
-  *LA = cadd(*LA, da);
-  *LB = cadd(*LB, db);
+  *LA = cadd(*LA, cj ? cconj(da) : da);
+  *LB = cadd(*LB, cj ? cconj(db) : db);
   C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc;
+}
+
+// The per-atom matrix M of k_hns_tmul, dense and column-major:
+// Mbuf[a][k][r] = M[(ro, la) = r][(rr, b) = k] (K = 2 nsl2), for the
+// library's strided-batched product of the split path.
+__global__ void __launch_bounds__(256) k_hns_mdense(int nsl2, const int* __restrict__ atype,
+                                                   const double2* __restrict__ tns, double2* __restrict__ Mbuf) {
+  const int a = blockIdx.x, K = 2 * nsl2;
+  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
+  for (int idx = threadIdx.x; idx < K * K; idx += 256) {
+    const int col = idx / K, row = idx % K;
+    const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
+    const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
+    Mbuf[(size_t)a * K * K + idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
+  }
 }
 
 // HS(i,j) += sum_k Lop[k][i] * Rop[k][j] on the lower triangle i >= j

@@ -604,15 +604,34 @@ static const int2* tiles_tri(lapw1gpu_kpoint* k, const char* name, int n, int T,
                   });
 }
 
-// HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom, LO-row terms
+// HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom, LO-row terms.
+// With a library handle h and a dense-M buffer (split path), L is formed
+// by one strided-batched ZGEMM over the atoms as conj(L) = R^T M^H
+// (column-major npad x K per atom), and the LO terms are added conjugated:
+// the slicer of the split HNS kernel takes the conjugate back.
+// Without Lop (the adjoint, which needs R and CLM only) L is not formed.
 static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* tns, const LoRange* lor, int nlor,
-                          double2* Lop, double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl) {
-  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
+                          double2* Lop, double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl,
+                          cublasHandle_t h = nullptr, double2* Mbuf = nullptr) {
+  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1), K = 2 * nsl2;
   k_hns_alm<<<dim3((P.npad + 127) / 128, P.ndf), 128, 0, s>>>(P, lor, nlor, Rop, Clo);
-  if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
-        : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
-    return LAPW1GPU_ERR_CUDA;
-  {
+  if (!Lop) {
+    *nl += 1;
+    return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  }
+  const bool lib = h && Mbuf;
+  if (lib) {
+    k_hns_mdense<<<P.ndf, 256, 0, s>>>(nsl2, P.atype, tns, Mbuf);
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    if (cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_C, P.npad, K, K, &one, (const cuDoubleComplex*)Rop,
+                                  P.npad, (long long)K * P.npad, (const cuDoubleComplex*)Mbuf, K, (long long)K * K,
+                                  &zero, (cuDoubleComplex*)Lop, P.npad, (long long)K * P.npad,
+                                  P.ndf) != CUBLAS_STATUS_SUCCESS)
+      return LAPW1GPU_ERR_CUDA;
+  } else {
+    if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
+          : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
+      return LAPW1GPU_ERR_CUDA;
     // two blocks per SM over the (atom, 64-column) items, contiguous ranges
     const int nitem = (P.npad + TMUL_I - 1) / TMUL_I * P.ndf;
     const int nblk = std::max(1, std::min(nitem, 2 * (c ? c->nsm : 148)));
@@ -622,7 +641,7 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
   }
   *nl += 2;
   if (P.nlo > 0) {
-    k_hns_lo_ops<<<dim3((P.nlo + 7) / 8, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo, C2lo);
+    k_hns_lo_ops<<<dim3((P.nlo + 7) / 8, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo, C2lo, lib ? 1 : 0);
     *nl += 1;
   }
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
@@ -889,11 +908,17 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     double2* Clo = (double2*)c->sbuf(set, "hnsClo", sizeof(double2) * nloc);
     double2* C2lo = (double2*)c->sbuf(set, "hnsC2lo", sizeof(double2) * nloc);
     if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
-    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    // split: L through the library's batched product (conj(L) in Lop)
+    const bool splitL = c->prec == LAPW1GPU_PREC_SPLIT;
+    double2* Mbuf = splitL ? (double2*)c->sbuf(set, "hnsM", sizeof(double2) * (size_t)ndf * 4 * nsl2 * nsl2) : nullptr;
+    cublasHandle_t hb = splitL ? c->handle(set, s) : nullptr;
+    if (splitL && (!Mbuf || !hb)) return LAPW1GPU_ERR_NOMEM;
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl,
+                            hb, Mbuf);
     if (rc) return rc;
     if (c->prec == LAPW1GPU_PREC_SPLIT)
       rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl, hp,
-                          ev ? ev + 14 : nullptr);
+                          ev ? ev + 14 : nullptr, 1);
     else {
       int ntiles = 0;
       const int2* tl = tiles_hns_diag(k, n, c->hns_diag_b, &ntiles);
@@ -1492,17 +1517,17 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   if (!k->nohns) {
     const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
     const int K = ndf * 2 * nsl2, Kc = ndf * nsl2;
-    double2* Lop = (double2*)c->buf("hnsL", sizeof(double2) * (size_t)K * k->npad);
     double2* Rop = (double2*)c->buf("hnsR", sizeof(double2) * (size_t)K * k->npad);
     size_t nloc = (size_t)Kc * std::max(1, nlo);
     double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
-    double2* C2lo = (double2*)c->buf("hnsC2lo", sizeof(double2) * nloc);
     double2* GC = (double2*)c->buf("frc_gc", sizeof(double2) * (size_t)4 * nb * n);
     double2* Y = (double2*)c->buf("frc_y", sizeof(double2) * (size_t)4 * nb * K);
     double2* Z = (double2*)c->buf("frc_z", sizeof(double2) * (size_t)4 * nb * K);
-    if (!Lop || !Rop || !Clo || !C2lo || !GC || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
+    if (!Rop || !Clo || !GC || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
     int nl = 0;
-    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+    // R and CLM only: the adjoint applies T to Y = R^H (G c), not L = M conj(R)
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), nullptr, Rop, Clo, nullptr, s,
+                            &nl);
     if (rc) return rc;
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
     CK(cudaGetLastError());

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(128) k_rowexp(const double2* __restrict__ X, i
 // the padding rows and columns), so the operand buffers need no clearing.
 template <int S>
 __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict__ X, int Kc, int Kcp, int npad,
-                                                       int np_out, int isB, const int* __restrict__ ex,
+                                                       int np_out, int isB, int cj, const int* __restrict__ ex,
                                                        int8_t* __restrict__ out) {
   __shared__ double2 tile[64][33];
   __shared__ int rexp[32];
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
     if (row >= np_out || col >= Kcp) continue;
     const int e = rexp[rr];
     const double2 v = tile[kk][rr];
-    double tr = digit_scale(v.x, e), ti = digit_scale(v.y, e);
+    double tr = digit_scale(v.x, e), ti = digit_scale(cj ? -v.y : v.y, e);  // cj: slice conj(X)
 #pragma unroll
     for (int p = 0; p < S; p++) {
       const int8_t ar = (int8_t)digit7(tr), ai = (int8_t)digit7(ti);
@@ -402,7 +402,7 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
 template <int S>
 static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                              const double2* Lop, const double2* Rop, double2* hs, int ld, cudaStream_t s,
-                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev) {
+                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL) {
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
@@ -420,8 +420,8 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
   const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
   split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
   split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
-  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, exA, A);
-  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, exB, B);
+  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, cjL, exA, A);
+  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B);
   *nlaunch += 4;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
@@ -490,8 +490,8 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
     return LAPW1GPU_ERR_CUDA;
   split::k_rowexp<<<dim3((npadL + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Lop, Kc, npadL, exA);
   split::k_rowexp<<<dim3((npadR + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Rop, Kc, npadR, exB);
-  split::k_slice_rows<S><<<dim3(npL / 32, Kcp / 64), 256, 0, s>>>(Lop, Kc, Kcp, npadL, npL, 0, exA, A);
-  split::k_slice_rows<S><<<dim3(npR / 32, Kcp / 64), 256, 0, s>>>(Rop, Kc, Kcp, npadR, npR, 1, exB, B);
+  split::k_slice_rows<S><<<dim3(npL / 32, Kcp / 64), 256, 0, s>>>(Lop, Kc, Kcp, npadL, npL, 0, 0, exA, A);
+  split::k_slice_rows<S><<<dim3(npR / 32, Kcp / 64), 256, 0, s>>>(Rop, Kc, Kcp, npadR, npR, 1, 0, exB, B);
   *nlaunch += 4;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, npL, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)npR, S, Cf::N))
@@ -527,17 +527,18 @@ static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
   }
 }
 
+// cjL: Lop holds conj(L) (sliced conjugated)
 static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                           const double2* Lop, const double2* Rop, double2* hs, int ld, int slices, cudaStream_t s,
-                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev) {
+                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL = 0) {
   switch (slices) {
-    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
-    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev);
+    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }
