@@ -88,30 +88,35 @@ __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* 
   const int tid = threadIdx.x;
   const int Kc = 2 * P.ndf, Kp = 2 * Kcp;
   const int nrow_real = isB ? 2 * ncrow : ncrow;  // real rows per l
-  // values
-  for (int idx = tid; idx < 32 * Kc; idx += 256) {
-    const int r = idx & 31, k = idx >> 5;
-    const int rc = rc0 + r;
-    const int row = isB ? (rc >> 1) : rc;  // J or I
-    double2 v = make_double2(0.0, 0.0);
-    if (rc < ncrow && row < P.nv) {
-      const int a = k >> 1, rr = k & 1, t = P.atype[a];
+  // values: one (row, atom) per thread and pass, AL/BL and the phase read
+  // once for the atom's two k (and, for B, for both the S and H rows of I)
+  const int nrr = isB ? 16 : 32;  // distinct basis rows of the block
+  for (int idx = tid; idx < nrr * P.ndf; idx += 256) {
+    const int rr = idx % nrr, a = idx / nrr;
+    const int row = isB ? (rc0 >> 1) + rr : rc0 + rr;  // J or I
+    double al = 0.0, bl = 0.0;
+    double2 ph = make_double2(0.0, 0.0);
+    const int t = P.atype[a];
+    if (row < P.nv) {
       const size_t o = ((size_t)t * L + l) * P.nvpad + row;
-      const double al = P.al[o], bl = P.bl[o];
-      double x;
-      if (!isB) {
-        x = rr ? bl : al;
-      } else {
-        const SphCoef c = coef[t * L + l];
-        if ((rc & 1) == 0)
-          x = c.vif * (rr ? c.chn * bl : al);
-        else
-          x = c.vif * (rr ? (c.mBA * al + c.mBB * bl) : (c.mAA * al + c.mAB * bl));
-      }
-      const double2 ph = P.phase[(size_t)a * P.npad + row];
-      v = make_double2(ph.x * x, ph.y * x);
+      al = P.al[o];
+      bl = P.bl[o];
+      ph = P.phase[(size_t)a * P.npad + row];
     }
-    tile[k * 33 + r] = v;
+    if (!isB) {
+      const bool in = rc0 + rr < ncrow;
+      tile[(2 * a) * 33 + rr] = in ? make_double2(ph.x * al, ph.y * al) : make_double2(0.0, 0.0);
+      tile[(2 * a + 1) * 33 + rr] = in ? make_double2(ph.x * bl, ph.y * bl) : make_double2(0.0, 0.0);
+    } else {
+      const SphCoef c = coef[t * L + l];
+      const double xs0 = c.vif * al, xs1 = c.vif * (c.chn * bl);                                  // S row
+      const double xh0 = c.vif * (c.mAA * al + c.mAB * bl), xh1 = c.vif * (c.mBA * al + c.mBB * bl);  // H row
+      const bool in0 = rc0 + 2 * rr < ncrow, in1 = rc0 + 2 * rr + 1 < ncrow;
+      tile[(2 * a) * 33 + 2 * rr] = in0 ? make_double2(ph.x * xs0, ph.y * xs0) : make_double2(0.0, 0.0);
+      tile[(2 * a + 1) * 33 + 2 * rr] = in0 ? make_double2(ph.x * xs1, ph.y * xs1) : make_double2(0.0, 0.0);
+      tile[(2 * a) * 33 + 2 * rr + 1] = in1 ? make_double2(ph.x * xh0, ph.y * xh0) : make_double2(0.0, 0.0);
+      tile[(2 * a + 1) * 33 + 2 * rr + 1] = in1 ? make_double2(ph.x * xh1, ph.y * xh1) : make_double2(0.0, 0.0);
+    }
   }
   __syncthreads();
   {
