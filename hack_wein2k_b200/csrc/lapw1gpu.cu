@@ -58,6 +58,10 @@ struct lapw1gpu_context {
   cudaStream_t side[L1G_MAX_SETS] = {};  // streams of scratch sets 1.. in a batch
   cudaEvent_t ev[16] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels
   cudaEvent_t fork = nullptr, join[L1G_MAX_SETS] = {};
+  // per scratch set: the stream that prepares the split HNS operands while
+  // the spherical stage runs, and its fork/join events
+  cudaStream_t aux[L1G_MAX_SETS] = {};
+  cudaEvent_t auxf[L1G_MAX_SETS] = {}, auxj[L1G_MAX_SETS] = {};
   cudaEvent_t hns_ev[L1G_MAX_GROUPS] = {}, sph_ev[L1G_MAX_GROUPS] = {};
   int* d_status = nullptr;
   int last_status = 0;
@@ -275,6 +279,11 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
     cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming);
   }
+  for (int i = 0; i < L1G_MAX_SETS; i++) {
+    cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&c->auxf[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->auxj[i], cudaEventDisableTiming);
+  }
   if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     delete c;
@@ -303,6 +312,11 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   for (int i = 1; i < L1G_MAX_SETS; i++) {
     cudaEventDestroy(c->join[i]);
     cudaStreamDestroy(c->side[i]);
+  }
+  for (int i = 0; i < L1G_MAX_SETS; i++) {
+    cudaEventDestroy(c->auxf[i]);
+    cudaEventDestroy(c->auxj[i]);
+    cudaStreamDestroy(c->aux[i]);
   }
   cudaStreamDestroy(c->stream);
   delete c;
@@ -838,6 +852,40 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
   CK(cudaGetLastError());
   if (ev) CK(cudaEventRecord(ev[1], s));
 
+  // HNS operand buffers; in split precision the operands (ALM/BLM/CLM, L,
+  // the LO terms, row exponents and int8 slices) are prepared on the set's
+  // auxiliary stream while the spherical stage runs on s: they read AL/BL
+  // and the phases only.  s joins it before the HNS products.
+  const bool hns = (stages & 2) && !k->nohns;
+  const bool hns_fork = hns && c->prec == LAPW1GPU_PREC_SPLIT;
+  const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
+  const int Khns = ndf * 2 * nsl2;
+  double2 *Lop = nullptr, *Rop = nullptr, *Clo = nullptr, *C2lo = nullptr;
+  if (hns) {
+    Lop = (double2*)c->sbuf(set, "hnsL", sizeof(double2) * (size_t)Khns * k->npad);
+    Rop = (double2*)c->sbuf(set, "hnsR", sizeof(double2) * (size_t)Khns * k->npad);
+    size_t nloc = (size_t)ndf * nsl2 * std::max(1, k->nlo);
+    Clo = (double2*)c->sbuf(set, "hnsClo", sizeof(double2) * nloc);
+    C2lo = (double2*)c->sbuf(set, "hnsC2lo", sizeof(double2) * nloc);
+    if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
+  }
+  if (hns_fork) {
+    cudaStream_t a = c->aux[set];
+    CK(cudaEventRecord(c->auxf[set], s));
+    CK(cudaStreamWaitEvent(a, c->auxf[set], 0));
+    // L through the library's batched product (conj(L) in Lop)
+    double2* Mbuf = (double2*)c->sbuf(set, "hnsM", sizeof(double2) * (size_t)ndf * 4 * nsl2 * nsl2);
+    cublasHandle_t hb = c->handle(set, a);
+    if (!Mbuf || !hb) return LAPW1GPU_ERR_NOMEM;
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, a, &nl,
+                            hb, Mbuf);
+    if (!rc)
+      rc = split_hns_gemm(c, k, set, n, k->npad, Khns, Lop, Rop, d_hs, ldhs, c->slices_hns, a, &nl, nullptr,
+                          nullptr, 1, 1);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->auxj[set], a));
+  }
+
   if (stages & 1) {
     // ---- K-c table + K-b spherical ----
     size_t ntab = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
@@ -898,28 +946,17 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     CK(cudaEventRecord(ev[3], s));
   }
 
-  if ((stages & 2) && !k->nohns) {
+  if (hns) {
     // ---- K-ns ----
-    const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
-    const int K = ndf * 2 * nsl2;
-    double2* Lop = (double2*)c->sbuf(set, "hnsL", sizeof(double2) * (size_t)K * k->npad);
-    double2* Rop = (double2*)c->sbuf(set, "hnsR", sizeof(double2) * (size_t)K * k->npad);
-    size_t nloc = (size_t)ndf * nsl2 * std::max(1, k->nlo);
-    double2* Clo = (double2*)c->sbuf(set, "hnsClo", sizeof(double2) * nloc);
-    double2* C2lo = (double2*)c->sbuf(set, "hnsC2lo", sizeof(double2) * nloc);
-    if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
-    // split: L through the library's batched product (conj(L) in Lop)
-    const bool splitL = c->prec == LAPW1GPU_PREC_SPLIT;
-    double2* Mbuf = splitL ? (double2*)c->sbuf(set, "hnsM", sizeof(double2) * (size_t)ndf * 4 * nsl2 * nsl2) : nullptr;
-    cublasHandle_t hb = splitL ? c->handle(set, s) : nullptr;
-    if (splitL && (!Mbuf || !hb)) return LAPW1GPU_ERR_NOMEM;
-    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl,
-                            hb, Mbuf);
-    if (rc) return rc;
-    if (c->prec == LAPW1GPU_PREC_SPLIT)
+    const int K = Khns;
+    int rc = LAPW1GPU_OK;
+    if (hns_fork) {
+      CK(cudaStreamWaitEvent(s, c->auxj[set], 0));
       rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl, hp,
-                          ev ? ev + 14 : nullptr, 1);
-    else {
+                          ev ? ev + 14 : nullptr, 1, 2);
+    } else {
+      rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
+      if (rc) return rc;
       int ntiles = 0;
       const int2* tl = tiles_hns_diag(k, n, c->hns_diag_b, &ntiles);
       if (!tl) return LAPW1GPU_ERR_NOMEM;

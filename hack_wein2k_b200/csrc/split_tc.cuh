@@ -402,7 +402,9 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
 template <int S>
 static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                              const double2* Lop, const double2* Rop, double2* hs, int ld, cudaStream_t s,
-                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL) {
+                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL, int phase) {
+  // phase 1: row exponents and slices only; 2: the products only (the
+  // slices of this set are ready); 3: both
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
@@ -412,17 +414,20 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
   int* exA = (int*)c->sbuf(set, "splitExA", sizeof(int) * np);
   int* exB = (int*)c->sbuf(set, "splitExB", sizeof(int) * np);
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
-  // row exponents (0x80808080 bytes: a very negative start for atomicMax),
-  // then the slices of every row and column of the padded operands
-  if (cudaMemsetAsync(exA, 0x80, sizeof(int) * np, s) != cudaSuccess ||
-      cudaMemsetAsync(exB, 0x80, sizeof(int) * np, s) != cudaSuccess)
-    return LAPW1GPU_ERR_CUDA;
-  const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
-  split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
-  split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
-  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, cjL, exA, A);
-  split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B);
-  *nlaunch += 4;
+  if (phase & 1) {
+    // row exponents (0x80808080 bytes: a very negative start for atomicMax),
+    // then the slices of every row and column of the padded operands
+    if (cudaMemsetAsync(exA, 0x80, sizeof(int) * np, s) != cudaSuccess ||
+        cudaMemsetAsync(exB, 0x80, sizeof(int) * np, s) != cudaSuccess)
+      return LAPW1GPU_ERR_CUDA;
+    const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
+    split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
+    split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
+    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, cjL, exA, A);
+    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B);
+    *nlaunch += 4;
+  }
+  if (!(phase & 2)) return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;
@@ -530,15 +535,15 @@ static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
 // cjL: Lop holds conj(L) (sliced conjugated)
 static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                           const double2* Lop, const double2* Rop, double2* hs, int ld, int slices, cudaStream_t s,
-                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL = 0) {
+                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL = 0, int phase = 3) {
   switch (slices) {
-    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
-    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL);
+    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }
