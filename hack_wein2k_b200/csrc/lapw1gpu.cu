@@ -267,7 +267,13 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
   lapw1gpu_context* c = new lapw1gpu_context();
   c->device = device;
   c->nsm = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // the main and chain streams at the highest priority, the auxiliary
+  // (HNS operand) streams at the lowest: the block scheduler then places the
+  // persistent spherical kernel's CTAs first and the operand kernels in the
+  // gaps
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
     delete c;
     return LAPW1GPU_ERR_CUDA;
   }
@@ -276,11 +282,11 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
   for (auto& e : c->hns_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : c->sph_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (int i = 1; i < L1G_MAX_SETS; i++) {
-    cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
+    cudaStreamCreateWithPriority(&c->side[i], cudaStreamNonBlocking, prio_hi);
     cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming);
   }
   for (int i = 0; i < L1G_MAX_SETS; i++) {
-    cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking);
+    cudaStreamCreateWithPriority(&c->aux[i], cudaStreamNonBlocking, prio_lo);
     cudaEventCreateWithFlags(&c->auxf[i], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->auxj[i], cudaEventDisableTiming);
   }
