@@ -189,8 +189,15 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
   }
 }
 
+// 256 threads: warp 0 lane 0 issues the MMAs, warp 1 lane 0 the TMA loads;
+// afterwards all 8 warps are the epilogue (warp w: TMEM lanes 32 (w%4).. =
+// rows, column half w/4).  The HS values the epilogue adds to are loaded
+// into registers when the CTA starts, so their latency hides behind the
+// MMA main loop (the tiles of one launch own disjoint HS elements, written
+// before the launch).
+#define SPLIT_THREADS 256
 template <int S>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(SPLIT_THREADS, 1)
     k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const int2* __restrict__ tiles, int nkb, int n, int nr, int rect, const int* __restrict__ exA,
                  const int* __restrict__ exB, double2* __restrict__ hs, int ld, int* __restrict__ status) {
@@ -204,6 +211,19 @@ __global__ void __launch_bounds__(128, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int2 t = tiles[blockIdx.x];
   const int i0 = t.x * 128, j0 = t.y * C::JT;
+  // this thread's epilogue share: row i, complex columns j0 + 8 c + q for
+  // the NC chunks c of its column half; prefetch the old HS values
+  constexpr int NCT = N / 16, NC = (NCT + 1) / 2;  // 16-column (8 complex) chunks: all, per half
+  const int i = i0 + (warp & 3) * 32 + lane, cbase = (warp >> 2) * NC;
+  double2 old[NC][8];
+#pragma unroll
+  for (int c = 0; c < NC; c++)
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int j = j0 + (cbase + c) * 8 + q;
+      old[c][q] = (cbase + c < NCT && i < n && j < nr && (rect || j <= i)) ? hs[(size_t)j * ld + i]
+                                                                           : make_double2(0.0, 0.0);
+    }
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -307,17 +327,18 @@ __global__ void __launch_bounds__(128, 1)
                  : "memory");
   }
   __syncwarp();
-  // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i0+32w..
+  // epilogue: warp w owns TMEM lanes 32(w%4).. = rows i0+32(w%4).., column half w/4
   const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(&accbar, 0));  // warp-uniform
   tc_fence_after();
   if (!acc_ok && lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
   __syncthreads();
   if (acc_ok && !abort_flag) {
-    const int i = i0 + warp * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     const double sa = (i < n) ? ldexp(1.0, exA[i] - 12) : 0.0;
-#pragma unroll 1
-    for (int c = 0; c < N / 16; c++) {
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const int cc = cbase + c;
+      if (cc >= NCT) break;  // warp-uniform
       double v[16];
 #pragma unroll
       for (int q = 0; q < 16; q++) v[q] = 0.0;
@@ -331,7 +352,7 @@ __global__ void __launch_bounds__(128, 1)
             : "=r"(r[d][0]), "=r"(r[d][1]), "=r"(r[d][2]), "=r"(r[d][3]), "=r"(r[d][4]), "=r"(r[d][5]),
               "=r"(r[d][6]), "=r"(r[d][7]), "=r"(r[d][8]), "=r"(r[d][9]), "=r"(r[d][10]), "=r"(r[d][11]),
               "=r"(r[d][12]), "=r"(r[d][13]), "=r"(r[d][14]), "=r"(r[d][15])
-            : "r"(trow + (uint32_t)(d * N + c * 16)));
+            : "r"(trow + (uint32_t)(d * N + cc * 16)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       double w = 1.0;
 #pragma unroll
@@ -343,14 +364,13 @@ __global__ void __launch_bounds__(128, 1)
       if (i < n) {
 #pragma unroll
         for (int q = 0; q < 8; q++) {
-          const int j = j0 + c * 8 + q;
+          const int j = j0 + cc * 8 + q;
           if (j < nr && (rect || j <= i)) {
             const double sc = sa * ldexp(1.0, exB[j]);
-            double2* dst = hs + (size_t)j * ld + i;
-            double2 o = *dst;
+            double2 o = old[c][q];
             o.x = fma(v[2 * q], sc, o.x);
             o.y = fma(v[2 * q + 1], sc, o.y);
-            *dst = o;
+            hs[(size_t)j * ld + i] = o;
           }
         }
       }
@@ -462,8 +482,8 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
                                       if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
                               });
     if (!dt) return LAPW1GPU_ERR_NOMEM;
-    split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, n, 0, exA, exB, hs, ld,
-                                                                   c->d_status);
+    split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, n, 0, exA, exB,
+                                                                             hs, ld, c->d_status);
     *nlaunch += 1;
     if (hp && hp->groups > 0 && hp->col[g + 1] <= k->nv) {
       if (cudaEventRecord(hp->ev[g], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
@@ -514,8 +534,8 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
                             });
   if (!dt) return LAPW1GPU_ERR_NOMEM;
   if (!c->smem((const void*)split::k_split_gemm<S>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
-  split::k_split_gemm<S><<<(unsigned)ntile, 128, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, 1, exA, exB, out, ld,
-                                                                 c->d_status);
+  split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, 1, exA, exB,
+                                                                           out, ld, c->d_status);
   *nlaunch += 1;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
