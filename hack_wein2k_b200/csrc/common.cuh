@@ -16,6 +16,12 @@
 // device status word bits (lapw1gpu context keeps one int on the device)
 #define L1G_STATUS_SPHBES 1     // SPHBES argument beyond its start table (sphbes.f:60-64)
 #define L1G_STATUS_NONFINITE 2  // a written matrix element is not finite
+
+// true when either component of v is Inf or NaN (all exponent bits set)
+__device__ __forceinline__ bool l1g_nonfinite(double2 v) {
+  return (((unsigned)(__double_as_longlong(v.x) >> 52) & 0x7ffu) == 0x7ffu) |
+         (((unsigned)(__double_as_longlong(v.y) >> 52) & 0x7ffu) == 0x7ffu);
+}
 #define L1G_STATUS_RANGE 4      // a difference vector fell outside a table
 
 __device__ __forceinline__ double2 cmk(double r, double i) { return make_double2(r, i); }

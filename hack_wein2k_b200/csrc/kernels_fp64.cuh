@@ -432,8 +432,10 @@ struct LoCol {
   double clr, cli;                       // i^l
 };
 
+// status: when non-null, a non-finite written element sets
+// L1G_STATUS_NONFINITE (the split path's writers check what they write)
 __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restrict__ hs, int ld,
-                     double2* __restrict__ hsdiag) {
+                     double2* __restrict__ hsdiag, int* __restrict__ status) {
   const LoCol c = cols[blockIdx.y];
   const int nv = P.nv;
   const int I = nv + c.nnlo - 1;  // 0-based row/column of this LO
@@ -537,6 +539,7 @@ __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restr
     hs[(size_t)I * ld + J] = S;
     hs[(size_t)J * ld + I] = H;
   }
+  if (status && (l1g_nonfinite(S) || l1g_nonfinite(H))) atomicOr(status, L1G_STATUS_NONFINITE);
 }
 
 // ---------------------------------------------------------------------
@@ -814,12 +817,15 @@ __global__ void __launch_bounds__(256, 2)
 
 // LO block of HNS through a library product: HS(nv+i, nv+j) += T(i, j) on
 // the lower triangle i >= j, T = C2^T CLM computed into a scratch block
-__global__ void k_add_lower(int nv, int nlo, const double2* __restrict__ T, double2* __restrict__ hs, int ld) {
+__global__ void k_add_lower(int nv, int nlo, const double2* __restrict__ T, double2* __restrict__ hs, int ld,
+                            int* __restrict__ status) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x;
   const int cj = blockIdx.y;
   if (ci >= nlo || ci < cj) return;
   double2* dst = hs + (size_t)(nv + cj) * ld + (nv + ci);
-  *dst = cadd(*dst, T[(size_t)cj * nlo + ci]);
+  const double2 v = cadd(*dst, T[(size_t)cj * nlo + ci]);
+  *dst = v;
+  if (status && l1g_nonfinite(v)) atomicOr(status, L1G_STATUS_NONFINITE);
 }
 
 // LO block of HNS: HS(i,j) += sum C2[k][i] CLM[k][j], nv <= j <= i < n

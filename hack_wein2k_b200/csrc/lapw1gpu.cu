@@ -65,6 +65,7 @@ struct lapw1gpu_context {
   cudaEvent_t hns_ev[L1G_MAX_GROUPS] = {}, sph_ev[L1G_MAX_GROUPS] = {};
   int* d_status = nullptr;
   int last_status = 0;
+  bool status_pending = false;  // an asynchronous run has not been read back
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 5;      // int8 slices of the spherical part (split precision)
   int slices_hns = 5;  // int8 slices of the HNS update
@@ -349,7 +350,18 @@ int lapw1gpu_set_slices(lapw1gpu_context* c, int slices_sph, int slices_hns) {
 
 void* lapw1gpu_stream(lapw1gpu_context* c) { return c ? (void*)c->stream : nullptr; }
 
-int lapw1gpu_last_status(lapw1gpu_context* c) { return c ? c->last_status : 0; }
+int lapw1gpu_last_status(lapw1gpu_context* c) {
+  if (!c) return 0;
+  if (c->status_pending) {  // the last run was asynchronous: wait for it and read its status
+    int hstat = 0;
+    if (cudaSetDevice(c->device) == cudaSuccess &&
+        cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
+        cudaStreamSynchronize(c->stream) == cudaSuccess)
+      c->last_status = hstat;
+    c->status_pending = false;
+  }
+  return c->last_status;
+}
 
 }  // extern "C"
 
@@ -731,8 +743,9 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   const int sl_smem = Kc * 33 * (int)sizeof(double2);
   if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
   if (!c->smem((const void*)sphtc::k_sph_slice<S>, sl_smem)) return LAPW1GPU_ERR_CUDA;
-  sphtc::k_sph_slice<S><<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, A, exA);
-  sphtc::k_sph_slice<S><<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, B, exB);
+  sphtc::k_sph_slice<S><<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, A, exA, c->d_status);
+  sphtc::k_sph_slice<S><<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, B, exB,
+                                                                           c->d_status);
   *nl += 2;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, 64) ||
@@ -892,6 +905,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     CK(cudaEventRecord(c->auxj[set], a));
   }
 
+  bool sph_tc_used = false;  // the spherical stage ran on the tensor-core kernel
   if (stages & 1) {
     // ---- K-c table + K-b spherical ----
     size_t ntab = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
@@ -907,6 +921,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     if (c->prec == LAPW1GPU_PREC_SPLIT && c->sph_tc && sph_tc_supported(c->slices)) {
       int rc = sph_tc_dispatch(c, k, set, P, coef, tab, d_hs, ldhs, d_hsdiag, s, &nl, ev ? ev + 12 : nullptr, sp);
       if (rc) return rc;
+      sph_tc_used = true;
     } else {
       int ntiles = 0;
       const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
@@ -937,7 +952,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     // ---- K-b': local-orbital columns ----
     if (k->nlo > 0) {
       nl++;
-      k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag);
+      k_lo<<<dim3((n + 127) / 128, k->nlo), 128, 0, s>>>(P, k->d_locols, d_hs, ldhs, d_hsdiag, c->d_status);
     }
     CK(cudaGetLastError());
     if (sp)  // groups whose columns reach the LO columns are final after k_lo
@@ -985,7 +1000,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
                       k->nlo, (const cuDoubleComplex*)Clo, k->nlo, &zero, (cuDoubleComplex*)T,
                       k->nlo) != CUBLAS_STATUS_SUCCESS)
         return LAPW1GPU_ERR_CUDA;
-      k_add_lower<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, T, d_hs, ldhs);
+      k_add_lower<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, T, d_hs, ldhs, c->d_status);
     }
     CK(cudaGetLastError());
     if (hp)  // the groups whose columns reach the LO block end here
@@ -1014,9 +1029,16 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     CK(cudaGetLastError());
   }
   if (ev) CK(cudaEventRecord(ev[5], s));
-  nl++;
-  k_check_finite<<<1184, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
-  CK(cudaGetLastError());
+  // Non-finite elements: the split path's writers (k_sph_tc, k_lo, the
+  // split HNS epilogue, k_add_lower) check what they write; the scan of HS
+  // and HSDIAG is needed when the spherical stage did not run (HS came from
+  // the caller), ran on the FP64 kernel, or HORB added to it.
+  const bool checked = sph_tc_used && !((stages & 4) && !k->orbs.empty());
+  if (!checked) {
+    nl++;
+    k_check_finite<<<1184, 256, 0, s>>>(n, d_hs, ldhs, d_hsdiag, c->d_status);
+    CK(cudaGetLastError());
+  }
   if (ev) CK(cudaEventRecord(ev[6], s));
   *nlaunch += nl;
   return LAPW1GPU_OK;
@@ -1058,6 +1080,7 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
   int rc = kpoint_run_impl(c, k, stages, reinterpret_cast<double2*>(d_hs_), ldhs, reinterpret_cast<double2*>(d_hsdiag_),
                            s, 0, st ? c->ev : nullptr, &nl);
   if (rc) return rc;
+  c->status_pending = !st;
   if (st) {
     int hstat = 0;
     CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1145,6 +1168,7 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
   CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->last_status = hstat;
+  c->status_pending = false;
   if (st) {
     memset(st, 0, sizeof(*st));
     float tot = 0.f;
@@ -1385,6 +1409,7 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
     rc = rc ? rc : LAPW1GPU_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
   c->last_status = hstat;
+  c->status_pending = false;
   if (st && rc == LAPW1GPU_OK) {
     fill_stats(c, k, nl, st);
     float a, b;
@@ -1614,6 +1639,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   c->last_status = hstat;
+  c->status_pending = false;
   return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
 }
 

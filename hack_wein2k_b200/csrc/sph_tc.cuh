@@ -78,8 +78,11 @@ struct Cfg {
 // [Re u | Im u] gives Re and Im of u conj(v).  out: [S][L][rows][Kp] int8,
 // Kp = 2 Kcp; ex: [L][complex rows] exponents.  32 complex rows per block.
 template <int S>
+// A non-finite operand value sets L1G_STATUS_NONFINITE in status (int8
+// slices cannot carry it into the products).
 __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* __restrict__ coef, int isB, int Kcp,
-                                                      int ncrow, int8_t* __restrict__ out, int* __restrict__ ex) {
+                                                      int ncrow, int8_t* __restrict__ out, int* __restrict__ ex,
+                                                      int* __restrict__ status) {
   extern __shared__ double2 tile[];  // [Kc][33]
   __shared__ double red[8][32];
   __shared__ int rexp[32];
@@ -119,6 +122,11 @@ __global__ void __launch_bounds__(256, 2) k_sph_slice(DevProb P, const SphCoef* 
     }
   }
   __syncthreads();
+  {
+    bool bad = false;
+    for (int idx = tid; idx < 32 * Kc; idx += 256) bad |= l1g_nonfinite(tile[(idx >> 5) * 33 + (idx & 31)]);
+    if (bad) atomicOr(status, L1G_STATUS_NONFINITE);
+  }
   {
     const int r = tid & 31, part = tid >> 5;
     double m = 0.0;
@@ -551,6 +559,7 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
           th[u] = tab[2 * ci];
           wp[u] = tab[2 * ci + 1];
         }
+        bool bad = false;  // a written element is not finite
 #pragma unroll
         for (int u = 0; u < HALF; u++) {
           const int I = i0 + hh * HALF + u;
@@ -564,7 +573,9 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
             hs[(size_t)I * ld + J] = s;  // S upper: HS(J,I)
             hs[(size_t)J * ld + I] = h;  // H lower: HS(I,J)
           }
+          bad |= l1g_nonfinite(s) | l1g_nonfinite(h);
         }
+        if (bad) atomicOr(status, L1G_STATUS_NONFINITE);
       }
     }
     if (!ok) {

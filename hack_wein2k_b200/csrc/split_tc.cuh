@@ -147,20 +147,26 @@ __global__ void __launch_bounds__(128) k_rowexp(const double2* __restrict__ X, i
 // x 64 k: every output byte of [0, np) x [0, 2 Kcp) is written (zeros for
 // the padding rows and columns), so the operand buffers need no clearing.
 template <int S>
+// A non-finite operand value sets L1G_STATUS_NONFINITE in status (int8
+// slices cannot carry it into the products).
 __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict__ X, int Kc, int Kcp, int npad,
                                                        int np_out, int isB, int cj, const int* __restrict__ ex,
-                                                       int8_t* __restrict__ out) {
+                                                       int8_t* __restrict__ out, int* __restrict__ status) {
   __shared__ double2 tile[64][33];
   __shared__ int rexp[32];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
   const int tid = threadIdx.x;
   const int Kp = 2 * Kcp;
   const size_t rows = isB ? 2 * (size_t)np_out : (size_t)np_out;
+  bool bad = false;
   for (int q = tid; q < 64 * 32; q += 256) {
     const int kk = q >> 5, r = q & 31;
     const int k = k0 + kk, row = r0 + r;
-    tile[kk][r] = (k < Kc && row < npad) ? X[(size_t)k * npad + row] : make_double2(0.0, 0.0);
+    const double2 v = (k < Kc && row < npad) ? X[(size_t)k * npad + row] : make_double2(0.0, 0.0);
+    tile[kk][r] = v;
+    bad |= l1g_nonfinite(v);
   }
+  if (bad) atomicOr(status, L1G_STATUS_NONFINITE);
   if (tid < 32) rexp[tid] = (r0 + tid < np_out) ? ex[r0 + tid] : 0;
   __syncthreads();
   // one element per thread and pass, lanes along k: conflict-free tile
@@ -332,6 +338,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
   tc_fence_after();
   if (!acc_ok && lane == 0) atomicOr(status, L1G_STATUS_TIMEOUT);
   __syncthreads();
+  bool bad = false;  // a written element is not finite
   if (acc_ok && !abort_flag) {
     const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     const double sa = (i < n) ? ldexp(1.0, exA[i] - 12) : 0.0;
@@ -371,11 +378,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
             o.x = fma(v[2 * q], sc, o.x);
             o.y = fma(v[2 * q + 1], sc, o.y);
             hs[(size_t)j * ld + i] = o;
+            bad |= l1g_nonfinite(o);
           }
         }
       }
     }
   }
+  if (bad) atomicOr(status, L1G_STATUS_NONFINITE);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -443,8 +452,8 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
     const dim3 ge((npad + 127) / 128, (Kc + 63) / 64), gs(np / 32, Kcp / 64);
     split::k_rowexp<<<ge, 128, 0, s>>>(Lop, Kc, npad, exA);
     split::k_rowexp<<<ge, 128, 0, s>>>(Rop, Kc, npad, exB);
-    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, cjL, exA, A);
-    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B);
+    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Lop, Kc, Kcp, npad, np, 0, cjL, exA, A, c->d_status);
+    split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B, c->d_status);
     *nlaunch += 4;
   }
   if (!(phase & 2)) return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
@@ -515,8 +524,8 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
     return LAPW1GPU_ERR_CUDA;
   split::k_rowexp<<<dim3((npadL + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Lop, Kc, npadL, exA);
   split::k_rowexp<<<dim3((npadR + 127) / 128, (Kc + 63) / 64), 128, 0, s>>>(Rop, Kc, npadR, exB);
-  split::k_slice_rows<S><<<dim3(npL / 32, Kcp / 64), 256, 0, s>>>(Lop, Kc, Kcp, npadL, npL, 0, 0, exA, A);
-  split::k_slice_rows<S><<<dim3(npR / 32, Kcp / 64), 256, 0, s>>>(Rop, Kc, Kcp, npadR, npR, 1, 0, exB, B);
+  split::k_slice_rows<S><<<dim3(npL / 32, Kcp / 64), 256, 0, s>>>(Lop, Kc, Kcp, npadL, npL, 0, 0, exA, A, c->d_status);
+  split::k_slice_rows<S><<<dim3(npR / 32, Kcp / 64), 256, 0, s>>>(Rop, Kc, Kcp, npadR, npR, 1, 0, exB, B, c->d_status);
   *nlaunch += 4;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, npL, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)npR, S, Cf::N))

@@ -126,9 +126,11 @@ class KPoint:
         _check("lapw1gpu_forces", rc)
 
     def free(self):
-        if self.h:
+        # a k-point outliving its context (closed first) is not freed: the
+        # context's finalize released the device and its handle is gone
+        if self.h and self.ctx.h:
             self.ctx.lib.lapw1gpu_kpoint_free(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

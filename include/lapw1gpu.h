@@ -205,7 +205,8 @@ int lapw1gpu_setup_stages(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
  * own work after an asynchronous lapw1gpu_kpoint_run */
 void* lapw1gpu_stream(lapw1gpu_context* ctx);
 
-/* device status word of the last run (L1G_STATUS_* bits), 0 if clean */
+/* device status word of the last run (L1G_STATUS_* bits), 0 if clean; after
+ * an asynchronous lapw1gpu_kpoint_run it waits for that run first */
 int lapw1gpu_last_status(lapw1gpu_context* ctx);
 
 /* Build the nine HNS T blocks from the reference's gaunt lists: the sums of

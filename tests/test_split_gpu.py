@@ -121,3 +121,37 @@ def test_split_matches_fp64_gpu_path(sctx):
     b = sctx.setup(p)
     err = rel_errors(a[0], a[1], b[0], b[1])
     assert err["H"] <= 1e-12 and err["S"] == 0.0, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "split"])
+def test_nonfinite_element_is_reported(ctx, prec):
+    """A NaN energy parameter (planted in the host inputs) makes H elements
+    non-finite: both paths end with the non-finite status (the FP64 path by
+    its scan of HS, the split path in the kernels that write HS)."""
+    import dataclasses
+
+    import torch
+    p = synth.small_case("lo")
+    e = np.array(p.e, dtype=np.float64, copy=True)
+    e.flat[0] = np.nan
+    p = dataclasses.replace(p, e=e)
+    if prec == "split":
+        ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    kp = None
+    try:
+        kp = ctx.upload(p)
+        dev = torch.device("cuda", ctx.device)
+        hs = torch.zeros((p.n, p.n), dtype=torch.complex128, device=dev)
+        hd = torch.zeros(p.n, dtype=torch.complex128, device=dev)
+        kp.run(hs.data_ptr(), p.n, hd.data_ptr())  # asynchronous: status read on request
+        async_status = ctx.last_status()
+        with pytest.raises(lapw1gpu.Lapw1GpuError) as ei:
+            kp.run(hs.data_ptr(), p.n, hd.data_ptr(), stats=True)
+    finally:
+        if kp is not None:
+            kp.free()
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    assert async_status & 2
+    assert ei.value.code == 4
+    assert ctx.last_status() & 2
