@@ -150,7 +150,7 @@ def int8_peak_tops(torch, device):
 
 
 def baseline_def_flops(p):
-    """BASELINE's work formula F = sum_atoms (16 N^2 (lmax+1)^2 + 8 N^2 (lmax_ns+1)^2):
+    """The benchmark definition's work formula F = sum_atoms (16 N^2 (lmax+1)^2 + 8 N^2 (lmax_ns+1)^2):
     the flops of the A^H T A form the benchmark definition counts."""
     n = p.n
     return p.ndf * (16.0 * n * n * p.ltop ** 2 + 8.0 * n * n * (p.lnsmax + 1) ** 2)
@@ -247,7 +247,7 @@ def _rel_err(torch, a, b, n):
     return out
 
 
-def north_star(args):
+def hundred_atoms(args):
     """The 100-atom configurations: c4 (16 k-points, RKmax 8, N ~ 12700) as
     one captured batch, split precision (spherical/HNS slices) against the
     plain FP64 GPU path, plus the adjoint forces of 400 bands (c3 for
@@ -374,13 +374,13 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the k-batch line")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the library's default tuning (profiling runs: timings under a profiler mislead the autotuner)")
-    ap.add_argument("--north-star", action="store_true",
+    ap.add_argument("--hundred-atoms", action="store_true",
                     help="instead: the 100-atom c4 batch (split vs FP64) and c3/c4 adjoint forces, one JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.north_star:
-        return north_star(args)
+    if args.hundred_atoms:
+        return hundred_atoms(args)
 
     import torch
     from hack_wein2k_b200 import lapw1gpu, synth
