@@ -687,23 +687,25 @@ __global__ void __launch_bounds__(32 * TMUL_WARPS, 2) k_hns_tmul(int npad, int n
 
 // LO rows: A2 += TUU21 conj(CLM), B2 += TUD21 conj(CLM),
 // C2 = TUU12 conj(ALM) + TDU12 conj(BLM) + TUU22 conj(CLM)  (hns.F:391-433).
-// One thread per (LO row, atom, la): block (32 la, 8 rows), the rows' ALM,
-// BLM, CLM staged in shared memory.
+// One thread per (la, 4 LO rows) of an atom: block (32 la, 8) over 32 rows,
+// the rows' ALM, BLM, CLM staged in shared memory; each T element read is
+// used for the 4 rows.
 // cj: Lop holds conj(L) (the library product of the split path), so the
 // LO terms are added conjugated.
+#define LOOPS_ROWS 32
 __global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __restrict__ tns,
                                                     double2* __restrict__ Lop, const double2* __restrict__ Rop,
                                                     const double2* __restrict__ Clo, double2* __restrict__ C2lo,
                                                     int cj) {
-  __shared__ double2 sX[8][3][L1G_NSL2];
+  __shared__ double2 sX[LOOPS_ROWS][3][L1G_NSL2];
   const int la = threadIdx.x, cy = threadIdx.y;
-  const int c = blockIdx.x * 8 + cy;  // LO row index
+  const int c0 = blockIdx.x * LOOPS_ROWS;  // first LO row of the block
   const int a = blockIdx.y;
   const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
   const size_t npad = P.npad;
-  for (int q = threadIdx.y * 32 + threadIdx.x; q < 8 * 3 * nsl2; q += 256) {
+  for (int q = threadIdx.y * 32 + threadIdx.x; q < LOOPS_ROWS * 3 * nsl2; q += 256) {
     const int r = q / (3 * nsl2), w = (q / nsl2) % 3, b = q % nsl2;
-    const int cc = blockIdx.x * 8 + r;
+    const int cc = c0 + r;
     double2 v = cmk(0.0, 0.0);
     if (cc < P.nlo) {
       const size_t i = P.nv + cc;
@@ -715,24 +717,35 @@ __global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __
     sX[r][w][b] = v;
   }
   __syncthreads();
-  if (c >= P.nlo || la >= nsl2) return;
+  if (la >= nsl2 || c0 + cy >= P.nlo) return;
   const double2* T = tns + (size_t)P.atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  double2 da = cmk(0, 0), db = cmk(0, 0), dc = cmk(0, 0);
+  double2 da[4], db[4], dc[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) da[u] = db[u] = dc[u] = cmk(0, 0);
   for (int b = 0; b < nsl2; b++) {
-    const double2 A = sX[cy][0][b], B = sX[cy][1][b], Cc = sX[cy][2][b];
 #define TT(blk) __ldg(T + ((size_t)(blk)*L1G_NSL2 + la) * L1G_NSL2 + b)
     const double2 tuu21 = TT(2), tud21 = TT(5), tuu12 = TT(6), tdu12 = TT(7), tuu22 = TT(8);
 #undef TT
-    da = cadd(da, cmul(tuu21, cconj(Cc)));
-    db = cadd(db, cmul(tud21, cconj(Cc)));
-    dc = cadd(dc, cadd(cadd(cmul(tuu12, cconj(A)), cmul(tdu12, cconj(B))), cmul(tuu22, cconj(Cc))));
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int r = cy + 8 * u;
+      const double2 A = sX[r][0][b], B = sX[r][1][b], Cc = sX[r][2][b];
+      da[u] = cadd(da[u], cmul(tuu21, cconj(Cc)));
+      db[u] = cadd(db[u], cmul(tud21, cconj(Cc)));
+      dc[u] = cadd(dc[u], cadd(cadd(cmul(tuu12, cconj(A)), cmul(tdu12, cconj(B))), cmul(tuu22, cconj(Cc))));
+    }
   }
-  const size_t i = P.nv + c;
-  double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2 + la) * npad + i;
-  double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2 + la) * npad + i;
-  *LA = cadd(*LA, cj ? cconj(da) : da);
-  *LB = cadd(*LB, cj ? cconj(db) : db);
-  C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc;
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int c = c0 + cy + 8 * u;
+    if (c >= P.nlo) break;
+    const size_t i = P.nv + c;
+    double2* LA = Lop + ((size_t)(a * 2 + 0) * nsl2 + la) * npad + i;
+    double2* LB = Lop + ((size_t)(a * 2 + 1) * nsl2 + la) * npad + i;
+    *LA = cadd(*LA, cj ? cconj(da[u]) : da[u]);
+    *LB = cadd(*LB, cj ? cconj(db[u]) : db[u]);
+    C2lo[((size_t)a * nsl2 + la) * P.nlo + c] = dc[u];
+  }
 }
 
 // The per-atom matrix M of k_hns_tmul, dense and column-major:

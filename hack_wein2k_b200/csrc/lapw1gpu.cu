@@ -673,7 +673,8 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
   }
   *nl += 2;
   if (P.nlo > 0) {
-    k_hns_lo_ops<<<dim3((P.nlo + 7) / 8, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo, C2lo, lib ? 1 : 0);
+    k_hns_lo_ops<<<dim3((P.nlo + LOOPS_ROWS - 1) / LOOPS_ROWS, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo,
+                                                                                           C2lo, lib ? 1 : 0);
     *nl += 1;
   }
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
