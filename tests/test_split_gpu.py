@@ -155,3 +155,29 @@ def test_nonfinite_element_is_reported(ctx, prec):
     assert async_status & 2
     assert ei.value.code == 4
     assert ctx.last_status() & 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["lo", "multilo"])
+def test_split_stages_compose(sctx, kind):
+    """HAMILT then HNS as two separate runs on the same device HS equals one
+    run of both, bit for bit (the HNS operands are prepared on their own
+    stream and joined before the products in both cases)."""
+    import torch
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    sctx.set_slices(5, 4)
+    p = synth.small_case(kind)
+    dev = torch.device("cuda", sctx.device)
+    kp = sctx.upload(p)
+    try:
+        a = torch.zeros((p.n, p.n), dtype=torch.complex128, device=dev)
+        ad = torch.zeros(p.n, dtype=torch.complex128, device=dev)
+        kp.run(a.data_ptr(), p.n, ad.data_ptr(), stages=3, stats=True)
+        b = torch.zeros_like(a)
+        bd = torch.zeros_like(ad)
+        kp.run(b.data_ptr(), p.n, bd.data_ptr(), stages=1, stats=True)
+        kp.run(b.data_ptr(), p.n, bd.data_ptr(), stages=2, stats=True)
+        assert torch.equal(a, b) and torch.equal(ad, bd)
+    finally:
+        kp.free()
+        sctx.set_precision(lapw1gpu.PREC_SPLIT, 7)
