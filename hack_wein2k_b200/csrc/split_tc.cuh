@@ -83,6 +83,10 @@ __device__ __forceinline__ double digit_scale(double x, int e) {
   const int k = 6 - e;
   return (k >= -1022 && k <= 1023) ? x * __longlong_as_double((long long)(k + 1023) << 52) : ldexp(x, k);
 }
+// 2^e exactly: exponent bits in the normal range, ldexp outside it
+__device__ __forceinline__ double pow2_exact(int e) {
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+}
 // One int8 digit of the slicing: t rounded to the nearest integer (ties to
 // even, as rint) by adding 1.5 2^52, whose low mantissa bits then hold the
 // integer; t becomes the exact remainder scaled by 2^7 for the next digit.
@@ -221,14 +225,19 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
   // the NC chunks c of its column half; prefetch the old HS values
   constexpr int NCT = N / 16, NC = (NCT + 1) / 2;  // 16-column (8 complex) chunks: all, per half
   const int i = i0 + (warp & 3) * 32 + lane, cbase = (warp >> 2) * NC;
+  // volatile loads: issued here, not sunk by the compiler to their use in
+  // the epilogue, so the main loop hides their latency
   double2 old[NC][8];
 #pragma unroll
   for (int c = 0; c < NC; c++)
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       const int j = j0 + (cbase + c) * 8 + q;
-      old[c][q] = (cbase + c < NCT && i < n && j < nr && (rect || j <= i)) ? hs[(size_t)j * ld + i]
-                                                                           : make_double2(0.0, 0.0);
+      old[c][q] = make_double2(0.0, 0.0);
+      if (cbase + c < NCT && i < n && j < nr && (rect || j <= i))
+        asm volatile("ld.global.v2.f64 {%0, %1}, [%2];"
+                     : "=d"(old[c][q].x), "=d"(old[c][q].y)
+                     : "l"(hs + (size_t)j * ld + i));
     }
 
   if (warp == 0) {
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
   bool bad = false;  // a written element is not finite
   if (acc_ok && !abort_flag) {
     const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const double sa = (i < n) ? ldexp(1.0, exA[i] - 12) : 0.0;
+    const double sa = (i < n) ? pow2_exact(exA[i] - 12) : 0.0;
 #pragma unroll
     for (int c = 0; c < NC; c++) {
       const int cc = cbase + c;
@@ -373,7 +382,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
         for (int q = 0; q < 8; q++) {
           const int j = j0 + cc * 8 + q;
           if (j < nr && (rect || j <= i)) {
-            const double sc = sa * ldexp(1.0, exB[j]);
+            const double sc = sa * pow2_exact(exB[j]);
             double2 o = old[c][q];
             o.x = fma(v[2 * q], sc, o.x);
             o.y = fma(v[2 * q + 1], sc, o.y);
