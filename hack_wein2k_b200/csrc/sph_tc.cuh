@@ -419,18 +419,19 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
     // one tile ahead (behind the previous tile's interstitial part)
     constexpr int QA = (SPH_LMAX * 128 + EPI - 1) / EPI, QB = (SPH_LMAX * 2 * IT + EPI - 1) / EPI;
     int16_t pa[QA], pb[QB];
-    auto fetch = [&](int t) {
-      const int2 tt = tiles[t];
-      const int j0 = tt.x * 128, i0 = tt.y * IT;
+    auto fetch = [&](int t) {  // volatile loads: issued here, ahead of their use
+      const int j0 = split::ld_early(&tiles[t].x) * 128, i0 = split::ld_early(&tiles[t].y) * IT;
 #pragma unroll
       for (int k = 0; k < QA; k++) {
         const int q = tid + k * EPI, l = q >> 7, J = j0 + (q & 127);
-        pa[k] = (int16_t)((q < L * 128 && J < nv) ? exA[(size_t)l * npA + J] - 12 : -2000);  // -2000: a zero scale
+        pa[k] = (int16_t)((q < L * 128 && J < nv) ? split::ld_early(&exA[(size_t)l * npA + J]) - 12
+                                                   : -2000);  // -2000: a zero scale
       }
 #pragma unroll
       for (int k = 0; k < QB; k++) {
         const int q = tid + k * EPI, l = q / (2 * IT), r = q % (2 * IT), I = i0 + (r >> 1);
-        pb[k] = (int16_t)((q < L * 2 * IT && I < nv) ? exB[(size_t)l * 2 * npB + 2 * I + (r & 1)] : -2000);
+        pb[k] = (int16_t)((q < L * 2 * IT && I < nv) ? split::ld_early(&exB[(size_t)l * 2 * npB + 2 * I + (r & 1)])
+                                                      : -2000);
       }
     };
     if (blockIdx.x < ntile) fetch(blockIdx.x);

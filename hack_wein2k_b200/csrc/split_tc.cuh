@@ -83,6 +83,12 @@ __device__ __forceinline__ double digit_scale(double x, int e) {
   const int k = 6 - e;
   return (k >= -1022 && k <= 1023) ? x * __longlong_as_double((long long)(k + 1023) << 52) : ldexp(x, k);
 }
+// a global load issued where it stands (volatile: not sunk to its use)
+__device__ __forceinline__ int ld_early(const int* p) {
+  int v;
+  asm volatile("ld.global.nc.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
 // 2^e exactly: exponent bits in the normal range, ldexp outside it
 __device__ __forceinline__ double pow2_exact(int e) {
   return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
