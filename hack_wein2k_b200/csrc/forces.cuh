@@ -36,51 +36,139 @@
 #pragma once
 #include "kernels_fp64.cuh"
 
-#define FRC_RED_ATOMS SPH_MAXA
 #define FRC_2PI 6.283185307179586476925287
 
-// One block per 32 x 32 pair tile, 512 threads: thread (tj = lane, ti =
-// warp) owns the pairs (J = j0 + tj, I = i0 + ti + 16 v), v = 0, 1, with
-// their Legendre weights in registers (16 warps per SM: the FP64 chains of
-// the l sums need the occupancy).
-#define FRC_THREADS 512
+// Rows of the spherical force operands, per (type, l, row): the J side
+// (a, b) and the I side, S = vif (a, chn b) and H = vif (mAA a + mAB b,
+// mBA a + mBB b), so that each l term of a pair is one 2-vector dot
+// product per side.  Rows nv..nvpad-1 are zero (k_albl zeroes them).
+__global__ void k_force_rows(DevProb P, const SphCoef* __restrict__ coef, double2* __restrict__ rowJ,
+                             double2* __restrict__ rowI) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, tl = blockIdx.y;  // tl = type * ltop + l
+  if (r >= P.nvpad) return;
+  const size_t o = (size_t)tl * P.nvpad + r;
+  const double a = P.al[o], b = P.bl[o];
+  const SphCoef c = coef[tl];
+  rowJ[o] = cmk(a, b);
+  rowI[2 * o] = cmk(c.vif * a, c.vif * (c.chn * b));
+  rowI[2 * o + 1] = cmk(c.vif * (c.mAA * a + c.mAB * b), c.vif * (c.mBA * a + c.mBB * b));
+}
+
+#define FRC_THREADS 256
+#define FRC_MAXA 16  // equivalent atoms per staged chunk (a type with more reads its phases from global)
+#define FRC_LT 11    // l count of the specialised kernel (lmax = 10)
+
+// types per staged chunk: as many as the shared memory holds twice
+__host__ __device__ constexpr int frc_tc(int lt) { return lt <= FRC_LT ? 4 : 3; }
+
+__device__ __forceinline__ void frc_cp16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void frc_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void frc_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// A chunk of types from t0: up to TC types whose equivalent atoms fit
+// FRC_MAXA; a single type with more atoms forms a chunk of its own whose
+// phases are not staged.
+struct FrcChunk {
+  int ntc, na, staged;
+};
+template <int TC>
+__device__ __forceinline__ FrcChunk frc_chunk(const DevProb& P, int t0) {
+  FrcChunk c{0, 0, 1};
+  while (c.ntc < TC && t0 + c.ntc < P.nat && c.na + P.mult[t0 + c.ntc] <= FRC_MAXA) c.na += P.mult[t0 + c.ntc++];
+  if (c.ntc == 0) c = FrcChunk{1, 0, 0};
+  return c;
+}
+
+// dynamic shared memory: two stages of type rows (J: 1, I: 2 double2 per
+// row and l) and of phases, then the per-warp force partials of a chunk's
+// atoms (8 per warp and component)
+__host__ __device__ constexpr int frc_smem_bytes(int lt) {
+  return (2 * frc_tc(lt) * lt * SPH_T * 3 + 2 * 2 * FRC_MAXA * SPH_T) * 16 + FRC_MAXA * 3 * FRC_THREADS / 4 * 8;
+}
+
+// One block per 32 x 32 pair tile, 256 threads.  Thread (warp, lane) owns
+// the 2 x 2 pairs J = j0 + jl0 + {0, 8}, I = i0 + il0 + {0, 4} with
+// jl0 = 16 (warp & 1) + (lane & 7), il0 = 8 (warp >> 1) + (lane >> 3):
+// a warp reads 8 distinct J rows and 4 distinct I rows per l, so that the
+// shared-memory reads (about one cycle each: the addresses of a read are
+// 8 or 4 distinct 16-byte words) stay below the FP64 pipe's rate.  The
+// Legendre weights, rho, rhoE and dK of the four pairs stay in registers
+// for all types.  The type rows (k_force_rows) and the phases of a chunk
+// are copied into shared memory by cp.async one chunk ahead (double
+// buffer), one warp per 32-row segment.
+template <int LT, bool GUARD>
 __global__ void __launch_bounds__(FRC_THREADS, 1)
-    k_force_sph(DevProb P, const int2* __restrict__ tiles, const SphCoef* __restrict__ coef, TabDesc T,
-                const double2* __restrict__ rho, const double2* __restrict__ rhoe, int ldr, int rt,
-                double* __restrict__ F, double* __restrict__ bins) {
+    k_force_sph(DevProb P, const int2* __restrict__ tiles, const double2* __restrict__ rowJ,
+                const double2* __restrict__ rowI, TabDesc T, const double2* __restrict__ rho,
+                const double2* __restrict__ rhoe, int ldr, int rt, double* __restrict__ F, double* __restrict__ bins) {
+  constexpr int TC = frc_tc(LT);
   extern __shared__ double2 sm2[];
-  double2* sJ = sm2;
-  double2* sI = sJ + SPH_TC * SPH_LMAX * SPH_T;
-  double2* sPJ = sI + 2 * SPH_TC * SPH_LMAX * SPH_T;
-  double2* sPI = sPJ + SPH_MAXA * SPH_T;
-  __shared__ double red[FRC_RED_ATOMS][3][FRC_THREADS / 32];
+  double2* sJ = sm2;                       // [2][TC][LT][SPH_T]
+  double2* sI = sJ + 2 * TC * LT * SPH_T;  // [2][TC][LT][SPH_T][S, H]
+  double2* sP = sI + 4 * TC * LT * SPH_T;  // [2][J, I][FRC_MAXA][SPH_T]
+  double* red = reinterpret_cast<double*>(sP + 4 * FRC_MAXA * SPH_T);  // [FRC_MAXA][3][8 warps x 8]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tj = lane, ti = warp;
   const int2 t = tiles[blockIdx.x];
   const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
-  const int nv = P.nv, ltop = P.ltop, nat = P.nat;
+  const int nv = P.nv, ltop = P.ltop, nat = P.nat, nvpad = P.nvpad;
+  const int jl0 = (warp & 1) * 16 + (lane & 7), il0 = (warp >> 1) * 8 + (lane >> 3);
 
-  double w[2][SPH_LMAX];
-  double dx[2][3];
-  double2 rj[2], re[2];  // rho(J,I) and rhoE(J,I) of the owned pairs
-  bool act[2];
-  const int J = j0 + tj;
+  // (type, l) rows of consecutive types are consecutive in rowJ / rowI:
+  // the chunk's rows are k = 0 .. ntc ltop - 1 from row t0 ltop, and with
+  // ltop = LT also consecutive in shared memory
+  auto stage = [&](int st, int t0, const FrcChunk& ch) {
+    double2* dJ = sJ + st * TC * LT * SPH_T;
+    double2* dI = sI + st * 2 * TC * LT * SPH_T;
+    const size_t g0 = (size_t)t0 * ltop;
+    for (int k = warp; k < ch.ntc * ltop; k += FRC_THREADS / 32) {
+      const int ks = GUARD ? (k / ltop) * LT + k % ltop : k;
+      const double2* src = rowJ + (g0 + k) * nvpad + j0;
+      frc_cp16(dJ + ks * SPH_T + lane, src + lane);
+      const double2* srci = rowI + 2 * ((g0 + k) * nvpad + i0);
+      frc_cp16(dI + ks * 2 * SPH_T + lane, srci + lane);
+      frc_cp16(dI + ks * 2 * SPH_T + SPH_T + lane, srci + SPH_T + lane);
+    }
+    if (ch.staged) {
+      double2* dP = sP + st * 2 * FRC_MAXA * SPH_T;
+      const int a0c = P.afirst[t0];
+      for (int k = warp; k < ch.na * 2; k += FRC_THREADS / 32) {
+        const int side = k & 1, e = k >> 1;
+        frc_cp16(dP + (side * FRC_MAXA + e) * SPH_T + lane,
+                 P.phase + (size_t)(a0c + e) * P.npad + (side ? i0 : j0) + lane);
+      }
+    }
+    frc_commit();
+  };
+
+  FrcChunk ch = frc_chunk<TC>(P, 0);
+  stage(0, 0, ch);
+
+  double w[4][LT];
+  double dx[4][3];
+  double2 rj[4], re[4];  // rho(J,I) and rhoE(J,I) of the owned pairs; zero for inactive pairs
 #pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int I = i0 + ti + 16 * q;
-    act[q] = (J < nv && I < nv && J < I);
+  for (int q = 0; q < 4; q++) {
+    const int J = j0 + jl0 + 8 * (q >> 1), I = i0 + il0 + 4 * (q & 1);
+    const bool act = (J < nv && I < nv && J < I);
     double x = 0.0;
     dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
     rj[q] = re[q] = cmk(0.0, 0.0);
-    if (act[q]) {
+    if (act) {
       x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
       double den = P.rk[I] * P.rk[J];
       if (den > 1.0e-8) x = x / den;
       const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
                 d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
-      dx[q][0] = FRC_2PI * d0;
-      dx[q][1] = FRC_2PI * d1;
-      dx[q][2] = FRC_2PI * d2;
+      // -2 of the pair term folded in
+      dx[q][0] = -2.0 * FRC_2PI * d0;
+      dx[q][1] = -2.0 * FRC_2PI * d1;
+      dx[q][2] = -2.0 * FRC_2PI * d2;
       // rt: the density matrices hold conj(rho(J,I)) at (I, J) instead
       rj[q] = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
       re[q] = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
@@ -94,9 +182,9 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
     const bool top = !(fabs(x) < 0.9999999);
     double pm2 = 1.0, pm1 = x;
     w[q][0] = 1.0;
-    w[q][1] = 3.0 * x;
+    if (LT > 1) w[q][1] = 3.0 * x;
 #pragma unroll
-    for (int l = 2; l < SPH_LMAX; l++) {
+    for (int l = 2; l < LT; l++) {
       double pl;
       if (!top) {
         const double pplx = x * pm1;
@@ -110,115 +198,100 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
     }
   }
 
+  int st = 0;
   for (int t0 = 0; t0 < nat;) {
-    int ntc = 0, na = 0;
-    while (ntc < SPH_TC && t0 + ntc < nat && na + P.mult[t0 + ntc] <= SPH_MAXA) na += P.mult[t0 + ntc++];
-    const bool staged = ntc > 0;
-    if (!staged) ntc = 1;
-    const int a0c = P.afirst[t0];
-    __syncthreads();
-    for (int idx = tid; idx < ntc * ltop * SPH_T; idx += FRC_THREADS) {
-      const int r = idx % SPH_T, l = (idx / SPH_T) % ltop, tc = idx / (SPH_T * ltop);
-      const int jn = t0 + tc;
-      const size_t ob = ((size_t)jn * ltop + l) * P.nvpad;
-      const int Jr = j0 + r, Ir = i0 + r;
-      double aj = 0.0, bj = 0.0, ai = 0.0, bi = 0.0;
-      if (Jr < nv) {
-        aj = P.al[ob + Jr];
-        bj = P.bl[ob + Jr];
-      }
-      if (Ir < nv) {
-        ai = P.al[ob + Ir];
-        bi = P.bl[ob + Ir];
-      }
-      const SphCoef c = coef[jn * ltop + l];
-      const int sx = (tc * SPH_LMAX + l) * SPH_T + r;
-      sJ[sx] = cmk(aj, bj);
-      sI[2 * sx] = cmk(c.vif * ai, c.vif * (c.chn * bi));
-      sI[2 * sx + 1] = cmk(c.vif * (c.mAA * ai + c.mAB * bi), c.vif * (c.mBA * ai + c.mBB * bi));
+    const int t1 = t0 + ch.ntc;
+    FrcChunk nx{0, 0, 1};
+    if (t1 < nat) {
+      nx = frc_chunk<TC>(P, t1);
+      stage(st ^ 1, t1, nx);
+      frc_wait<1>();
+    } else {
+      frc_wait<0>();
     }
-    if (staged)
-      for (int idx = tid; idx < na * SPH_T; idx += FRC_THREADS) {
-        const int r = idx % SPH_T, e = idx / SPH_T;
-        const double2* pa = P.phase + (size_t)(a0c + e) * P.npad;
-        sPJ[idx] = pa[j0 + r];
-        sPI[idx] = pa[i0 + r];
-      }
     __syncthreads();
-    int nred = 0;  // atoms of this chunk reduced through red[]
-    for (int tc = 0; tc < ntc; tc++) {
-      const int jn = t0 + tc;
-      double tS[2], tH[2];
+    const double2* cJ = sJ + st * TC * LT * SPH_T;
+    const double2* cI = sI + st * 2 * TC * LT * SPH_T;
+    const double2* cPJ = sP + st * 2 * FRC_MAXA * SPH_T;
+    const double2* cPI = cPJ + FRC_MAXA * SPH_T;
+    const int a0c = P.afirst[t0];
+    for (int tc = 0; tc < ch.ntc; tc++) {
+      double tS[4], tH[4];
 #pragma unroll
-      for (int q = 0; q < 2; q++) tS[q] = tH[q] = 0.0;
+      for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
+      const double2* bJ = cJ + tc * LT * SPH_T + jl0;
+      const double2* bI = cI + tc * LT * 2 * SPH_T + 2 * il0;
 #pragma unroll
-      for (int l = 0; l < SPH_LMAX; l++) {
-        if (l < ltop) {
-          const int sx = (tc * SPH_LMAX + l) * SPH_T;
-          const double2 jv = sJ[sx + tj];
+      for (int l = 0; l < LT; l++) {
+        if (GUARD && l >= ltop) break;
+        const int o = l * SPH_T;
+        const double2 av[2] = {bJ[o], bJ[o + 8]};
+        const double2 sv[2] = {bI[2 * o], bI[2 * o + 8]}, hv[2] = {bI[2 * o + 1], bI[2 * o + 9]};
 #pragma unroll
-          for (int q = 0; q < 2; q++) {
-            const double2 is = sI[2 * (sx + ti + 16 * q)], ih = sI[2 * (sx + ti + 16 * q) + 1];
-            const double sv = fma(jv.y, is.y, jv.x * is.x);
-            const double hv = fma(jv.y, ih.y, jv.x * ih.x);
-            tS[q] = fma(w[q][l], sv, tS[q]);
-            tH[q] = fma(w[q][l], hv, tH[q]);
-          }
+        for (int q = 0; q < 4; q++) {
+          const double2 a = av[q >> 1], s = sv[q & 1], h = hv[q & 1];
+          tS[q] = fma(w[q][l], fma(a.y, s.y, a.x * s.x), tS[q]);
+          tH[q] = fma(w[q][l], fma(a.y, h.y, a.x * h.x), tH[q]);
         }
       }
-      const int ae = P.afirst[jn], me = P.mult[jn];
+      const int jn = t0 + tc, ae = P.afirst[jn], me = P.mult[jn];
       for (int e = 0; e < me; e++) {
-        double fr[3] = {0.0, 0.0, 0.0};
-        double2 fj, fi[2];
-        if (staged) {
+        double2 fj[2], fi[2];
+        if (ch.staged) {
           const int b = (ae - a0c + e) * SPH_T;
-          fj = sPJ[b + tj];
-#pragma unroll
-          for (int q = 0; q < 2; q++) fi[q] = sPI[b + ti + 16 * q];
+          fj[0] = cPJ[b + jl0];
+          fj[1] = cPJ[b + jl0 + 8];
+          fi[0] = cPI[b + il0];
+          fi[1] = cPI[b + il0 + 4];
         } else {
           const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
-          fj = pa[j0 + tj];
-#pragma unroll
-          for (int q = 0; q < 2; q++) fi[q] = pa[i0 + ti + 16 * q];
+          fj[0] = pa[j0 + jl0];
+          fj[1] = pa[j0 + jl0 + 8];
+          fi[0] = pa[i0 + il0];
+          fi[1] = pa[i0 + il0 + 4];
         }
+        double fr[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
-          if (!act[q]) continue;
-          // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I))
-          const double cpr = fj.x * fi[q].x + fj.y * fi[q].y;
-          const double cpi = fj.x * fi[q].y - fj.y * fi[q].x;
-          const double uim = cpr * rj[q].y + cpi * rj[q].x;  // Im(cP rho(J,I))
-          const double vim = cpr * re[q].y + cpi * re[q].x;  // Im(cP rhoE(J,I))
-          const double g = -2.0 * (tH[q] * uim - tS[q] * vim);
-          fr[0] = fma(g, dx[q][0], fr[0]);
-          fr[1] = fma(g, dx[q][1], fr[1]);
-          fr[2] = fma(g, dx[q][2], fr[2]);
+        for (int q = 0; q < 4; q++) {
+          // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I)); inactive pairs have
+          // rho = rhoE = 0 and add nothing
+          const double2 pj = fj[q >> 1], pi = fi[q & 1];
+          const double cpr = fma(pj.x, pi.x, pj.y * pi.y);
+          const double cpi = fma(pj.x, pi.y, -(pj.y * pi.x));
+          const double uim = fma(cpr, rj[q].y, cpi * rj[q].x);  // Im(cP rho(J,I))
+          const double vim = fma(cpr, re[q].y, cpi * re[q].x);  // Im(cP rhoE(J,I))
+          const double g = fma(tH[q], uim, -(tS[q] * vim));
+#pragma unroll
+          for (int c = 0; c < 3; c++) fr[c] = fma(g, dx[q][c], fr[c]);
         }
-        // warp partials of this atom
+        // sum over the lanes that share lane & 7 (their I rows); lanes 0..7
+        // keep the warp's 8 partials for the end of the chunk
 #pragma unroll
         for (int c = 0; c < 3; c++) {
           double sacc = fr[c];
+          sacc += __shfl_xor_sync(0xffffffffu, sacc, 16);
+          sacc += __shfl_xor_sync(0xffffffffu, sacc, 8);
+          if (ch.staged) {
+            if (lane < 8) red[((ae - a0c + e) * 3 + c) * (FRC_THREADS / 4) + warp * 8 + lane] = sacc;
+          } else {
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
-          if (lane == 0) {
-            if (staged && nred < FRC_RED_ATOMS)
-              red[nred][c][warp] = sacc;
-            else
-              atomicAdd(&F[(ae + e) * 3 + c], sacc);
+            for (int o = 4; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+            if (lane == 0) atomicAdd(&F[(ae + e) * 3 + c], sacc);
           }
         }
-        if (staged) nred++;
       }
     }
     __syncthreads();
-    if (staged)
-      for (int q = tid; q < nred * 3; q += FRC_THREADS) {
-        const int e = q / 3, c = q % 3;
-        double sacc = 0.0;
-        for (int wq = 0; wq < FRC_THREADS / 32; wq++) sacc += red[e][c][wq];
-        atomicAdd(&F[(a0c + e) * 3 + c], sacc);
+    if (ch.staged)  // one warp per (atom, component): 64 partials
+      for (int q = warp; q < ch.na * 3; q += FRC_THREADS / 32) {
+        double sacc = red[q * (FRC_THREADS / 4) + lane] + red[q * (FRC_THREADS / 4) + 32 + lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+        if (lane == 0) atomicAdd(&F[(a0c + q / 3) * 3 + q % 3], sacc);
       }
-    t0 += ntc;
+    t0 = t1;
+    ch = nx;
+    st ^= 1;
   }
 }
 

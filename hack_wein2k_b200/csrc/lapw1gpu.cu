@@ -1573,12 +1573,25 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   int ntiles = 0;
   const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
-  if (!c->smem((const void*)k_force_sph, SPH_DYN_SMEM)) return LAPW1GPU_ERR_CUDA;
+  const size_t nrow = (size_t)nat * ltop * k->nvpad;
+  double2* rowJ = (double2*)c->buf("frc_rowj", sizeof(double2) * nrow);
+  double2* rowI = (double2*)c->buf("frc_rowi", 2 * sizeof(double2) * nrow);
+  if (!rowJ || !rowI) return LAPW1GPU_ERR_NOMEM;
+  k_force_rows<<<dim3((k->nvpad + 127) / 128, nat * ltop), 128, 0, s>>>(P, coef, rowJ, rowI);
+  const bool lt11 = ltop == FRC_LT;
+  const void* fsph = lt11 ? (const void*)k_force_sph<FRC_LT, false> : (const void*)k_force_sph<SPH_LMAX, true>;
+  const int fsmem = frc_smem_bytes(lt11 ? FRC_LT : SPH_LMAX);
+  if (!c->smem(fsph, fsmem)) return LAPW1GPU_ERR_CUDA;
   const size_t nbox = (size_t)(2 * k->tab.d1 + 1) * (2 * k->tab.d2 + 1) * (2 * k->tab.d3 + 1);
   double* bins = (double*)c->buf("frc_bins", sizeof(double) * 2 * nbox);
   if (!bins) return LAPW1GPU_ERR_NOMEM;
   CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
-  k_force_sph<<<ntiles, FRC_THREADS, SPH_DYN_SMEM, s>>>(P, tl, coef, k->tab, rho, rhoe, n, rt, d_grad, bins);
+  if (lt11)
+    k_force_sph<FRC_LT, false><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
+                                                                  d_grad, bins);
+  else
+    k_force_sph<SPH_LMAX, true><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
+                                                                   d_grad, bins);
   k_force_step<<<ndf, 256, 0, s>>>(P, k->tab, bins, d_grad);
   CK(cudaGetLastError());
   if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, rt, d_grad);
