@@ -86,10 +86,11 @@ __device__ __forceinline__ FrcChunk frc_chunk(const DevProb& P, int t0) {
 }
 
 // dynamic shared memory: two stages of type rows (J: 1, I: 2 double2 per
-// row and l) and of phases, then the per-warp force partials of a chunk's
-// atoms (8 per warp and component)
+// row and l) and of phases, the per-warp force partials of a chunk's atoms
+// (8 per warp and component), and -4 pi KZZ of the tile's 64 rows
 __host__ __device__ constexpr int frc_smem_bytes(int lt) {
-  return (2 * frc_tc(lt) * lt * SPH_T * 3 + 2 * 2 * FRC_MAXA * SPH_T) * 16 + FRC_MAXA * 3 * FRC_THREADS / 4 * 8;
+  return (2 * frc_tc(lt) * lt * SPH_T * 3 + 2 * 2 * FRC_MAXA * SPH_T) * 16 + FRC_MAXA * 3 * FRC_THREADS / 4 * 8 +
+         2 * SPH_T * 4 * 8;
 }
 
 // One block per 32 x 32 pair tile, 256 threads.  Thread (warp, lane) owns
@@ -113,6 +114,7 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
   double2* sI = sJ + 2 * TC * LT * SPH_T;  // [2][TC][LT][SPH_T][S, H]
   double2* sP = sI + 4 * TC * LT * SPH_T;  // [2][J, I][FRC_MAXA][SPH_T]
   double* red = reinterpret_cast<double*>(sP + 4 * FRC_MAXA * SPH_T);  // [FRC_MAXA][3][8 warps x 8]
+  double* sK = red + FRC_MAXA * 3 * (FRC_THREADS / 4);                   // [J 0..31, I 32..63][4]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int2 t = tiles[blockIdx.x];
   const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
@@ -148,16 +150,23 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
 
   FrcChunk ch = frc_chunk<TC>(P, 0);
   stage(0, 0, ch);
+  // the pair term carries -2 (2 pi dK) = -4 pi (KZZ_I - KZZ_J): per row
+  // -4 pi KZZ, read once per atom
+  if (tid < 2 * SPH_T) {
+    const int R = (tid < SPH_T ? j0 : i0 - SPH_T) + tid;
+    const bool in = R < nv;
+#pragma unroll
+    for (int c = 0; c < 3; c++) sK[tid * 4 + c] = in ? -2.0 * FRC_2PI * P.kzz[3 * R + c] : 0.0;
+    sK[tid * 4 + 3] = 0.0;
+  }
 
   double w[4][LT];
-  double dx[4][3];
   double2 rj[4], re[4];  // rho(J,I) and rhoE(J,I) of the owned pairs; zero for inactive pairs
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int J = j0 + jl0 + 8 * (q >> 1), I = i0 + il0 + 4 * (q & 1);
     const bool act = (J < nv && I < nv && J < I);
     double x = 0.0;
-    dx[q][0] = dx[q][1] = dx[q][2] = 0.0;
     rj[q] = re[q] = cmk(0.0, 0.0);
     if (act) {
       x = P.xk[I] * P.xk[J] + P.yk[I] * P.yk[J] + P.zk[I] * P.zk[J];
@@ -165,10 +174,6 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
       if (den > 1.0e-8) x = x / den;
       const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
                 d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
-      // -2 of the pair term folded in
-      dx[q][0] = -2.0 * FRC_2PI * d0;
-      dx[q][1] = -2.0 * FRC_2PI * d1;
-      dx[q][2] = -2.0 * FRC_2PI * d2;
       // rt: the density matrices hold conj(rho(J,I)) at (I, J) instead
       rj[q] = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
       re[q] = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
@@ -221,15 +226,24 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
       for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
       const double2* bJ = cJ + tc * LT * SPH_T + jl0;
       const double2* bI = cI + tc * LT * 2 * SPH_T + 2 * il0;
+      // the row values of l + 1 are read while l is summed
+      double2 av[2] = {bJ[0], bJ[8]}, sv[2] = {bI[0], bI[8]}, hv[2] = {bI[1], bI[9]};
 #pragma unroll
       for (int l = 0; l < LT; l++) {
         if (GUARD && l >= ltop) break;
-        const int o = l * SPH_T;
-        const double2 av[2] = {bJ[o], bJ[o + 8]};
-        const double2 sv[2] = {bI[2 * o], bI[2 * o + 8]}, hv[2] = {bI[2 * o + 1], bI[2 * o + 9]};
+        const double2 a0 = av[0], a1 = av[1], s0 = sv[0], s1 = sv[1], h0 = hv[0], h1 = hv[1];
+        if (l + 1 < LT) {
+          const int o = (l + 1) * SPH_T;
+          av[0] = bJ[o];
+          av[1] = bJ[o + 8];
+          sv[0] = bI[2 * o];
+          sv[1] = bI[2 * o + 8];
+          hv[0] = bI[2 * o + 1];
+          hv[1] = bI[2 * o + 9];
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          const double2 a = av[q >> 1], s = sv[q & 1], h = hv[q & 1];
+          const double2 a = (q >> 1) ? a1 : a0, s = (q & 1) ? s1 : s0, h = (q & 1) ? h1 : h0;
           tS[q] = fma(w[q][l], fma(a.y, s.y, a.x * s.x), tS[q]);
           tH[q] = fma(w[q][l], fma(a.y, h.y, a.x * h.x), tH[q]);
         }
@@ -250,7 +264,7 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
           fi[0] = pa[i0 + il0];
           fi[1] = pa[i0 + il0 + 4];
         }
-        double fr[3] = {0.0, 0.0, 0.0};
+        double g[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I)); inactive pairs have
@@ -260,10 +274,19 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
           const double cpi = fma(pj.x, pi.y, -(pj.y * pi.x));
           const double uim = fma(cpr, rj[q].y, cpi * rj[q].x);  // Im(cP rho(J,I))
           const double vim = fma(cpr, re[q].y, cpi * re[q].x);  // Im(cP rhoE(J,I))
-          const double g = fma(tH[q], uim, -(tS[q] * vim));
-#pragma unroll
-          for (int c = 0; c < 3; c++) fr[c] = fma(g, dx[q][c], fr[c]);
+          g[q] = fma(tH[q], uim, -(tS[q] * vim));
         }
+        // sum_q g_q (K_I - K_J): by I row and by J row
+        const double gi0 = g[0] + g[2], gi1 = g[1] + g[3], gj0 = g[0] + g[1], gj1 = g[2] + g[3];
+        const double2* k2 = reinterpret_cast<const double2*>(sK);  // row r: k2[2r] = (x, y), k2[2r + 1].x = z
+        const double2 kI0 = k2[2 * (SPH_T + il0)], kI1 = k2[2 * (SPH_T + il0 + 4)];
+        const double2 kJ0 = k2[2 * jl0], kJ1 = k2[2 * (jl0 + 8)];
+        const double zI0 = k2[2 * (SPH_T + il0) + 1].x, zI1 = k2[2 * (SPH_T + il0 + 4) + 1].x;
+        const double zJ0 = k2[2 * jl0 + 1].x, zJ1 = k2[2 * (jl0 + 8) + 1].x;
+        double fr[3];
+        fr[0] = fma(gi0, kI0.x, fma(gi1, kI1.x, -fma(gj0, kJ0.x, gj1 * kJ1.x)));
+        fr[1] = fma(gi0, kI0.y, fma(gi1, kI1.y, -fma(gj0, kJ0.y, gj1 * kJ1.y)));
+        fr[2] = fma(gi0, zI0, fma(gi1, zI1, -fma(gj0, zJ0, gj1 * zJ1)));
         // sum over the lanes that share lane & 7 (their I rows); lanes 0..7
         // keep the warp's 8 partials for the end of the chunk
 #pragma unroll
