@@ -220,8 +220,8 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
     const double2* cPJ = sP + st * 2 * FRC_MAXA * SPH_T;
     const double2* cPI = cPJ + FRC_MAXA * SPH_T;
     const int a0c = P.afirst[t0];
-    for (int tc = 0; tc < ch.ntc; tc++) {
-      double tS[4], tH[4];
+    // l sums of type tc for the four pairs
+    auto lsum = [&](int tc, double(&tS)[4], double(&tH)[4]) {
 #pragma unroll
       for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
       const double2* bJ = cJ + tc * LT * SPH_T + jl0;
@@ -248,58 +248,87 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
           tH[q] = fma(w[q][l], fma(a.y, h.y, a.x * h.x), tH[q]);
         }
       }
-      const int jn = t0 + tc, ae = P.afirst[jn], me = P.mult[jn];
-      for (int e = 0; e < me; e++) {
-        double2 fj[2], fi[2];
-        if (ch.staged) {
-          const int b = (ae - a0c + e) * SPH_T;
-          fj[0] = cPJ[b + jl0];
-          fj[1] = cPJ[b + jl0 + 8];
-          fi[0] = cPI[b + il0];
-          fi[1] = cPI[b + il0 + 4];
-        } else {
-          const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
-          fj[0] = pa[j0 + jl0];
-          fj[1] = pa[j0 + jl0 + 8];
-          fi[0] = pa[i0 + il0];
-          fi[1] = pa[i0 + il0 + 4];
-        }
-        double g[4];
+    };
+    // this thread's share of one atom's force (phases fj of the J rows, fi
+    // of the I rows), reduced over the lanes that share lane & 7 (their I
+    // rows): lanes 0..7 hold the warp's 8 partials
+    auto fterm = [&](const double2(&fj)[2], const double2(&fi)[2], const double(&tS)[4], const double(&tH)[4],
+                     double(&fr)[3]) {
+      double g[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I)); inactive pairs have
+        // rho = rhoE = 0 and add nothing
+        const double2 pj = fj[q >> 1], pi = fi[q & 1];
+        const double cpr = fma(pj.x, pi.x, pj.y * pi.y);
+        const double cpi = fma(pj.x, pi.y, -(pj.y * pi.x));
+        const double uim = fma(cpr, rj[q].y, cpi * rj[q].x);  // Im(cP rho(J,I))
+        const double vim = fma(cpr, re[q].y, cpi * re[q].x);  // Im(cP rhoE(J,I))
+        g[q] = fma(tH[q], uim, -(tS[q] * vim));
+      }
+      // sum_q g_q (K_I - K_J): by I row and by J row
+      const double gi0 = g[0] + g[2], gi1 = g[1] + g[3], gj0 = g[0] + g[1], gj1 = g[2] + g[3];
+      const double2* k2 = reinterpret_cast<const double2*>(sK);  // row r: k2[2r] = (x, y), k2[2r + 1].x = z
+      const double2 kI0 = k2[2 * (SPH_T + il0)], kI1 = k2[2 * (SPH_T + il0 + 4)];
+      const double2 kJ0 = k2[2 * jl0], kJ1 = k2[2 * (jl0 + 8)];
+      const double zI0 = k2[2 * (SPH_T + il0) + 1].x, zI1 = k2[2 * (SPH_T + il0 + 4) + 1].x;
+      const double zJ0 = k2[2 * jl0 + 1].x, zJ1 = k2[2 * (jl0 + 8) + 1].x;
+      fr[0] = fma(gi0, kI0.x, fma(gi1, kI1.x, -fma(gj0, kJ0.x, gj1 * kJ1.x)));
+      fr[1] = fma(gi0, kI0.y, fma(gi1, kI1.y, -fma(gj0, kJ0.y, gj1 * kJ1.y)));
+      fr[2] = fma(gi0, zI0, fma(gi1, zI1, -fma(gj0, zJ0, gj1 * zJ1)));
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], 16);
+        fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], 8);
+      }
+    };
+    // staged atom slot e of the chunk: partials into red[] for the chunk's end
+    auto fstaged = [&](int e, const double(&tS)[4], const double(&tH)[4]) {
+      const int b = e * SPH_T;
+      const double2 fj[2] = {cPJ[b + jl0], cPJ[b + jl0 + 8]}, fi[2] = {cPI[b + il0], cPI[b + il0 + 4]};
+      double fr[3];
+      fterm(fj, fi, tS, tH, fr);
+      if (lane < 8) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) red[(e * 3 + c) * (FRC_THREADS / 4) + warp * 8 + lane] = fr[c];
+      }
+    };
+    if (ch.staged && ch.na == ch.ntc) {
+      // one atom per type (slot tc): the force terms of type tc - 1 are
+      // formed in the same straight-line block as the l sums of type tc,
+      // so that the reduction's latency overlaps the sums
+      double pS[4], pH[4];
+      lsum(0, pS, pH);
+      for (int tc = 1; tc < ch.ntc; tc++) {
+        double tS[4], tH[4];
+        lsum(tc, tS, tH);
+        fstaged(tc - 1, pS, pH);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          // cP = conj(phi_J) phi_I = conj(PHASE_a(J,I)); inactive pairs have
-          // rho = rhoE = 0 and add nothing
-          const double2 pj = fj[q >> 1], pi = fi[q & 1];
-          const double cpr = fma(pj.x, pi.x, pj.y * pi.y);
-          const double cpi = fma(pj.x, pi.y, -(pj.y * pi.x));
-          const double uim = fma(cpr, rj[q].y, cpi * rj[q].x);  // Im(cP rho(J,I))
-          const double vim = fma(cpr, re[q].y, cpi * re[q].x);  // Im(cP rhoE(J,I))
-          g[q] = fma(tH[q], uim, -(tS[q] * vim));
+          pS[q] = tS[q];
+          pH[q] = tH[q];
         }
-        // sum_q g_q (K_I - K_J): by I row and by J row
-        const double gi0 = g[0] + g[2], gi1 = g[1] + g[3], gj0 = g[0] + g[1], gj1 = g[2] + g[3];
-        const double2* k2 = reinterpret_cast<const double2*>(sK);  // row r: k2[2r] = (x, y), k2[2r + 1].x = z
-        const double2 kI0 = k2[2 * (SPH_T + il0)], kI1 = k2[2 * (SPH_T + il0 + 4)];
-        const double2 kJ0 = k2[2 * jl0], kJ1 = k2[2 * (jl0 + 8)];
-        const double zI0 = k2[2 * (SPH_T + il0) + 1].x, zI1 = k2[2 * (SPH_T + il0 + 4) + 1].x;
-        const double zJ0 = k2[2 * jl0 + 1].x, zJ1 = k2[2 * (jl0 + 8) + 1].x;
-        double fr[3];
-        fr[0] = fma(gi0, kI0.x, fma(gi1, kI1.x, -fma(gj0, kJ0.x, gj1 * kJ1.x)));
-        fr[1] = fma(gi0, kI0.y, fma(gi1, kI1.y, -fma(gj0, kJ0.y, gj1 * kJ1.y)));
-        fr[2] = fma(gi0, zI0, fma(gi1, zI1, -fma(gj0, zJ0, gj1 * zJ1)));
-        // sum over the lanes that share lane & 7 (their I rows); lanes 0..7
-        // keep the warp's 8 partials for the end of the chunk
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          double sacc = fr[c];
-          sacc += __shfl_xor_sync(0xffffffffu, sacc, 16);
-          sacc += __shfl_xor_sync(0xffffffffu, sacc, 8);
+      }
+      fstaged(ch.ntc - 1, pS, pH);
+    } else {
+      for (int tc = 0; tc < ch.ntc; tc++) {
+        double tS[4], tH[4];
+        lsum(tc, tS, tH);
+        const int jn = t0 + tc, ae = P.afirst[jn], me = P.mult[jn];
+        for (int e = 0; e < me; e++) {
           if (ch.staged) {
-            if (lane < 8) red[((ae - a0c + e) * 3 + c) * (FRC_THREADS / 4) + warp * 8 + lane] = sacc;
+            fstaged(ae - a0c + e, tS, tH);
           } else {
+            const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
+            const double2 fj[2] = {pa[j0 + jl0], pa[j0 + jl0 + 8]}, fi[2] = {pa[i0 + il0], pa[i0 + il0 + 4]};
+            double fr[3];
+            fterm(fj, fi, tS, tH, fr);
 #pragma unroll
-            for (int o = 4; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
-            if (lane == 0) atomicAdd(&F[(ae + e) * 3 + c], sacc);
+            for (int c = 0; c < 3; c++) {
+#pragma unroll
+              for (int o = 4; o > 0; o >>= 1) fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], o);
+              if (lane == 0) atomicAdd(&F[(ae + e) * 3 + c], fr[c]);
+            }
           }
         }
       }
