@@ -59,7 +59,7 @@ __global__ void k_force_rows(DevProb P, const SphCoef* __restrict__ coef, double
 #define FRC_LT 11    // l count of the specialised kernel (lmax = 10)
 
 // types per staged chunk: as many as the shared memory holds twice
-__host__ __device__ constexpr int frc_tc(int lt) { return lt <= FRC_LT ? 4 : 3; }
+__host__ __device__ constexpr int frc_tc(int lt) { return lt <= FRC_LT ? 5 : 4; }
 
 __device__ __forceinline__ void frc_cp16(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
