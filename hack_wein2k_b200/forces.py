@@ -101,3 +101,49 @@ def finite_difference(gctx: "lapw1gpu.Context", prob: Problem, occ: torch.Tensor
         kp.free()
         vals.append(float(E))
     return (vals[0] - vals[1]) / (2.0 * h)
+
+
+def _main() -> None:
+    """Time the adjoint on a seeded workload: one setup, the device
+    eigen-solve for the lowest `--bands` states, then `--repeat` calls of
+    lapw1gpu_forces timed with CUDA events on the current stream.  Prints
+    one JSON line."""
+    import argparse
+    import json
+
+    from . import synth
+    ap = argparse.ArgumentParser(prog="python -m hack_wein2k_b200.forces")
+    ap.add_argument("--case", default="c3", help="synthetic workload name (c0..c4)")
+    ap.add_argument("--prec", choices=["fp64", "split"], default="split")
+    ap.add_argument("--bands", type=int, default=400)
+    ap.add_argument("--repeat", type=int, default=3)
+    a = ap.parse_args()
+    dev = torch.device("cuda", 0)
+    gctx = lapw1gpu.Context(0)
+    if a.prec == "split":
+        gctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+        gctx.set_slices(5, 4)
+    prob = synth.config(a.case)[0]
+    occ = torch.ones(a.bands, dtype=torch.float64, device=dev)
+    kp, hs, hd = _setup_device(gctx, prob)
+    H, S = hermitian_from_packed_device(hs, hd)
+    del hs, hd
+    w, X = solve(H, S, nmax=a.bands)
+    del H, S
+    torch.cuda.empty_cache()
+    ms = []
+    for _ in range(a.repeat):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g = gradient(gctx, kp, X, occ, w)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"case": a.case, "n": prob.n, "prec": a.prec, "bands": a.bands, "forces_ms": ms,
+                      "max_abs_grad": float(g.abs().max())}))
+    kp.free()
+    gctx.close()
+
+
+if __name__ == "__main__":
+    _main()
