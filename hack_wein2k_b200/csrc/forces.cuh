@@ -30,7 +30,7 @@
 //                   -Im sum_n f_n sum_k [Y0 conj(Zc) - Yc conj(Z0)],
 //                 Y = conj(X)^T (G c), Z = T Y.  Y = R^H (G c) for the
 //                 (ALM, BLM) rows and CLM^H (G c) over the LO rows (library
-//                 ZGEMMs); Z = T Y per atom (k_force_hns_z, k_force_hns_zc):
+//                 ZGEMMs); Z = T Y per atom (k_force_hns_z, zc = 0 and 1):
 //                 for the CLM rows this is the CLM row of T applied to
 //                 plane-wave rows too, which the lower triangle never uses
 #pragma once
@@ -222,8 +222,6 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
     const int a0c = P.afirst[t0];
     // l sums of type tc for the four pairs
     auto lsum = [&](int tc, double(&tS)[4], double(&tH)[4]) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) tS[q] = tH[q] = 0.0;
       const double2* bJ = cJ + tc * LT * SPH_T + jl0;
       const double2* bI = cI + tc * LT * 2 * SPH_T + 2 * il0;
       // the row values of l + 1 are read while l is summed
@@ -244,8 +242,13 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           const double2 a = (q >> 1) ? a1 : a0, s = (q & 1) ? s1 : s0, h = (q & 1) ? h1 : h0;
-          tS[q] = fma(w[q][l], fma(a.y, s.y, a.x * s.x), tS[q]);
-          tH[q] = fma(w[q][l], fma(a.y, h.y, a.x * h.x), tH[q]);
+          if (l == 0) {  // w_0 = P_0 = 1
+            tS[q] = fma(a.y, s.y, a.x * s.x);
+            tH[q] = fma(a.y, h.y, a.x * h.x);
+          } else {
+            tS[q] = fma(w[q][l], fma(a.y, s.y, a.x * s.x), tS[q]);
+            tH[q] = fma(w[q][l], fma(a.y, h.y, a.x * h.x), tH[q]);
+          }
         }
       }
     };
@@ -557,51 +560,60 @@ __global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int
   Ce[(size_t)b * n + i] = cscale(v, f[b] * eps[b]);
 }
 
-// Z_AB[a][(ro, lm)][col] = sum_(r,b) M[(ro,lm)][(r,b)] Y[a][(r,b)][col]
-//                          + T_(ro,C)[lm][b] Y_C[a][b][col]
-// (M = [[TUU, TDU], [TUD, TDD]], T_(A,C) = TUU21, T_(B,C) = TUD21): the
-// product L^T (G c) through the small T of each atom instead of a second
-// N x K GEMM, because L = M conj(R) (+ the CLM terms of the LO rows).
-// Y, Z: [col][K]; Yc: [col][Kc] (null when there are no LO rows)
-__global__ void k_force_hns_z(int nsl2, int K, int Kc, const int* __restrict__ atype, const double2* __restrict__ tns,
-                              const double2* __restrict__ Y, const double2* __restrict__ Yc,
-                              double2* __restrict__ Z) {
-  const int col = blockIdx.x, a = blockIdx.y, ko = threadIdx.x;
-  if (ko >= 2 * nsl2) return;
-  const int ro = ko / nsl2, la = ko % nsl2;
+// Z = T Y per atom: the product L^T (G c) through the small T of each atom
+// instead of a second N x K GEMM, because L = M conj(R) (+ the CLM terms of
+// the LO rows).  FRC_ZCOLS columns of Y per block: the atom type's T blocks
+// and the columns' Y entries of the atom are staged in shared memory once.  Y: [col][K] (k = (a*2 + r)*nsl2 + b), Yc, Zc: [col][Kc]
+// (k = a*nsl2 + lm), col < ncol = 4 nb.
+//   zc = 0: Z[a][(r, lm)] = sum_b T_(r,A)[lm][b] Y_A[b] + T_(r,B)[lm][b] Y_B[b]
+//           (+ T_(r,C)[lm][b] Yc[b] with LOs), with (A, B, C) = (TUU, TDU,
+//           TUU21) for r = 0 and (TUD, TDD, TUD21) for r = 1;
+//   zc = 1: Zc[a][lm] = sum_b TUU12[lm][b] Y_A[b] + TDU12[lm][b] Y_B[b] +
+//           TUU22[lm][b] Yc[b]: the CLM row of T applied to Y over all rows.
+#define FRC_ZCOLS 32
+#define FRC_ZSMEM ((6 * L1G_NSL2 * L1G_NSL2 + FRC_ZCOLS * 3 * L1G_NSL2) * 16)
+__global__ void __launch_bounds__(256) k_force_hns_z(int zc, int nsl2, int K, int Kc, int ncol,
+                                                     const int* __restrict__ atype, const double2* __restrict__ tns,
+                                                     const double2* __restrict__ Y, const double2* __restrict__ Yc,
+                                                     double2* __restrict__ Z, double2* __restrict__ Zc) {
+  extern __shared__ double2 zsm[];
+  double2* sT = zsm;                            // [6 blocks][L1G_NSL2][L1G_NSL2]
+  double2* sY = sT + 6 * L1G_NSL2 * L1G_NSL2;  // [FRC_ZCOLS][A, B, C][L1G_NSL2]
+  const int a = blockIdx.y, c0 = blockIdx.x * FRC_ZCOLS, tid = threadIdx.x;
+  const int nc = min(FRC_ZCOLS, ncol - c0);
   const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  const double2* y = Y + (size_t)col * K + (size_t)a * 2 * nsl2;
-  const int bA = ro == 0 ? 0 : 3, bB = ro == 0 ? 1 : 4, bC = ro == 0 ? 2 : 5;  // TUU TDU TUU21 / TUD TDD TUD21
-  double2 z = cmk(0.0, 0.0);
-  for (int b = 0; b < nsl2; b++) {
-    z = cadd(z, cmul(T[((size_t)bA * L1G_NSL2 + la) * L1G_NSL2 + b], y[b]));
-    z = cadd(z, cmul(T[((size_t)bB * L1G_NSL2 + la) * L1G_NSL2 + b], y[nsl2 + b]));
+  const int nb = zc ? 3 : 6, b0 = zc ? 6 : 0;  // T blocks used
+  for (int i = tid; i < nb * nsl2 * nsl2; i += blockDim.x) {
+    const int blk = i / (nsl2 * nsl2), r = i % (nsl2 * nsl2), lm = r / nsl2, b = r % nsl2;
+    sT[(blk * L1G_NSL2 + lm) * L1G_NSL2 + b] = T[((size_t)(b0 + blk) * L1G_NSL2 + lm) * L1G_NSL2 + b];
   }
-  if (Yc) {
-    const double2* yc = Yc + (size_t)col * Kc + (size_t)a * nsl2;
-    for (int b = 0; b < nsl2; b++) z = cadd(z, cmul(T[((size_t)bC * L1G_NSL2 + la) * L1G_NSL2 + b], yc[b]));
+  for (int i = tid; i < nc * 3 * nsl2; i += blockDim.x) {
+    const int cl = i / (3 * nsl2), r = i % (3 * nsl2), part = r / nsl2, b = r % nsl2;
+    double2 v = cmk(0.0, 0.0);
+    if (part < 2)
+      v = Y[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + part * nsl2 + b];
+    else if (Yc)
+      v = Yc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + b];
+    sY[(cl * 3 + part) * L1G_NSL2 + b] = v;
   }
-  Z[(size_t)col * K + (size_t)a * 2 * nsl2 + ko] = z;
-}
-
-// Z_C[a][lm][col] = sum_(r,b) T_(C,r)[lm][b] Y[a][(r,b)][col] + TUU22 Y_C:
-// the CLM row of T applied to Y over all rows.  Y: [col][K] (k = (a*2 +
-// r)*nsl2 + b), Yc and Zc: [col][Kc] (k = a*nsl2 + lm), col < 4 nb
-__global__ void k_force_hns_zc(int nsl2, int K, int Kc, const int* __restrict__ atype,
-                               const double2* __restrict__ tns, const double2* __restrict__ Y,
-                               const double2* __restrict__ Yc, double2* __restrict__ Zc) {
-  const int col = blockIdx.x, a = blockIdx.y, la = threadIdx.x;
-  if (la >= nsl2) return;
-  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  const double2* y = Y + (size_t)col * K + (size_t)a * 2 * nsl2;
-  const double2* yc = Yc + (size_t)col * Kc + (size_t)a * nsl2;
-  double2 z = cmk(0.0, 0.0);
-  for (int b = 0; b < nsl2; b++) {
-    z = cadd(z, cmul(T[((size_t)6 * L1G_NSL2 + la) * L1G_NSL2 + b], y[b]));          // TUU12
-    z = cadd(z, cmul(T[((size_t)7 * L1G_NSL2 + la) * L1G_NSL2 + b], y[nsl2 + b]));   // TDU12
-    z = cadd(z, cmul(T[((size_t)8 * L1G_NSL2 + la) * L1G_NSL2 + b], yc[b]));         // TUU22
+  __syncthreads();
+  const int nout = zc ? nsl2 : 2 * nsl2;
+  for (int i = tid; i < nc * nout; i += blockDim.x) {
+    const int cl = i / nout, ko = i % nout;
+    const int ro = zc ? 0 : ko / nsl2, lm = zc ? ko : ko % nsl2;
+    const double2* tA = sT + ((3 * ro) * L1G_NSL2 + lm) * L1G_NSL2;  // blocks (A, B, C) of row ro
+    const double2* y = sY + cl * 3 * L1G_NSL2;
+    double2 z = cmk(0.0, 0.0);
+    for (int b = 0; b < nsl2; b++) {
+      z = cadd(z, cmul(tA[b], y[b]));
+      z = cadd(z, cmul(tA[L1G_NSL2 * L1G_NSL2 + b], y[L1G_NSL2 + b]));
+      z = cadd(z, cmul(tA[2 * L1G_NSL2 * L1G_NSL2 + b], y[2 * L1G_NSL2 + b]));  // zero without LOs
+    }
+    if (zc)
+      Zc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + lm] = z;
+    else
+      Z[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + ko] = z;
   }
-  Zc[(size_t)col * Kc + (size_t)a * nsl2 + la] = z;
 }
 
 // F_a,c -= Im sum_n f_n sum_{k in a} [Y0 conj(Zc) - Yc conj(Z0)]; Y*, Z* are

@@ -1640,11 +1640,13 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
                       (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc, Kc) != CUBLAS_STATUS_SUCCESS)
         return LAPW1GPU_ERR_CUDA;
     }
-    k_force_hns_z<<<dim3(4 * nb, ndf), 64, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Z);
+    if (!c->smem((const void*)k_force_hns_z, FRC_ZSMEM)) return LAPW1GPU_ERR_CUDA;
+    const dim3 zgrid((4 * nb + FRC_ZCOLS - 1) / FRC_ZCOLS, ndf);
+    k_force_hns_z<<<zgrid, 256, FRC_ZSMEM, s>>>(0, nsl2, K, Kc, 4 * nb, P.atype, k->d_tns, Y, Yc, Z, nullptr);
     k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
     CK(cudaGetLastError());
     if (nlo > 0) {
-      k_force_hns_zc<<<dim3(4 * nb, ndf), 32, 0, s>>>(nsl2, K, Kc, P.atype, k->d_tns, Y, Yc, Zc);
+      k_force_hns_z<<<zgrid, 256, FRC_ZSMEM, s>>>(1, nsl2, K, Kc, 4 * nb, P.atype, k->d_tns, Y, Yc, nullptr, Zc);
       k_force_hns_reduce<<<ndf, 256, 0, s>>>(nsl2, Kc, nb, Yc, Zc, d_occ, d_grad);
       CK(cudaGetLastError());
     }
