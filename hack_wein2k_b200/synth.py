@@ -295,6 +295,15 @@ def cell_small_mixed():
     ])
 
 
+def cell_many_equiv():
+    """P cubic cell (10.5 bohr) on a 3 x 3 x 3 grid of sites 3.5 bohr apart:
+    one type of MULT 17 (more equivalent atoms than one staged chunk of the
+    force kernel holds) and five one-atom types, Rmt 1.1 everywhere."""
+    sites = [[(i + 0.5) / 3.0, (j + 0.5) / 3.0, (k + 0.5) / 3.0] for i in range(3) for j in range(3) for k in range(3)]
+    types = [dict(pos=sites[:17], rmt=1.1)] + [dict(pos=[sites[17 + 2 * t]], rmt=1.1) for t in range(5)]
+    return Cell("P", (10.5, 10.5, 10.5), (90.0, 90.0, 90.0), types)
+
+
 def small_case(kind: str = "lo", seed: int = 7, rkmax: float = 5.0) -> Problem:
     """Small problems that exercise every branch: LOs with MULT>1, APW+lo,
     local rotations, HORB, INS != 0."""
@@ -317,4 +326,6 @@ def small_case(kind: str = "lo", seed: int = 7, rkmax: float = 5.0) -> Problem:
                              name="small-multilo")
     if kind == "gamma":
         return synth_problem(cell, rkmax, (0.0, 0.0, 0.0), seed=seed, lo_l=(0, 1), name="small-gamma")
+    if kind == "manyeq":
+        return synth_problem(cell_many_equiv(), rkmax, k, seed=seed, name="small-manyeq")
     raise ValueError(kind)

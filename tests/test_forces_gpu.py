@@ -67,6 +67,40 @@ def test_split_density_matrices_match_fp64(ctx, kind):
     assert np.abs(gs - g64).max() <= 1e-8 * scale, (gs, g64)
 
 
+@pytest.fixture(scope="module")
+def manyeq_ref():
+    p = synth.small_case("manyeq", rkmax=2.5)
+    w, _ = FR.eigh(p)
+    nb, _ = FR.gapped_nb(w)
+    return p, nb, w, FR.hf_gradient(p, nb)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "split"])
+def test_adjoint_many_equivalent_atoms(ctx, manyeq_ref, prec):
+    """One type of 17 equivalent atoms (more than a staged chunk of the
+    spherical force kernel holds: its phases are read from global memory)
+    and five one-atom types (the path that forms one type's force terms
+    beside the next type's l sums): the gradient of all 22 atoms matches
+    the oracle's Hellmann-Feynman sum (split: density matrices as int8
+    slice products, 1e-7 of the largest component)."""
+    p, nb, w, ref = manyeq_ref
+    dev = torch.device("cuda", ctx.device)
+    occ = _occ(p, nb).to(dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    if prec == "split":
+        ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    try:
+        g = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+        kp.free()
+    assert np.abs(eps.cpu().numpy() - w[:nb]).max() <= 1e-9
+    scale = np.abs(ref).max()
+    assert scale > 0
+    assert np.abs(g - ref).max() <= (TOL_HF if prec == "fp64" else 1e-7) * scale, (g, ref)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["lo", "ins"])
 def test_autograd_matches_band_energy_fd(ctx, kind):

@@ -13,7 +13,7 @@ from tests.helpers import rel_errors
 
 TOL_FP64 = 1e-12
 
-SMALL = ["plain", "lo", "apw", "ins", "orb", "multilo", "gamma"]
+SMALL = ["plain", "lo", "apw", "ins", "orb", "multilo", "gamma", "manyeq"]
 
 
 @pytest.mark.gpu

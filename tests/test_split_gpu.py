@@ -32,7 +32,7 @@ def sctx():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("slices", [4, 5, 6, 7, 8])
-@pytest.mark.parametrize("kind", ["lo", "apw", "multilo"])
+@pytest.mark.parametrize("kind", ["lo", "apw", "multilo", "manyeq"])
 def test_split_small(sctx, kind, slices):
     sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
     p = synth.small_case(kind)
