@@ -1555,11 +1555,11 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
                            cudaMemcpyDeviceToDevice, s));
       Cn = Cc;
     }
-    CK(cudaMemsetAsync(rho, 0, sizeof(double2) * (size_t)n * n, s));
-    CK(cudaMemsetAsync(rhoe, 0, sizeof(double2) * (size_t)n * n, s));
+    // written, not added (no zero fill): every lower-triangle element the
+    // force kernels read is a product tile's element
     int nlr = 0;
-    int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices, s, &nlr, nullptr, nullptr);
-    if (!rc) rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices, s, &nlr, nullptr, nullptr);
+    int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
+    if (!rc) rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
     if (rc) return rc;
     rt = 1;
   } else {
@@ -1622,9 +1622,8 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       if (!Lt || !Gt) return LAPW1GPU_ERR_NOMEM;
       k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
       k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
-      CK(cudaMemsetAsync(Y, 0, sizeof(double2) * (size_t)4 * nb * K, s));
       int nly = 0;
-      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices, s, &nly);
+      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices, s, &nly, 1);
       if (rc) return rc;
     } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
                            (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS) {

@@ -215,8 +215,12 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows(const double2* __restrict
 template <int S>
 __global__ void __launch_bounds__(SPLIT_THREADS, 1)
     k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                 const int2* __restrict__ tiles, int nkb, int n, int nr, int rect, const int* __restrict__ exA,
+                 const int2* __restrict__ tiles, int nkb, int n, int nr, int mode, const int* __restrict__ exA,
                  const int* __restrict__ exB, double2* __restrict__ hs, int ld, int* __restrict__ status) {
+  // mode bit 0: rectangular product (all i < n, j < nr) instead of the
+  // lower triangle j <= i; bit 1: overwrite the output instead of adding
+  // to it (no prefetch of the old values)
+  const int rect = mode & 1, ovw = mode & 2;
   using C = Cfg<S>;
   constexpr int N = C::N, STAGES = C::STAGES;
   extern __shared__ uint8_t smem_raw[];
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1)
     for (int q = 0; q < 8; q++) {
       const int j = j0 + (cbase + c) * 8 + q;
       old[c][q] = make_double2(0.0, 0.0);
-      if (cbase + c < NCT && i < n && j < nr && (rect || j <= i))
+      if (!ovw && cbase + c < NCT && i < n && j < nr && (rect || j <= i))
         asm volatile("ld.global.v2.f64 {%0, %1}, [%2];"
                      : "=d"(old[c][q].x), "=d"(old[c][q].y)
                      : "l"(hs + (size_t)j * ld + i));
@@ -446,9 +450,10 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
 template <int S>
 static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                              const double2* Lop, const double2* Rop, double2* hs, int ld, cudaStream_t s,
-                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL, int phase) {
+                             int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL, int phase, int ovw) {
   // phase 1: row exponents and slices only; 2: the products only (the
-  // slices of this set are ready); 3: both
+  // slices of this set are ready); 3: both.  ovw: write the products
+  // instead of adding them to hs
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
@@ -506,8 +511,8 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
                                       if (bj * Cf::JT <= bi * 128 + 127) t.push_back(make_int2(bi, bj));
                               });
     if (!dt) return LAPW1GPU_ERR_NOMEM;
-    split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, n, 0, exA, exB,
-                                                                             hs, ld, c->d_status);
+    split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, n, n, ovw ? 2 : 0,
+                                                                             exA, exB, hs, ld, c->d_status);
     *nlaunch += 1;
     if (hp && hp->groups > 0 && hp->col[g + 1] <= k->nv) {
       if (cudaEventRecord(hp->ev[g], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
@@ -524,7 +529,7 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
 template <int S>
 static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
                            const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
-                           cudaStream_t s, int* nlaunch) {
+                           cudaStream_t s, int* nlaunch, int ovw) {
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
@@ -558,20 +563,20 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
                             });
   if (!dt) return LAPW1GPU_ERR_NOMEM;
   if (!c->smem((const void*)split::k_split_gemm<S>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
-  split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, 1, exA, exB,
-                                                                           out, ld, c->d_status);
+  split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, ovw ? 3 : 1,
+                                                                           exA, exB, out, ld, c->d_status);
   *nlaunch += 1;
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
 static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
                            const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
-                           int slices, cudaStream_t s, int* nlaunch) {
+                           int slices, cudaStream_t s, int* nlaunch, int ovw = 0) {
   switch (slices) {
-    case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
-    case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
-    case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
-    case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch);
+    case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }
@@ -579,15 +584,16 @@ static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
 // cjL: Lop holds conj(L) (sliced conjugated)
 static int split_hns_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int n, int npad, int Kc,
                           const double2* Lop, const double2* Rop, double2* hs, int ld, int slices, cudaStream_t s,
-                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL = 0, int phase = 3) {
+                          int* nlaunch, HnsPipe* hp, const cudaEvent_t* ev, int cjL = 0, int phase = 3,
+                          int ovw = 0) {
   switch (slices) {
-    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
-    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase);
+    case 2: return split_gemm_launch<2>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 3: return split_gemm_launch<3>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 4: return split_gemm_launch<4>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 5: return split_gemm_launch<5>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 6: return split_gemm_launch<6>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 7: return split_gemm_launch<7>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
+    case 8: return split_gemm_launch<8>(c, k, set, n, npad, Kc, Lop, Rop, hs, ld, s, nlaunch, hp, ev, cjL, phase, ovw);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }
