@@ -1614,11 +1614,13 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
     CK(cudaGetLastError());
     // Y = R^H (G c): K x 4nb (rows of R beyond n unused); Yc = CLM^H (G c)
-    // over the LO rows; Z = T (Y; Yc) per atom.  Split precision: Y as int8
-    // slice products over the n rows, from k-major copies conj(R)^T, (G c)^T
+    // over the LO rows; Z = T (Y; Yc) per atom.  Split precision: Y and Yc
+    // as int8 slice products, from k-major copies conj(R)^T, conj(CLM)^T
+    // and (G c)^T
+    double2* Gt = nullptr;
     if (split_rho) {
       double2* Lt = (double2*)c->buf("frc_rt", sizeof(double2) * (size_t)n * K);
-      double2* Gt = (double2*)c->buf("frc_gt", sizeof(double2) * (size_t)n * 4 * nb);
+      Gt = (double2*)c->buf("frc_gt", sizeof(double2) * (size_t)n * 4 * nb);
       if (!Lt || !Gt) return LAPW1GPU_ERR_NOMEM;
       k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
       k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
@@ -1635,9 +1637,19 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       Yc = (double2*)c->buf("frc_yc", sizeof(double2) * (size_t)4 * nb * Kc);
       Zc = (double2*)c->buf("frc_zc", sizeof(double2) * (size_t)4 * nb * Kc);
       if (!Yc || !Zc) return LAPW1GPU_ERR_NOMEM;
-      if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
-                      (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc, Kc) != CUBLAS_STATUS_SUCCESS)
+      if (split_rho) {  // the LO rows of (G c)^T follow its PW rows in Gt
+        double2* Lc = (double2*)c->buf("frc_lc", sizeof(double2) * (size_t)nlo * Kc);
+        if (!Lc) return LAPW1GPU_ERR_NOMEM;
+        k_force_trans<<<dim3((nlo + 31) / 32, (Kc + 31) / 32), 256, 0, s>>>(Clo, nlo, Kc, nlo, 1, Lc, Kc);
+        int nly = 0;
+        rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices, s,
+                             &nly, 1);
+        if (rc) return rc;
+      } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
+                             (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc,
+                             Kc) != CUBLAS_STATUS_SUCCESS) {
         return LAPW1GPU_ERR_CUDA;
+      }
     }
     if (!c->smem((const void*)k_force_hns_z, FRC_ZSMEM)) return LAPW1GPU_ERR_CUDA;
     const dim3 zgrid((4 * nb + FRC_ZCOLS - 1) / FRC_ZCOLS, ndf);
