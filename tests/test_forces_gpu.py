@@ -148,3 +148,16 @@ def test_horb_problems_are_rejected(ctx):
         FO.gradient(ctx, kp, X, occ, eps)
     kp.free()
     assert ei.value.code == 1
+
+
+@pytest.mark.gpu
+def test_forces_timing_entry_point(ctx, monkeypatch, capsys):
+    """`python -m hack_wein2k_b200.forces` on the one-atom c0 case prints one
+    JSON line with finite timings and a finite gradient."""
+    import json
+    import sys
+    monkeypatch.setattr(sys, "argv", ["forces", "--case", "c0", "--bands", "4", "--repeat", "2"])
+    FO._main()
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["case"] == "c0" and len(out["forces_ms"]) == 2
+    assert all(np.isfinite(out["forces_ms"])) and np.isfinite(out["max_abs_grad"])
