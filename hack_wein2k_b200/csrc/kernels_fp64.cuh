@@ -986,7 +986,7 @@ __global__ void k_horb_pairs(DevProb P, int a, int lvor, const double2* __restri
   }
 }
 
-// non-finite scan of the n x n block and hsdiag
+// non-finite scan of the n x n block and hsdiag (hsdiag may be null)
 __global__ void k_check_finite(int n, const double2* __restrict__ hs, int ld, const double2* __restrict__ hsdiag,
                                int* status) {
   // a component is non-finite when its exponent bits are all ones
@@ -999,7 +999,7 @@ __global__ void k_check_finite(int n, const double2* __restrict__ hs, int ld, co
       bad |= ((unsigned)(__double_as_longlong(v.y) >> 52) & 0x7ffu) == 0x7ffu;
     }
   }
-  if (blockIdx.x == 0)
+  if (blockIdx.x == 0 && hsdiag)
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const double2 d = hsdiag[i];
       bad |= ((unsigned)(__double_as_longlong(d.x) >> 52) & 0x7ffu) == 0x7ffu;

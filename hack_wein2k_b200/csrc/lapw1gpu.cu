@@ -56,8 +56,11 @@ struct lapw1gpu_context {
   int nsm = 148;  // streaming multiprocessors (persistent grids)
   cudaStream_t stream = nullptr;
   cudaStream_t side[L1G_MAX_SETS] = {};  // streams of scratch sets 1.. in a batch
-  cudaEvent_t ev[16] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels
+  cudaEvent_t ev[22] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels,
+                            // 16-21 k_albl, k_table, the spherical slicers
   cudaEvent_t fork = nullptr, join[L1G_MAX_SETS] = {};
+  cudaEvent_t fev[6] = {};  // the last forces call: start, density matrices, k_force_sph, LO columns, end
+  float fms[5] = {};        // its intervals (ms), read by lapw1gpu_forces_stats
   // per scratch set: the stream that prepares the split HNS operands while
   // the spherical stage runs, and its fork/join events
   cudaStream_t aux[L1G_MAX_SETS] = {};
@@ -75,6 +78,8 @@ struct lapw1gpu_context {
   int split_group = 16;    // split HNS: row tiles per rasterisation group
   int sph_tc = 1;          // split precision: spherical part on tcgen05 (1) or FP64 (0)
   int batch_sets = 2;      // concurrent k-point chains in a batch
+  int test_never_wait = 0; // test hook: the spherical tensor kernel's consumer wait runs out
+  int last_launches = 0;   // kernels launched by the last call (a library product counts as one)
   std::map<std::string, DevBuf> bufs;
   std::map<std::string, std::pair<int2*, int>> tiles;  // tile lists per shape (kp_tiles)
   struct Graph {
@@ -84,6 +89,7 @@ struct lapw1gpu_context {
   };
   std::vector<Graph> graphs;  // captured batches
   std::map<const void*, int> smem_attr;  // kernels whose dynamic shared memory limit is raised
+  std::vector<void*> host_pinned;        // caller buffers page-locked by lapw1gpu_host_register
 
   // raise a kernel's dynamic shared-memory limit once per context (not a
   // stream operation, and kept out of captured sequences)
@@ -279,6 +285,7 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
     return LAPW1GPU_ERR_CUDA;
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  for (auto& e : c->fev) cudaEventCreate(&e);
   cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
   for (auto& e : c->hns_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : c->sph_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -305,6 +312,7 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   if (!c) return LAPW1GPU_ERR_ARG;
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
+  for (void* h : c->host_pinned) cudaHostUnregister(h);
   c->drop_graphs();
   for (auto& h : c->blas)
     if (h) cublasDestroy(h);
@@ -313,6 +321,7 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   for (auto& kv : c->tiles) cudaFree(kv.second.first);
   if (c->d_status) cudaFree(c->d_status);
   for (auto& e : c->ev) cudaEventDestroy(e);
+  for (auto& e : c->fev) cudaEventDestroy(e);
   cudaEventDestroy(c->fork);
   for (auto& e : c->hns_ev) cudaEventDestroy(e);
   for (auto& e : c->sph_ev) cudaEventDestroy(e);
@@ -349,6 +358,54 @@ int lapw1gpu_set_slices(lapw1gpu_context* c, int slices_sph, int slices_hns) {
 }
 
 void* lapw1gpu_stream(lapw1gpu_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int lapw1gpu_last_launches(lapw1gpu_context* c) { return c ? c->last_launches : 0; }
+
+int lapw1gpu_forces_stats(lapw1gpu_context* c, lapw1gpu_stats* st) {
+  if (!c || !st) return LAPW1GPU_ERR_ARG;
+  memset(st, 0, sizeof(*st));
+  st->ms_albl = c->fms[0];      // operands and the density matrices
+  st->ms_spherical = c->fms[1] + c->fms[2];
+  st->ms_sph_main = c->fms[2];  // k_force_sph
+  st->ms_lo = c->fms[3];        // the step-function sums and the LO columns
+  st->ms_hns = c->fms[4];       // the HNS part
+  st->ms_total = c->fms[0] + c->fms[1] + c->fms[2] + c->fms[3] + c->fms[4];
+  st->kernel_launches = c->last_launches;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_host_register(lapw1gpu_context* c, void* ptr, size_t bytes) {
+  if (!c || !ptr || bytes == 0) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  if (std::find(c->host_pinned.begin(), c->host_pinned.end(), ptr) != c->host_pinned.end()) return LAPW1GPU_OK;
+  const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {  // the caller pinned it already: nothing to undo later
+    cudaGetLastError();
+    return LAPW1GPU_OK;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? LAPW1GPU_ERR_NOMEM : LAPW1GPU_ERR_CUDA;
+  }
+  c->host_pinned.push_back(ptr);
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_host_unregister(lapw1gpu_context* c, void* ptr) {
+  if (!c || !ptr) return LAPW1GPU_ERR_ARG;
+  auto it = std::find(c->host_pinned.begin(), c->host_pinned.end(), ptr);
+  if (it == c->host_pinned.end()) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  c->host_pinned.erase(it);
+  CK(cudaHostUnregister(ptr));
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_test_wait_timeout(lapw1gpu_context* c, int on) {
+  if (!c || (on != 0 && on != 1)) return LAPW1GPU_ERR_ARG;
+  c->test_never_wait = on;
+  return LAPW1GPU_OK;
+}
 
 int lapw1gpu_last_status(lapw1gpu_context* c) {
   if (!c) return 0;
@@ -744,9 +801,11 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   const int sl_smem = Kc * 33 * (int)sizeof(double2);
   if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
   if (!c->smem((const void*)sphtc::k_sph_slice<S>, sl_smem)) return LAPW1GPU_ERR_CUDA;
+  if (ev && cudaEventRecord(c->ev[20], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   sphtc::k_sph_slice<S><<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, A, exA, c->d_status);
   sphtc::k_sph_slice<S><<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, B, exB,
                                                                            c->d_status);
+  if (ev && cudaEventRecord(c->ev[21], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   *nl += 2;
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, 64) ||
@@ -784,7 +843,7 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
       const int grid = (int)std::min<long>(t1 - t0, c->nsm);
       sphtc::k_sph_tc<S, LS><<<grid, Cf::THREADS, Cf::SMEM, s>>>(
           ta, tb, P, dt + t0, (int)(t1 - t0), (Kp + 63) / 64, (Kp % 64) != 0, npA, npB, exA, exB, tab, k->tab, hs,
-          ld, hsdiag, c->d_status);
+          ld, hsdiag, c->d_status, c->test_never_wait);
       *nl += 1;
     }
     if (sp && sp->col[g + 1] <= k->nv) {
@@ -858,15 +917,17 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
   P.phase = (double2*)c->sbuf(set, "phase", sizeof(double2) * (size_t)ndf * k->npad);
   if (!P.al || !P.bl || !P.phase) return LAPW1GPU_ERR_NOMEM;
   if (ev) {
-    // main-kernel events start equal, so a stage that does not run reads 0
-    for (int q = 12; q < 16; q++) CK(cudaEventRecord(ev[q], s));
+    // kernel events start equal, so a kernel that does not run reads 0
+    for (int q = 12; q < 22; q++) CK(cudaEventRecord(ev[q], s));
     CK(cudaEventRecord(ev[0], s));
   }
   int nl = 0;  // kernels launched by this run
 
   // ---- K-a: matching coefficients and phases (always needed) ----
   nl++;
+  if (ev) CK(cudaEventRecord(ev[16], s));
   k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
+  if (ev) CK(cudaEventRecord(ev[17], s));
   nl++;
   k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
   CK(cudaGetLastError());
@@ -914,7 +975,9 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     SphCoef* coef = (SphCoef*)c->sbuf(set, "coef", sizeof(SphCoef) * nat * ltop);
     if (!tab || !coef) return LAPW1GPU_ERR_NOMEM;
     nl++;
+    if (ev) CK(cudaEventRecord(ev[18], s));
     k_table<<<(unsigned)((ntab + 127) / 128), 128, 0, s>>>(P, k->tab, k->d_warp, tab);
+    if (ev) CK(cudaEventRecord(ev[19], s));
     nl++;
     k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
     // column groups of the spherical contraction (the caller's boundaries)
@@ -1066,6 +1129,10 @@ static void fill_stats(lapw1gpu_context* c, const lapw1gpu_kpoint* k, int nl, la
     st->ms_sph_main = a;
   if (cudaEventQuery(c->ev[15]) == cudaSuccess && cudaEventElapsedTime(&b, c->ev[14], c->ev[15]) == cudaSuccess)
     st->ms_hns_main = b;
+  float ka = 0.f, kt = 0.f, ks = 0.f;
+  if (cudaEventElapsedTime(&ka, c->ev[16], c->ev[17]) == cudaSuccess) st->ms_k_albl = ka;
+  if (cudaEventElapsedTime(&kt, c->ev[18], c->ev[19]) == cudaSuccess) st->ms_table = kt;
+  if (cudaEventElapsedTime(&ks, c->ev[20], c->ev[21]) == cudaSuccess) st->ms_sph_slice = ks;
   cudaGetLastError();
 }
 
@@ -1081,6 +1148,7 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
   int rc = kpoint_run_impl(c, k, stages, reinterpret_cast<double2*>(d_hs_), ldhs, reinterpret_cast<double2*>(d_hsdiag_),
                            s, 0, st ? c->ev : nullptr, &nl);
   if (rc) return rc;
+  c->last_launches = nl;
   c->status_pending = !st;
   if (st) {
     int hstat = 0;
@@ -1125,7 +1193,8 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
   std::vector<uintptr_t> key = {(uintptr_t)nk,         (uintptr_t)stages,        (uintptr_t)c->prec,
                                 (uintptr_t)(c->slices * 16 + c->slices_hns), (uintptr_t)c->hns_diag_b,
                                 (uintptr_t)c->split_group,
-                                (uintptr_t)c->sph_tc,  (uintptr_t)c->batch_sets};
+                                (uintptr_t)c->sph_tc,  (uintptr_t)c->batch_sets,
+                                (uintptr_t)c->test_never_wait};
   for (int i = 0; i < nk; i++) {
     key.push_back((uintptr_t)kps[i]);
     key.push_back((uintptr_t)d_hs[i]);
@@ -1170,6 +1239,7 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
   CK(cudaStreamSynchronize(c->stream));
   c->last_status = hstat;
   c->status_pending = false;
+  c->last_launches = g->launches;
   if (st) {
     memset(st, 0, sizeof(*st));
     float tot = 0.f;
@@ -1348,6 +1418,7 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
     hp.sev[g] = c->sph_ev[g];
   }
   rc = kpoint_run_impl(c, k, stages, d_hs, n, d_hd, s, 0, c->ev, &nl, pipe ? &hp : nullptr);
+  c->last_launches = nl;
   if (rc == LAPW1GPU_OK) {
     CK(cudaEventRecord(e2, s));
     bool grouped = pipe && hp.groups > 0 && hp.col[hp.groups] == n;
@@ -1531,6 +1602,8 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   cublasHandle_t h = c->handle(0, s);
   if (!h) return LAPW1GPU_ERR_CUDA;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  int nlf = 0;  // kernels launched (a library product counts as one)
+  CK(cudaEventRecord(c->fev[0], s));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
   CK(cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * ndf, s));
   k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
@@ -1538,6 +1611,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
   const bool split_rho = c->prec == LAPW1GPU_PREC_SPLIT;
   k_force_weight<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, C, ldc, d_occ, d_eps, split_rho ? 1 : 0, Cf, Ce);
+  nlf += 4;  // k_albl, k_phase, k_sph_coef, k_force_weight
   CK(cudaGetLastError());
   // rho(J,I) = sum_b f_b c_b(J) conj(c_b(I)), column-major n x n, and rhoE:
   // Hermitian, and only J < I is read.  FP64: the library forms the upper
@@ -1561,6 +1635,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
     if (!rc) rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
     if (rc) return rc;
+    nlf += nlr;
     rt = 1;
   } else {
     const double rzero = 0.0;
@@ -1569,7 +1644,9 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
         cublasZherkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nb, &one, (const cuDoubleComplex*)Ce, n,
                      (const cuDoubleComplex*)C, ldc, &rzero, (cuDoubleComplex*)rhoe, n) != CUBLAS_STATUS_SUCCESS)
       return LAPW1GPU_ERR_CUDA;
+    nlf += 2;
   }
+  CK(cudaEventRecord(c->fev[1], s));
   int ntiles = 0;
   const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
@@ -1578,6 +1655,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   double2* rowI = (double2*)c->buf("frc_rowi", 2 * sizeof(double2) * nrow);
   if (!rowJ || !rowI) return LAPW1GPU_ERR_NOMEM;
   k_force_rows<<<dim3((k->nvpad + 127) / 128, nat * ltop), 128, 0, s>>>(P, coef, rowJ, rowI);
+  nlf += 3;  // k_force_rows, k_force_sph, k_force_step
   const bool lt11 = ltop == FRC_LT;
   const void* fsph = lt11 ? (const void*)k_force_sph<FRC_LT, false> : (const void*)k_force_sph<SPH_LMAX, true>;
   const int fsmem = frc_smem_bytes(lt11 ? FRC_LT : SPH_LMAX);
@@ -1586,15 +1664,21 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   double* bins = (double*)c->buf("frc_bins", sizeof(double) * 2 * nbox);
   if (!bins) return LAPW1GPU_ERR_NOMEM;
   CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
+  CK(cudaEventRecord(c->fev[2], s));
   if (lt11)
     k_force_sph<FRC_LT, false><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
                                                                   d_grad, bins);
   else
     k_force_sph<SPH_LMAX, true><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
                                                                    d_grad, bins);
+  CK(cudaEventRecord(c->fev[3], s));
   k_force_step<<<ndf, 256, 0, s>>>(P, k->tab, bins, d_grad);
   CK(cudaGetLastError());
-  if (nlo > 0) k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, rt, d_grad);
+  if (nlo > 0) {
+    k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, rt, d_grad);
+    nlf++;
+  }
+  CK(cudaEventRecord(c->fev[4], s));
   CK(cudaGetLastError());
   if (!k->nohns) {
     const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
@@ -1612,6 +1696,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
                             &nl);
     if (rc) return rc;
     k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
+    nlf += nl + 1;
     CK(cudaGetLastError());
     // Y = R^H (G c): K x 4nb (rows of R beyond n unused); Yc = CLM^H (G c)
     // over the LO rows; Z = T (Y; Yc) per atom.  Split precision: Y and Yc
@@ -1627,9 +1712,12 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       int nly = 0;
       rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices, s, &nly, 1);
       if (rc) return rc;
+      nlf += nly + 2;
     } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
                            (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS) {
       return LAPW1GPU_ERR_CUDA;
+    } else {
+      nlf++;
     }
     double2* Yc = nullptr;
     double2* Zc = nullptr;
@@ -1645,28 +1733,37 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
         rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices, s,
                              &nly, 1);
         if (rc) return rc;
+        nlf += nly + 1;
       } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, Kc, 4 * nb, nlo, &one, (const cuDoubleComplex*)Clo, nlo,
                              (const cuDoubleComplex*)(GC + nv), n, &zero, (cuDoubleComplex*)Yc,
                              Kc) != CUBLAS_STATUS_SUCCESS) {
         return LAPW1GPU_ERR_CUDA;
+      } else {
+        nlf++;
       }
     }
     if (!c->smem((const void*)k_force_hns_z, FRC_ZSMEM)) return LAPW1GPU_ERR_CUDA;
     const dim3 zgrid((4 * nb + FRC_ZCOLS - 1) / FRC_ZCOLS, ndf);
     k_force_hns_z<<<zgrid, 256, FRC_ZSMEM, s>>>(0, nsl2, K, Kc, 4 * nb, P.atype, k->d_tns, Y, Yc, Z, nullptr);
     k_force_hns_reduce<<<ndf, 256, 0, s>>>(2 * nsl2, K, nb, Y, Z, d_occ, d_grad);
+    nlf += 2;
     CK(cudaGetLastError());
     if (nlo > 0) {
       k_force_hns_z<<<zgrid, 256, FRC_ZSMEM, s>>>(1, nsl2, K, Kc, 4 * nb, P.atype, k->d_tns, Y, Yc, nullptr, Zc);
       k_force_hns_reduce<<<ndf, 256, 0, s>>>(nsl2, Kc, nb, Yc, Zc, d_occ, d_grad);
+      nlf += 2;
       CK(cudaGetLastError());
     }
   }
+  CK(cudaEventRecord(c->fev[5], s));
   int hstat = 0;
   CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   c->last_status = hstat;
   c->status_pending = false;
+  c->last_launches = nlf;
+  for (int q = 0; q < 5; q++) cudaEventElapsedTime(&c->fms[q], c->fev[q], c->fev[q + 1]);
+  cudaGetLastError();
   return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
 }
 
@@ -1712,11 +1809,26 @@ __global__ void k_noalloc_tables(int nat, const int* __restrict__ mult, const in
     for (int bj = 0; bj <= bi; bj++) tiles[t++] = make_int2(bi, bj);
 }
 
-extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, int ldhs, void* stream) {
+// true when SPHBES would refuse an argument RMT |k+G| of this problem's
+// plane-wave rows (the check k_albl makes on the device, made here on the
+// host because this entry point returns before its kernels run)
+static bool sphbes_out_of_range(const lapw1gpu_problem* p) {
+  for (int jn = 0; jn < p->nat; jn++)
+    for (int i = 0; i < p->nv; i++)
+      if (l1g_sphbes_refuses(p->ltop - 1, p->rmt[jn] * p->rk[i])) return true;
+  return false;
+}
+
+extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, int ldhs, void* stream,
+                                    int* d_status_out) {
   int rc = validate(p);
   if (rc) return rc;
   if (!d_hs_ || ldhs < p->n) return LAPW1GPU_ERR_ARG;
-  if (p->nohns) return LAPW1GPU_OK;  // calkpt.F:169: nothing to add
+  if (sphbes_out_of_range(p)) return LAPW1GPU_ERR_RANGE;  // as the HNS stage reports it
+  if (p->nohns) {  // calkpt.F:169: nothing to add
+    if (d_status_out) CK(cudaMemsetAsync(d_status_out, 0, sizeof(int), (cudaStream_t)stream));
+    return LAPW1GPU_OK;
+  }
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= L1G_NOALLOC_MAXDEV) return LAPW1GPU_ERR_RANGE;
@@ -1822,6 +1934,7 @@ extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, in
   double2* C2lo = (double2*)take(sizeof(double2) * nloc);
   int* d_status = (int*)take(sizeof(int));
   if (!fits) return LAPW1GPU_ERR_RANGE;  // beyond L1G_NOALLOC_BYTES
+  if (d_status_out) d_status = d_status_out;  // the caller reads the bits after the stream
 
   for (int q = 0; q < npend; q++)
     if (pend[q].src && pend[q].bytes)
@@ -1837,6 +1950,9 @@ extern "C" int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs_, in
   k_hns_gemm<<<(unsigned)ntiles, 256, 0, s>>>(n, npad, K, d_tiles, Lop, Rop, d_hs, ldhs);
   if (p->nlo > 0)
     k_hns_lo<<<dim3((p->nlo + 127) / 128, p->nlo), 128, 0, s>>>(nv, p->nlo, ndf * nsl2, C2lo, Clo, d_hs, ldhs);
+  // a non-finite element of the updated HS sets L1G_STATUS_NONFINITE, as
+  // the HNS stage of the allocating entry points reports it
+  if (d_status_out) k_check_finite<<<1184, 256, 0, s>>>(n, d_hs, ldhs, nullptr, d_status);
   CK(cudaGetLastError());
   return LAPW1GPU_OK;
 }

@@ -259,12 +259,13 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
     k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
              const int2* __restrict__ tiles, int ntile, int nkb, int khalf, int npA, int npB,
              const int* __restrict__ exA, const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T,
-             double2* __restrict__ hs, int ld, double2* __restrict__ hsdiag, int* __restrict__ status) {
+             double2* __restrict__ hs, int ld, double2* __restrict__ hsdiag, int* __restrict__ status,
+             int never_wait) {
   using C = Cfg<S>;
   constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = C::IPT, EPI = C::EPI;
   constexpr int MMA_WARP = 4 * C::EG, TMA_WARP = 4 * C::EG + 1;
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar, ebar;
+  __shared__ uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], accbar, ebar, never;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -289,6 +290,7 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
     }
     mbar_init(&accbar, 1);
     mbar_init(&ebar, EPI);  // the epilogue threads' barrier (bounded waits)
+    mbar_init(&never, 1);   // nothing arrives here (the never_wait test hook)
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -340,6 +342,17 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
       long g = 0;   // pipeline iterations over all tiles
       long gl = 0;  // accumulations (tile, l) over all tiles
       bool ok = true;
+      if (never_wait) {
+        // test hook: the consumer waits on a barrier that nothing arrives
+        // at, with a short bound (about half a millisecond), and takes the
+        // timeout path below (the other roles' waits keep their full bound)
+        const long long t0 = clock64();
+        while (!mbar_try_wait(&never, 0))
+          if (clock64() - t0 > (1LL << 20)) {
+            ok = false;
+            break;
+          }
+      }
       for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
         for (int it = 0; it < nit; it++, g++) {
           const int st = (int)(g % STAGES), kb = it % nkb, buf = (int)(gl & 1);

@@ -33,7 +33,8 @@ EXPORTS = [
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
-    "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices",
+    "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices", "lapw1gpu_test_wait_timeout",
+    "lapw1gpu_last_launches", "lapw1gpu_host_register", "lapw1gpu_host_unregister", "lapw1gpu_forces_stats",
 ]
 
 _lib = None
@@ -81,13 +82,18 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_version.restype = C.c_char_p
     lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
                                             dp, dp, dp, ip, dp]
-    lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p]
+    lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.lapw1gpu_forces.argtypes = [vp, vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lapw1gpu_setup_batch.argtypes = [vp, C.POINTER(vp), C.c_int, C.c_int, C.POINTER(C.c_void_p),
                                          C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(CStats)]
     lib.lapw1gpu_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
     lib.lapw1gpu_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
     lib.lapw1gpu_autotune.argtypes = [vp, vp, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(Tuning)]
+    lib.lapw1gpu_test_wait_timeout.argtypes = [vp, C.c_int]
+    lib.lapw1gpu_last_launches.argtypes = [vp]
+    lib.lapw1gpu_forces_stats.argtypes = [vp, C.POINTER(CStats)]
+    lib.lapw1gpu_host_register.argtypes = [vp, C.c_void_p, C.c_size_t]
+    lib.lapw1gpu_host_unregister.argtypes = [vp, C.c_void_p]
     _lib = lib
     return lib
 
@@ -165,6 +171,29 @@ class Context:
     def last_status(self) -> int:
         return int(self.lib.lapw1gpu_last_status(self.h))
 
+    def host_register(self, arr: np.ndarray) -> None:
+        """page-lock a host array for the context's lifetime (lapw1gpu_host_register)"""
+        _check("lapw1gpu_host_register", self.lib.lapw1gpu_host_register(self.h, C.c_void_p(arr.ctypes.data),
+                                                                         arr.nbytes))
+
+    def host_unregister(self, arr: np.ndarray) -> None:
+        _check("lapw1gpu_host_unregister", self.lib.lapw1gpu_host_unregister(self.h, C.c_void_p(arr.ctypes.data)))
+
+    def forces_stats(self) -> dict:
+        """device times of the last forces call (lapw1gpu_forces_stats)"""
+        st = CStats()
+        _check("lapw1gpu_forces_stats", self.lib.lapw1gpu_forces_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def last_launches(self) -> int:
+        """kernels the last setup, batch or forces call launched"""
+        return int(self.lib.lapw1gpu_last_launches(self.h))
+
+    def test_wait_timeout(self, on: bool) -> None:
+        """Test hook (lapw1gpu_test_wait_timeout): make the spherical tensor
+        kernel's consumer wait run out on later split-precision runs."""
+        _check("lapw1gpu_test_wait_timeout", self.lib.lapw1gpu_test_wait_timeout(self.h, 1 if on else 0))
+
     def setup(self, prob: Problem, stages: int = 7, hs: Optional[np.ndarray] = None,
               hsdiag: Optional[np.ndarray] = None, stats: bool = False):
         """calkpt.F:153-185 on host buffers.  Returns (HS, HSDIAG[, stats]);
@@ -235,12 +264,15 @@ def version() -> str:
     return load().lapw1gpu_version().decode()
 
 
-def hns_noalloc(prob: Problem, d_hs_ptr: int, ldhs: int, stream: int = 0) -> None:
+def hns_noalloc(prob: Problem, d_hs_ptr: int, ldhs: int, stream: int = 0, d_status_ptr: int = 0) -> None:
     """lapw1gpu_hns_noalloc: add the HNS update into a caller-owned device
-    HS without any allocation by the library (see include/lapw1gpu.h)."""
+    HS without any allocation by the library (see include/lapw1gpu.h).
+    d_status_ptr (optional): a device int that receives the call's status
+    bits once the stream has run the call."""
     cp = prob.to_c()
     _check("lapw1gpu_hns_noalloc",
-           load().lapw1gpu_hns_noalloc(C.byref(cp), C.c_void_p(d_hs_ptr), ldhs, C.c_void_p(stream)))
+           load().lapw1gpu_hns_noalloc(C.byref(cp), C.c_void_p(d_hs_ptr), ldhs, C.c_void_p(stream),
+                                       C.c_void_p(d_status_ptr) if d_status_ptr else None))
 
 
 def tns_from_gaunt(nat, lnsmax, lqind, lqns, gfac, vns1, vns2, vns3, vnslo1, vnslo2, vnslo3, loor):

@@ -253,33 +253,37 @@ def wedge_kpoints(rng, nk):
     return out
 
 
-def config(name: str, nk: int | None = None) -> List[Problem]:
-    """Workloads c0..c4 (see module docstring) and small test cases."""
+def config(name: str, nk: int | None = None, kofs: int = 0) -> List[Problem]:
+    """Workloads c0..c4 (see module docstring) and small test cases.
+
+    For the k-point lists (c2, c4) the k-points come from their own seeded
+    stream, apart from the crystal's draws: k-points kofs .. kofs+nk-1 of
+    that stream, on the same crystal for every kofs (a k-point shard of one
+    run, as lapw1para splits a k-list)."""
     if name == "c0":
         rng = np.random.default_rng(1000)
         return [synth_problem(cell_fcc1(), 7.0, (0.1, 0.2, 0.3), rng=rng, name="c0")]
-    if name in ("c1", "c2"):
-        idx = 1 if name == "c1" else 2
+    if name == "c1":
+        rng = np.random.default_rng(1001)
+        return [synth_problem(cell_abo3_222(), 7.0, wedge_kpoints(rng, 1)[0], lo_l=(0, 1, 2), rng=rng, name="c1k0")]
+    if name == "c3":
+        rng = np.random.default_rng(1003)
+        k = rng.uniform(0.0, 0.5, size=3)
+        return [synth_problem(cell_random100(), 6.0, k, lo_l=(0, 1, 2), rng=rng, name="c3k0")]
+    if name in ("c2", "c4"):
+        idx = 2 if name == "c2" else 4
         rng = np.random.default_rng(1000 + idx)
-        cell = cell_abo3_222()
-        nkk = 1 if name == "c1" else (nk or 64)
-        ks = wedge_kpoints(rng, nkk)
+        rng_k = np.random.default_rng([1000 + idx, 1])
+        nkk = nk or (64 if name == "c2" else 16)
+        if name == "c2":
+            cell, rkmax = cell_abo3_222(), 7.0
+            ks = wedge_kpoints(rng_k, kofs + nkk)[kofs:]
+        else:
+            cell, rkmax = cell_random100(), 8.0
+            ks = [rng_k.uniform(0.0, 0.5, size=3) for _ in range(kofs + nkk)][kofs:]
         out, params = [], None
         for i, k in enumerate(ks):
-            pr = synth_problem(cell, 7.0, k, lo_l=(0, 1, 2), rng=rng, params=params, name=f"{name}k{i}")
-            params = pr._params
-            out.append(pr)
-        return out
-    if name in ("c3", "c4"):
-        idx = 3 if name == "c3" else 4
-        rng = np.random.default_rng(1000 + idx)
-        cell = cell_random100()
-        rk = 6.0 if name == "c3" else 8.0
-        nkk = 1 if name == "c3" else (nk or 16)
-        ks = [rng.uniform(0.0, 0.5, size=3) for _ in range(nkk)]
-        out, params = [], None
-        for i, k in enumerate(ks):
-            pr = synth_problem(cell, rk, k, lo_l=(0, 1, 2), rng=rng, params=params, name=f"{name}k{i}")
+            pr = synth_problem(cell, rkmax, k, lo_l=(0, 1, 2), rng=rng, params=params, name=f"{name}k{kofs + i}")
             params = pr._params
             out.append(pr)
         return out

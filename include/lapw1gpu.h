@@ -31,6 +31,8 @@
 #ifndef LAPW1GPU_H
 #define LAPW1GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -154,6 +156,10 @@ typedef struct lapw1gpu_stats {
                            or k_sph_tc), inside ms_spherical               */
   double ms_hns_main;   /* the HNS update alone (k_hns_gemm + ZGEMM panels, or
                            the tcgen05 slice products), inside ms_hns      */
+  double ms_k_albl;     /* K-a: the matching-coefficient kernel k_albl alone  */
+  double ms_table;      /* K-c: the Theta/WARP table kernel k_table alone     */
+  double ms_sph_slice;  /* K-a, split path: the two spherical operand slicers
+                           (phases x AL/BL cut into int8 slices)             */
 } lapw1gpu_stats;
 
 typedef struct lapw1gpu_context lapw1gpu_context;
@@ -205,6 +211,30 @@ int lapw1gpu_setup_stages(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
  * own work after an asynchronous lapw1gpu_kpoint_run */
 void* lapw1gpu_stream(lapw1gpu_context* ctx);
 
+/* Test hook of the bounded device waits.  No counterpart in the reference.
+ * With on = 1, later runs of the split-precision spherical tensor-core
+ * kernel make its MMA issuer wait on a barrier that nothing arrives at,
+ * bounded to about half a millisecond: the kernel takes its timeout path
+ * (status bit, copies in flight drained, TMEM freed) and the run returns
+ * LAPW1GPU_ERR_TIMEOUT with the context still usable.  on = 0 (the
+ * default) restores normal runs. */
+int lapw1gpu_test_wait_timeout(lapw1gpu_context* ctx, int on);
+
+/* Page-lock a caller buffer (typically HS, allocated once by INIT_MATRICES,
+ * modules.F:526-535) for the context's lifetime, so that the host entry
+ * points copy HS at full link speed and overlap those copies with the later
+ * stages; without it the copies into pageable memory are staged by the
+ * driver and serialise.  A buffer already page-locked by the caller is
+ * accepted as is.  lapw1gpu_finalize (or lapw1gpu_host_unregister) undoes
+ * it; the caller must not free the buffer before then.  No counterpart in
+ * the reference. */
+int lapw1gpu_host_register(lapw1gpu_context* ctx, void* ptr, size_t bytes);
+int lapw1gpu_host_unregister(lapw1gpu_context* ctx, void* ptr);
+
+/* kernels launched by the last setup, batch or forces call on the context
+ * (a library product counts as one launch); no counterpart in the reference */
+int lapw1gpu_last_launches(lapw1gpu_context* ctx);
+
 /* device status word of the last run (L1G_STATUS_* bits), 0 if clean; after
  * an asynchronous lapw1gpu_kpoint_run it waits for that run first */
 int lapw1gpu_last_status(lapw1gpu_context* ctx);
@@ -238,11 +268,21 @@ int lapw1gpu_tns_from_gaunt(int nat, int lnsmax, int ngau, int lmmx,
  * (a cudaStream_t, NULL for the default stream), asynchronously.  All of its
  * intermediate buffers live in one 64 MiB device array inside the library
  * (held by every GPU that loads the library until the process exits);
- * problems needing more return LAPW1GPU_ERR_RANGE.  The first call on a
- * device looks up that array's device address: make it before any stream
- * capture.  Calls share the array, so calls that overlap on the GPU race. */
+ * problems needing more return LAPW1GPU_ERR_RANGE, and so do problems whose
+ * RMT |k+G| lies beyond SPHBES's range (checked on the host, before any
+ * device work, as the HNS stage reports it).  The problem's host arrays are
+ * copied with cudaMemcpyAsync on `stream`.
+ * d_status (optional, device int, NULL to skip): cleared on `stream`, then
+ * given the L1G status bits of the call once the stream reaches its end
+ * (2: a non-finite element in the updated HS; 0 clean).  Reading it after
+ * the stream is the caller's way to learn what the HNS stage reports as
+ * LAPW1GPU_ERR_NONFINITE.
+ * The first call on a device looks up that array's device address and keeps
+ * it for the process: make it before any stream capture, and make no call
+ * on a device after cudaDeviceReset there.  Calls share the array, so calls
+ * that overlap on the GPU race. */
 int lapw1gpu_hns_noalloc(const lapw1gpu_problem* p, double* d_hs, int ldhs,
-                         void* stream);
+                         void* stream, int* d_status);
 
 /* A k-point batch (a lapw1 k-list, lapw1.F:50-67 calls CALKPT per k) set
  * up in one launch: the stage sequences of all nk uploaded k-points are
@@ -289,6 +329,14 @@ int lapw1gpu_autotune(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp, double* d_hs,
 int lapw1gpu_forces(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp,
                     const double* d_c, int ldc, int nb, const double* d_occ,
                     const double* d_eps, double* d_grad);
+
+/* Device times of the last lapw1gpu_forces call on the context, in the
+ * fields of lapw1gpu_stats: ms_total the whole call, ms_albl the operands
+ * and the density matrices, ms_spherical the plane-wave pair sums with
+ * ms_sph_main the pair kernel k_force_sph alone, ms_lo the step-function
+ * sums and the local-orbital columns, ms_hns the non-spherical part,
+ * kernel_launches its launches.  No counterpart in the reference. */
+int lapw1gpu_forces_stats(lapw1gpu_context* ctx, lapw1gpu_stats* st);
 
 /* version string of the library */
 const char* lapw1gpu_version(void);

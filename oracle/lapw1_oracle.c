@@ -30,6 +30,7 @@
  * macros, so each line can be read against the Fortran.
  */
 #include <complex.h>
+#include <dlfcn.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -707,9 +708,29 @@ static void lohns(const lapw1gpu_problem* p, int jneq, int l0, int jlo, int* i1,
   *i2 = I2 - 1;
 }
 
+/* Optional BLAS for the timed CPU baseline: a CBLAS zgemm loaded at run
+   time (OpenBLAS), as the reference links MKL for ZHER2M's ZGEMMs.  The
+   parity checks leave it unset and use the plain loops below. */
+typedef void (*cblas_zgemm_fn)(int order, int ta, int tb, int m, int n, int k, const void* alpha, const void* a,
+                               int lda, const void* b, int ldb, const void* beta, void* c, int ldc);
+static cblas_zgemm_fn g_zgemm = NULL;
+
+/* Load `symbol` (a cblas_zgemm) from the shared library at `path`; NULL
+   path switches BLAS off again.  Returns 0 on success. */
+int oracle_use_blas(const char* path, const char* symbol) {
+  if (!path) {
+    g_zgemm = NULL;
+    return 0;
+  }
+  void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  if (!h) return 1;
+  g_zgemm = (cblas_zgemm_fn)dlsym(h, symbol ? symbol : "cblas_zgemm");
+  return g_zgemm ? 0 : 2;
+}
+
 /* lower-triangle update C(i,j) += sum_k A(i,k) B(j,k), i >= j, rows r0..r1
    (1-based, inclusive): the 'L','N','T' case of zher2m.f:69-80 */
-static void zher2m_lnt(int r0, int r1, int kdim, const zc* A, const zc* B, int lda, double* hs, int ldhs) {
+static void zher2m_lnt_block(int r0, int r1, int kdim, const zc* A, const zc* B, int lda, double* hs, int ldhs) {
 #pragma omp parallel for schedule(dynamic, 16)
   for (int i = r0; i <= r1; i++) {
     const zc* ai = A + (size_t)(i - 1) * lda;
@@ -721,6 +742,23 @@ static void zher2m_lnt(int r0, int r1, int kdim, const zc* A, const zc* B, int l
       hs[2 * o] += creal(s);
       hs[2 * o + 1] += cimag(s);
     }
+  }
+}
+static void zher2m_lnt(int r0, int r1, int kdim, const zc* A, const zc* B, int lda, double* hs, int ldhs) {
+  if (!g_zgemm) {
+    zher2m_lnt_block(r0, r1, kdim, A, B, lda, hs, ldhs);
+    return;
+  }
+  /* zher2m.f:69-80 with NBLOCK = 128: the diagonal blocks element by
+     element, the rows below each block by one ZGEMM (A and B are row-major
+     [row][lda], i.e. column-major K x rows: C = A^T B in column-major) */
+  const double one[2] = {1.0, 0.0};
+  for (int ii = r0; ii <= r1; ii += 128) {
+    const int imax = ii + 127 < r1 ? ii + 127 : r1;
+    zher2m_lnt_block(ii, imax, kdim, A, B, lda, hs, ldhs);
+    if (imax < r1)
+      g_zgemm(102 /* ColMajor */, 112 /* Trans */, 111 /* NoTrans */, r1 - imax, imax - ii + 1, kdim, one,
+              A + (size_t)imax * lda, lda, B + (size_t)(ii - 1) * lda, lda, one, hs + 2 * HS_IDX(imax + 1, ii), ldhs);
   }
 }
 

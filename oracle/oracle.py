@@ -23,22 +23,66 @@ def build(force: bool = False) -> str:
     return _SO
 
 
+_NATIVE_SO = os.path.join(_HERE, "liblapw1_oracle_native.so")
+_native = None
+
+
+def _bind(lib):
+    dp = C.POINTER(C.c_double)
+    lib.oracle_sphbes.argtypes = [C.c_int, C.c_double, dp]
+    lib.oracle_ylm.argtypes = [dp, C.c_int, dp]
+    lib.oracle_albl.argtypes = [C.c_void_p, dp, dp]
+    for f in ("oracle_setup", "oracle_hamilt"):
+        getattr(lib, f).argtypes = [C.c_void_p, dp, C.c_int, dp]
+    lib.oracle_hamilt_range.argtypes = [C.c_void_p, dp, C.c_int, dp, C.c_int, C.c_int, C.c_int]
+    lib.oracle_swapdiag.argtypes = [C.c_void_p, dp, C.c_int, dp]
+    lib.oracle_hns.argtypes = [C.c_void_p, dp, C.c_int]
+    lib.oracle_hns_range.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_int]
+    lib.oracle_horb.argtypes = [C.c_void_p, dp, C.c_int]
+    lib.oracle_use_blas.argtypes = [C.c_char_p, C.c_char_p]
+    return lib
+
+
+def openblas_path():
+    """The LP64 OpenBLAS that ships with scipy (its CBLAS symbols carry the
+    scipy_ prefix), or None."""
+    try:
+        import glob
+        import scipy
+        d = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs")
+        hits = sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so")))
+        return hits[0] if hits else None
+    except Exception:
+        return None
+
+
+def baseline_lib():
+    """The oracle built for the timed CPU baseline: -O3 -march=native on the
+    machine that runs it (the portable build if that compile fails), with
+    the ZHER2M blocks on OpenBLAS zgemm when scipy's OpenBLAS is found.
+    Returns (library, description)."""
+    global _native
+    if _native is None:
+        try:
+            subprocess.check_call(["make", "-s", "-C", _HERE, "native"], stdout=subprocess.DEVNULL,
+                                  stderr=subprocess.DEVNULL)
+            lib_, flags = _bind(C.CDLL(_NATIVE_SO)), "gcc -O3 -march=native -fopenmp"
+        except Exception:
+            lib_, flags = lib(), "gcc -O3 -march=x86-64-v3 -fopenmp"
+        blas = openblas_path()
+        if blas and lib_.oracle_use_blas(blas.encode(), b"scipy_cblas_zgemm") == 0:
+            flags += ", ZHER2M blocks on OpenBLAS zgemm (" + os.path.basename(blas) + ")"
+        else:
+            flags += ", ZHER2M as plain loops (no OpenBLAS found)"
+        _native = (lib_, flags)
+    return _native
+
+
 def lib():
     global _lib
     if _lib is None:
         build()
-        _lib = C.CDLL(_SO)
-        dp = C.POINTER(C.c_double)
-        _lib.oracle_sphbes.argtypes = [C.c_int, C.c_double, dp]
-        _lib.oracle_ylm.argtypes = [dp, C.c_int, dp]
-        _lib.oracle_albl.argtypes = [C.c_void_p, dp, dp]
-        for f in ("oracle_setup", "oracle_hamilt"):
-            getattr(_lib, f).argtypes = [C.c_void_p, dp, C.c_int, dp]
-        _lib.oracle_hamilt_range.argtypes = [C.c_void_p, dp, C.c_int, dp, C.c_int, C.c_int, C.c_int]
-        _lib.oracle_swapdiag.argtypes = [C.c_void_p, dp, C.c_int, dp]
-        _lib.oracle_hns.argtypes = [C.c_void_p, dp, C.c_int]
-        _lib.oracle_hns_range.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_int]
-        _lib.oracle_horb.argtypes = [C.c_void_p, dp, C.c_int]
+        _lib = _bind(C.CDLL(_SO))
     return _lib
 
 
@@ -97,24 +141,25 @@ def setup(prob, stages: int = 7):
     return hs, hsd
 
 
-def hamilt_sample(prob, col_lo: int, col_hi: int):
+def hamilt_sample(prob, col_lo: int, col_hi: int, L=None):
     """HAMILT over PW columns col_lo..col_hi only (a bounded CPU sample)."""
     cp = prob.to_c()
     n = prob.n
     hs = np.zeros((n, n), dtype=np.complex128, order="F")
     hsd = np.zeros(n, dtype=np.complex128)
-    rc = lib().oracle_hamilt_range(C.byref(cp), _dp(hs.reshape(-1, order="F").view(np.float64)), n,
+    rc = (L or lib()).oracle_hamilt_range(C.byref(cp), _dp(hs.reshape(-1, order="F").view(np.float64)), n,
                                    _dp(hsd.view(np.float64)), col_lo, col_hi, 0)
     if rc:
         raise RuntimeError("oracle_hamilt_range failed")
     return hs, hsd
 
 
-def hns_sample(prob, atom_lo: int, atom_hi: int):
+def hns_sample(prob, atom_lo: int, atom_hi: int, L=None):
+    """HNS over equivalent atoms atom_lo..atom_hi only (a bounded CPU sample)."""
     cp = prob.to_c()
     n = prob.n
     hs = np.zeros((n, n), dtype=np.complex128, order="F")
-    rc = lib().oracle_hns_range(C.byref(cp), _dp(hs.reshape(-1, order="F").view(np.float64)), n,
+    rc = (L or lib()).oracle_hns_range(C.byref(cp), _dp(hs.reshape(-1, order="F").view(np.float64)), n,
                                 atom_lo, atom_hi)
     if rc:
         raise RuntimeError("oracle_hns_range failed")

@@ -14,7 +14,7 @@ This script reads those text files once (in the build container, where the
 reference tree is mounted) and writes the extracted numbers; the tests use
 only the committed JSON.  Usage:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 """
 from __future__ import annotations
 
@@ -196,4 +196,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference tree root>")
+    main(sys.argv[1])

@@ -59,3 +59,19 @@ def test_problem_struct_layout_matches_header():
             if m:
                 names.append(m.group(1))
     assert names == [f for f, _ in CProblem._fields_]
+
+
+def test_hns_noalloc_range_check_runs_on_the_host():
+    """The allocation-free HNS entry point rejects an RMT |k+G| beyond
+    SPHBES's range before any device work: the check needs no GPU."""
+    import dataclasses
+
+    import numpy as np
+
+    from hack_wein2k_b200 import synth
+    p = synth.small_case("lo")
+    rmt = np.array(p.rmt, dtype=np.float64, copy=True)
+    rmt[0] = 25.0 / float(np.max(p.rk[: p.nv]))
+    with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
+        lapw1gpu.hns_noalloc(dataclasses.replace(p, rmt=rmt), 0x1000, p.n, 0)
+    assert e.value.code == 7

@@ -38,14 +38,16 @@ def test_hns_noalloc_matches_hns_stage_twice(kind):
 
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
+    status = torch.full((1,), -1, dtype=torch.int32, device=dev)  # the call clears it
     for call in range(2):
         d_hs = torch.from_numpy(base.reshape(-1, order="F").view(np.float64).copy()).to(dev)
-        lapw1gpu.hns_noalloc(p, d_hs.data_ptr(), n, stream.cuda_stream)
+        lapw1gpu.hns_noalloc(p, d_hs.data_ptr(), n, stream.cuda_stream, status.data_ptr())
         torch.cuda.synchronize(dev)
         out = d_hs.cpu().numpy().view(np.complex128).reshape((n, n), order="F")
         err = rel_errors(out, based, ref, refd)
         assert err["H"] <= TOL_FP64 and err["S"] == 0.0, (call, err)
         assert np.array_equal(np.triu(out, 1), np.triu(base, 1)), call
+        assert int(status.item()) == 0, call
 
 
 @pytest.mark.gpu
@@ -59,3 +61,68 @@ def test_hns_noalloc_rejects_problems_beyond_its_array():
     with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
         lapw1gpu.hns_noalloc(p, d_hs.data_ptr(), p.n, 0)
     assert e.value.code == 7  # LAPW1GPU_ERR_RANGE
+
+
+def _oversized_rmt(p):
+    """The problem with type 0's RMT stretched so that RMT |k+G| reaches 25,
+    beyond SPHBES's start table (sphbes.f:60-64)."""
+    import dataclasses
+    rmt = np.array(p.rmt, dtype=np.float64, copy=True)
+    rmt[0] = 25.0 / float(np.max(p.rk[: p.nv]))
+    return dataclasses.replace(p, rmt=rmt)
+
+
+@pytest.mark.gpu
+def test_hns_noalloc_reports_sphbes_range_like_the_hns_stage():
+    """An RMT that puts RMT |k+G| beyond SPHBES's range: the HNS stage
+    returns LAPW1GPU_ERR_RANGE from its device status word, and the
+    allocation-free entry point returns the same code from its host check,
+    before any device work (the caller's HS is left untouched)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    import torch
+
+    p = _oversized_rmt(synth.small_case("lo"))
+    n = p.n
+    with lapw1gpu.Context(0) as ctx:
+        with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
+            ctx.setup(p, stages=2, hs=np.zeros((n, n), dtype=np.complex128, order="F"))
+        assert e.value.code == 7
+    d_hs = torch.zeros(n * n * 2, dtype=torch.float64, device="cuda")
+    with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
+        lapw1gpu.hns_noalloc(p, d_hs.data_ptr(), n, 0)
+    assert e.value.code == 7
+    torch.cuda.synchronize()
+    assert float(d_hs.abs().max()) == 0.0
+
+
+@pytest.mark.gpu
+def test_hns_noalloc_status_word_reports_nonfinite():
+    """A non-finite T entry: the HNS stage returns LAPW1GPU_ERR_NONFINITE, and
+    the allocation-free entry point leaves bit 2 (non-finite) in the caller's
+    status word; a clean call afterwards clears it again."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    import dataclasses
+
+    import torch
+
+    p = synth.small_case("lo")
+    tns = np.array(p.tns, copy=True)
+    tns[0, 0, 0, 0] = np.nan
+    bad = dataclasses.replace(p, tns=tns)
+    n = p.n
+    with lapw1gpu.Context(0) as ctx:
+        with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
+            ctx.setup(bad, stages=2, hs=np.zeros((n, n), dtype=np.complex128, order="F"))
+        assert e.value.code == 4
+    dev = torch.device("cuda", 0)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    d_hs = torch.zeros(n * n * 2, dtype=torch.float64, device=dev)
+    lapw1gpu.hns_noalloc(bad, d_hs.data_ptr(), n, 0, status.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert int(status.item()) & 2
+    d_hs.zero_()
+    lapw1gpu.hns_noalloc(p, d_hs.data_ptr(), n, 0, status.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert int(status.item()) == 0
