@@ -78,6 +78,20 @@ def baseline_lib():
     return _native
 
 
+class blas_zgemm:
+    """Context manager: the portable oracle's ZHER2M blocks on OpenBLAS
+    zgemm (the loops otherwise).  Same sums in another order: for checks of
+    large problems that the loops make slow."""
+
+    def __enter__(self):
+        path = openblas_path()
+        self.on = bool(path) and lib().oracle_use_blas(path.encode(), b"scipy_cblas_zgemm") == 0
+        return self
+
+    def __exit__(self, *a):
+        lib().oracle_use_blas(None, None)
+
+
 def lib():
     global _lib
     if _lib is None:

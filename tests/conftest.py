@@ -3,6 +3,11 @@ import sys
 
 import pytest
 
+# the oracle's OpenMP threads sleep between parallel regions instead of
+# spinning, leaving the cores to OpenBLAS where a check uses it (set before
+# any OpenMP runtime is loaded)
+os.environ.setdefault("OMP_WAIT_POLICY", "passive")
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)

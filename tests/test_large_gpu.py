@@ -1,0 +1,148 @@
+"""The 100-atom workloads against the oracle and against central differences.
+
+  * c3 (100 atoms, RKmax 6, N = 5904): the full FP64 setup against the
+    oracle's HAMILT + HNS at the parity bar, 1e-12 per matrix;
+  * c3: the split-precision eigenvalues in the window SECLR4 solves in
+    against the eigenvalues of the oracle's matrices, 1e-6 Ry;
+  * c4 k-point 0 (RKmax 8, N = 12726): the FP64 HAMILT stage on sampled
+    column blocks, and the HNS stage of three atoms (the other atom types'
+    non-spherical T blocks zeroed), against the oracle at 1e-12;
+  * c3 forces: the adjoint (FP64 and split) against central differences of
+    the band energy of the lowest 400 bands with step 1e-4 bohr, on 12
+    components, within 1e-4 Ry/bohr.
+The oracle runs its ZHER2M blocks on OpenBLAS zgemm here (the same sums in
+another order) to keep the c3 reference at tens of seconds.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from hack_wein2k_b200 import forces as FO
+from hack_wein2k_b200 import lapw1gpu, synth
+from hack_wein2k_b200.problem import hermitian_from_packed
+from hack_wein2k_b200.seclr import solve
+from oracle import oracle as O
+from tests.helpers import rel_errors
+
+NB = 400
+TOL_FD_RY_BOHR = 1.0e-4
+
+
+@pytest.fixture(scope="module")
+def c3():
+    p = synth.config("c3")[0]
+    with O.blas_zgemm():
+        hs_o, hsd_o = O.setup(p)
+    return p, hs_o, hsd_o
+
+
+@pytest.mark.gpu
+def test_c3_full_setup_fp64_matches_oracle(ctx, c3):
+    p, hs_o, hsd_o = c3
+    hs, hsd = ctx.setup(p)
+    err = rel_errors(hs, hsd, hs_o, hsd_o)
+    assert err["H"] <= 1e-12 and err["S"] <= 1e-12, err
+
+
+def _window(w, lo=-10.0, hi=10.0):
+    return (w > lo) & (w < hi)
+
+
+@pytest.mark.gpu
+def test_c3_split_eigenvalues_match_oracle_matrices(ctx, c3):
+    p, hs_o, hsd_o = c3
+    dev = torch.device("cuda", ctx.device)
+    H, S = hermitian_from_packed(hs_o, hsd_o)
+    w0, _ = solve(torch.from_numpy(H).to(dev), torch.from_numpy(S).to(dev))
+    w0 = w0.cpu().numpy()
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    ctx.set_slices(5, 4)
+    try:
+        hs, hsd = ctx.setup(p)
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    H, S = hermitian_from_packed(hs, hsd)
+    w, _ = solve(torch.from_numpy(H).to(dev), torch.from_numpy(S).to(dev))
+    w = w.cpu().numpy()
+    win = _window(w0)
+    assert win.sum() > 20
+    assert np.abs(w[win] - w0[win]).max() <= 1e-6, np.abs(w[win] - w0[win]).max()
+
+
+@pytest.fixture(scope="module")
+def c4k0():
+    return synth.config("c4", nk=1)[0]
+
+
+@pytest.mark.gpu
+def test_c4_hamilt_sampled_columns_match_oracle(ctx, c4k0):
+    """HAMILT's loop over columns I (hamilt.F:188-466) writes S into column
+    I above the diagonal and conj(H) into row I left of it; the oracle runs
+    that loop over three blocks of I only, and the stage's result (after
+    ZSWAP: diag(HS) = H, HSDIAG = S) is compared on those rows/columns."""
+    p = c4k0
+    hs, hsd = ctx.setup(p, stages=1)
+    nv = p.nv
+    for lo, hi in ((1, 96), (nv // 2, nv // 2 + 63), (nv - 127, nv)):
+        ho, hdo = O.hamilt_sample(p, lo, hi)  # before the ZSWAP
+        s_err = s_max = h_err = h_max = 0.0
+        for i in range(lo - 1, hi):
+            s_g = np.append(hs[:i, i], hsd[i])          # S(1:I, I) incl. the diagonal
+            s_o = np.append(ho[:i, i], ho[i, i])
+            h_g = np.append(hs[i, :i], hs[i, i])        # conj(H)(I, 1:I-1) and H(I, I)
+            h_o = np.append(ho[i, :i], hdo[i])
+            s_err, s_max = max(s_err, np.abs(s_g - s_o).max()), max(s_max, np.abs(s_o).max())
+            h_err, h_max = max(h_err, np.abs(h_g - h_o).max()), max(h_max, np.abs(h_o).max())
+        assert s_err <= 1e-12 * s_max and h_err <= 1e-12 * h_max, (lo, hi, s_err / s_max, h_err / h_max)
+
+
+@pytest.mark.gpu
+def test_c4_hns_three_atoms_match_oracle(ctx, c4k0):
+    keep = (0, 37, 99)
+    tns = np.zeros_like(c4k0.tns)
+    for t in keep:
+        tns[t] = c4k0.tns[t]
+    p = dataclasses.replace(c4k0, tns=tns)
+    n = p.n
+    hs, _ = ctx.setup(p, stages=2, hs=np.zeros((n, n), dtype=np.complex128, order="F"))
+    ref = np.zeros((n, n), dtype=np.complex128, order="F")
+    with O.blas_zgemm():
+        for t in keep:  # one atom per type: atom t + 1 (1-based)
+            ref += O.hns_sample(p, t + 1, t + 1)
+    low = np.tril_indices(n)
+    assert np.abs(hs[low] - ref[low]).max() <= 1e-12 * np.abs(ref[low]).max()
+    assert np.abs(ref[low]).max() > 0
+
+
+@pytest.fixture(scope="module")
+def c3_forces(ctx):
+    p = synth.config("c3")[0]
+    dev = torch.device("cuda", ctx.device)
+    occ = torch.ones(NB, dtype=torch.float64, device=dev)
+    E, w, X, kp = FO.band_energy(ctx, p, occ)
+    g64 = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    try:
+        gsp = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    kp.free()
+    return p, occ, g64, gsp
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ac", [(0, 0), (9, 1), (18, 2), (27, 0), (36, 1), (45, 2),
+                                (54, 0), (63, 1), (72, 2), (81, 0), (90, 1), (99, 2)])
+def test_c3_forces_match_central_differences(ctx, c3_forces, ac):
+    """dE/dR of the adjoint against (E(R + h) - E(R - h)) / 2h, h = 1e-4
+    bohr, through the FP64 setup and the device eigen-solve."""
+    p, occ, g64, gsp = c3_forces
+    a, c = ac
+    bk = np.asarray(p.bkzz, dtype=np.float64).reshape(3, 3)
+    h = 1.0e-4 * bk[c, c] / (2.0 * np.pi)  # lattice step of the orthorhombic cell
+    fd = FO.finite_difference(ctx, p, occ, a, c, h=h)
+    to_cart = bk[c, c] / (2.0 * np.pi)
+    assert abs(fd - g64[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, g64[a, c] * to_cart)
+    assert abs(fd - gsp[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gsp[a, c] * to_cart)
