@@ -432,19 +432,28 @@ def north_star(args):
     occ = torch.ones(NBANDS, dtype=torch.float64, device=dev)
     grads = [torch.empty((q.ndf, 3), dtype=torch.float64, device=dev) for q in ps]
 
+    fargs = (kps, [x.data_ptr() for x in Xc], [q.n for q in ps], NBANDS, occ.data_ptr(), [w.data_ptr() for w in W],
+             [g.data_ptr() for g in grads])
+
     def forces_all():
-        nf = 0
-        for i, q in enumerate(ps):
-            kps[i].forces(Xc[i].data_ptr(), q.n, NBANDS, occ.data_ptr(), W[i].data_ptr(), grads[i].data_ptr())
-            nf += ctx.last_launches()
-        return nf
+        """the adjoint of all 16 k-points, queued back to back (one library call)"""
+        ms_f = ctx.forces_batch(*fargs)
+        return ctx.last_launches(), ms_f
 
     launches = {}
+    host = {"setup_wall_ms": [], "setup_dev_ms": [], "forces_wall_ms": [], "forces_dev_ms": []}
 
     def step():
-        ctx.setup_batch(*bargs)
+        t0 = time.perf_counter()
+        st_b = ctx.setup_batch(*bargs)
+        t1 = time.perf_counter()
         launches["setup"] = ctx.last_launches()
-        launches["forces"] = forces_all()
+        launches["forces"], ms_f = forces_all()
+        t2 = time.perf_counter()
+        host["setup_wall_ms"].append((t1 - t0) * 1e3)
+        host["setup_dev_ms"].append(st_b["ms_total"])
+        host["forces_wall_ms"].append((t2 - t1) * 1e3)
+        host["forces_dev_ms"].append(ms_f)
 
     for _ in range(args.warmup):
         step()
@@ -455,14 +464,15 @@ def north_star(args):
     ms = maxr(ms)
     ms_step = ms / args.steps
     value = ms_step / (NK * world)
+    step_parts = {k: float(np.mean(v[args.warmup:])) for k, v in host.items()}
     g0_split = grads[0].cpu().numpy()
     # parts of the split step: the batched setup alone, the forces alone
     ms_setup_split = min(ctx.setup_batch(*bargs)["ms_total"] for _ in range(3)) / NK
+    ms_forces_split = min(forces_all()[1] for _ in range(2)) / NK
     fst_split = []
     for i, q in enumerate(ps[:4]):
         kps[i].forces(Xc[i].data_ptr(), q.n, NBANDS, occ.data_ptr(), W[i].data_ptr(), grads[i].data_ptr())
         fst_split.append(ctx.forces_stats())
-    ms_forces_split = float(np.mean([f["ms_total"] for f in fst_split]))
     ms_fsph_split = float(np.mean([f["ms_sph_main"] for f in fst_split]))
     # per-kernel times of one split k-point (stats pass)
     st_k = kps[0].run(hs[0].data_ptr(), ps[0].n, hd[0].data_ptr(), stats=True)
@@ -480,11 +490,7 @@ def north_star(args):
     ms64 = maxr(_timed_loop(torch, stream, step64, n64)) / n64
     g0_fp64_same = grads[0].cpu().numpy()  # FP64 adjoint, the split path's eigenvectors
     ms_setup_fp64 = min(ctx.setup_batch(*bargs)["ms_total"] for _ in range(2)) / NK
-    fst64 = []
-    for i, q in enumerate(ps[:2]):
-        kps[i].forces(Xc[i].data_ptr(), q.n, NBANDS, occ.data_ptr(), W[i].data_ptr(), grads[i].data_ptr())
-        fst64.append(ctx.forces_stats())
-    ms_forces_fp64 = float(np.mean([f["ms_total"] for f in fst64]))
+    ms_forces_fp64 = forces_all()[1] / NK
     # accuracy at k-point 0: split against FP64 matrices, eigenvalues, forces
     ctx.setup_batch(*bargs)
     err_hs = _rel_err_c(torch, hs0_split, hs[0])
@@ -629,7 +635,8 @@ def north_star(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": f"int8 x{s_sph}/x{s_hns} slices (spherical/HNS) with f64 combine; f64 force pair sums",
+        "dtype": f"int8 x{s_sph}/x{s_hns}/x6 slices (spherical/HNS/adjoint products) with f64 combine; "
+                 "f64 force pair sums",
         "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD_C4, "kpoints_per_gpu": NK, "n": [q.n for q in ps], "nv0": p0.nv,
                    "nlo": p0.nlo, "atoms": p0.ndf, "bands": NBANDS, "lmax": p0.ltop - 1, "lmax_ns": p0.lnsmax,
@@ -658,6 +665,7 @@ def north_star(args):
         "gpu_launches": int((launches.get("setup", 0) + launches.get("forces", 0)) * args.steps),
         "clocks": clocks,
         "prep_s": {"total": time.time() - t_prep, "eigen_solves": t_eig},
+        "step_parts_ms": step_parts,
     }
     if c1 is not None:
         line["c1"] = c1

@@ -18,7 +18,7 @@ SOURCES = ["lapw1gpu.cu"]
 HEADERS = ["common.cuh", "kernels_fp64.cuh", "split_tc.cuh", "forces.cuh", "sph_tc.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-ccbin", "/usr/bin/g++",
-              "-lcublas", "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
+              "-lcublas", "-lcusolver", "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
 
 
 def _inputs():

@@ -748,20 +748,6 @@ __global__ void __launch_bounds__(256) k_hns_lo_ops(DevProb P, const double2* __
   }
 }
 
-// The per-atom matrix M of k_hns_tmul, dense and column-major:
-// Mbuf[a][k][r] = M[(ro, la) = r][(rr, b) = k] (K = 2 nsl2), for the
-// library's strided-batched product of the split path.
-__global__ void __launch_bounds__(256) k_hns_mdense(int nsl2, const int* __restrict__ atype,
-                                                   const double2* __restrict__ tns, double2* __restrict__ Mbuf) {
-  const int a = blockIdx.x, K = 2 * nsl2;
-  const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
-  for (int idx = threadIdx.x; idx < K * K; idx += 256) {
-    const int col = idx / K, row = idx % K;
-    const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
-    const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
-    Mbuf[(size_t)a * K * K + idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
-  }
-}
 
 // HS(i,j) += sum_k Lop[k][i] * Rop[k][j] on the lower triangle i >= j
 // (zher2m.f:69-80, 'L','N','T').  64x64 tiles, 4x4 complex per thread.
@@ -1006,4 +992,23 @@ __global__ void k_check_finite(int n, const double2* __restrict__ hs, int ld, co
       bad |= ((unsigned)(__double_as_longlong(d.y) >> 52) & 0x7ffu) == 0x7ffu;
     }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, L1G_STATUS_NONFINITE);
+}
+
+// The generalized problem SECLR4 solves (seclr4.F:158-345), unpacked from
+// the packed state: H(i,j) = conj(HS(i,j)) and S(i,j) = conj(HS(j,i)) for
+// i > j (ZHCGST factors S**T), real diagonals from HS(i,i) and HSDIAG(i);
+// the lower triangles of H and S, column-major n x n (ld n).
+__global__ void k_unpack_seclr(int n, const double2* __restrict__ hs, int ld, const double2* __restrict__ hsdiag,
+                               double2* __restrict__ H, double2* __restrict__ S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
+  const int j = blockIdx.y;                             // column
+  if (i >= n || i < j) return;
+  const size_t o = (size_t)j * n + i;
+  if (i == j) {
+    H[o] = cmk(hs[(size_t)i * ld + i].x, 0.0);
+    S[o] = cmk(hsdiag[i].x, 0.0);
+  } else {
+    H[o] = cconj(hs[(size_t)j * ld + i]);
+    S[o] = cconj(hs[(size_t)i * ld + j]);
+  }
 }

@@ -10,8 +10,10 @@
 //   HORB    -> k_horb_rows, k_horb_pairs per U-atom and l
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -72,7 +74,9 @@ struct lapw1gpu_context {
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 5;      // int8 slices of the spherical part (split precision)
   int slices_hns = 5;  // int8 slices of the HNS update
+  int slices_frc = 6;  // int8 slices of the adjoint's density matrices and projections
   cublasHandle_t blas[L1G_MAX_SETS] = {};  // library ZGEMMs, one handle (and workspace) per scratch set
+  cusolverDnHandle_t solver = nullptr;      // the eigen-solve (lapw1gpu_seclr4)
   // tunables (lapw1gpu_autotune)
   int hns_diag_b = 512;    // FP64 HNS: diagonal block of the blocked ZHER2M form
   int split_group = 16;    // split HNS: row tiles per rasterisation group
@@ -316,6 +320,7 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   c->drop_graphs();
   for (auto& h : c->blas)
     if (h) cublasDestroy(h);
+  if (c->solver) cusolverDnDestroy(c->solver);
   for (auto& kv : c->bufs)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   for (auto& kv : c->tiles) cudaFree(kv.second.first);
@@ -345,6 +350,13 @@ int lapw1gpu_set_precision(lapw1gpu_context* c, int prec, int slices) {
   if (prec == LAPW1GPU_PREC_SPLIT && (slices < 2 || slices > L1G_MAX_SLICES)) return LAPW1GPU_ERR_RANGE;
   c->prec = prec;
   if (prec == LAPW1GPU_PREC_SPLIT) c->slices = c->slices_hns = slices;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_set_force_slices(lapw1gpu_context* c, int slices) {
+  if (!c) return LAPW1GPU_ERR_ARG;
+  if (slices < 4 || slices > L1G_MAX_SLICES) return LAPW1GPU_ERR_RANGE;
+  c->slices_frc = slices;
   return LAPW1GPU_OK;
 }
 
@@ -693,45 +705,30 @@ static const int2* tiles_tri(lapw1gpu_kpoint* k, const char* name, int n, int T,
                   });
 }
 
-// HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom, LO-row terms.
-// With a library handle h and a dense-M buffer (split path), L is formed
-// by one strided-batched ZGEMM over the atoms as conj(L) = R^T M^H
-// (column-major npad x K per atom), and the LO terms are added conjugated:
-// the slicer of the split HNS kernel takes the conjugate back.
-// Without Lop (the adjoint, which needs R and CLM only) L is not formed.
+// HNS operands: R = {ALM, BLM} per row, L = M conj(R) per atom (k_hns_tmul),
+// LO-row terms (k_hns_lo_ops).  Without Lop (the adjoint, which needs R and
+// CLM only) L is not formed.
 static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* tns, const LoRange* lor, int nlor,
-                          double2* Lop, double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl,
-                          cublasHandle_t h = nullptr, double2* Mbuf = nullptr) {
-  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1), K = 2 * nsl2;
+                          double2* Lop, double2* Rop, double2* Clo, double2* C2lo, cudaStream_t s, int* nl) {
+  const int nsl2 = (P.lnsmax + 1) * (P.lnsmax + 1);
   k_hns_alm<<<dim3((P.npad + 127) / 128, P.ndf), 128, 0, s>>>(P, lor, nlor, Rop, Clo);
   if (!Lop) {
     *nl += 1;
     return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
   }
-  const bool lib = h && Mbuf;
-  if (lib) {
-    k_hns_mdense<<<P.ndf, 256, 0, s>>>(nsl2, P.atype, tns, Mbuf);
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-    if (cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_C, P.npad, K, K, &one, (const cuDoubleComplex*)Rop,
-                                  P.npad, (long long)K * P.npad, (const cuDoubleComplex*)Mbuf, K, (long long)K * K,
-                                  &zero, (cuDoubleComplex*)Lop, P.npad, (long long)K * P.npad,
-                                  P.ndf) != CUBLAS_STATUS_SUCCESS)
-      return LAPW1GPU_ERR_CUDA;
-  } else {
-    if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
-          : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
-      return LAPW1GPU_ERR_CUDA;
-    // two blocks per SM over the (atom, 64-column) items, contiguous ranges
-    const int nitem = (P.npad + TMUL_I - 1) / TMUL_I * P.ndf;
-    const int nblk = std::max(1, std::min(nitem, 2 * (c ? c->nsm : 148)));
-    const int per = (nitem + nblk - 1) / nblk;
-    k_hns_tmul<<<(nitem + per - 1) / per, 32 * TMUL_WARPS, TMUL_SMEM, s>>>(P.npad, nsl2, P.ndf, per, P.atype, tns,
-                                                                         Rop, Lop);
-  }
+  if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
+        : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
+    return LAPW1GPU_ERR_CUDA;
+  // two blocks per SM over the (atom, 64-column) items, contiguous ranges
+  const int nitem = (P.npad + TMUL_I - 1) / TMUL_I * P.ndf;
+  const int nblk = std::max(1, std::min(nitem, 2 * (c ? c->nsm : 148)));
+  const int per = (nitem + nblk - 1) / nblk;
+  k_hns_tmul<<<(nitem + per - 1) / per, 32 * TMUL_WARPS, TMUL_SMEM, s>>>(P.npad, nsl2, P.ndf, per, P.atype, tns, Rop,
+                                                                       Lop);
   *nl += 2;
   if (P.nlo > 0) {
     k_hns_lo_ops<<<dim3((P.nlo + LOOPS_ROWS - 1) / LOOPS_ROWS, P.ndf), dim3(32, 8), 0, s>>>(P, tns, Lop, Rop, Clo,
-                                                                                           C2lo, lib ? 1 : 0);
+                                                                                           C2lo, 0);
     *nl += 1;
   }
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
@@ -951,18 +948,21 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     if (!Lop || !Rop || !Clo || !C2lo) return LAPW1GPU_ERR_NOMEM;
   }
   if (hns_fork) {
+    // on the set's auxiliary stream: the operands, their int8 slices and
+    // the LO-LO block T = C2 CLM^T (tensor cores, added after the HNS products)
     cudaStream_t a = c->aux[set];
     CK(cudaEventRecord(c->auxf[set], s));
     CK(cudaStreamWaitEvent(a, c->auxf[set], 0));
-    // L through the library's batched product (conj(L) in Lop)
-    double2* Mbuf = (double2*)c->sbuf(set, "hnsM", sizeof(double2) * (size_t)ndf * 4 * nsl2 * nsl2);
-    cublasHandle_t hb = c->handle(set, a);
-    if (!Mbuf || !hb) return LAPW1GPU_ERR_NOMEM;
-    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, a, &nl,
-                            hb, Mbuf);
+    int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, a, &nl);
     if (!rc)
       rc = split_hns_gemm(c, k, set, n, k->npad, Khns, Lop, Rop, d_hs, ldhs, c->slices_hns, a, &nl, nullptr,
-                          nullptr, 1, 1);
+                          nullptr, 0, 1);
+    if (!rc && k->nlo > 0) {
+      double2* T = (double2*)c->sbuf(set, "hnsLoT", sizeof(double2) * (size_t)k->nlo * k->nlo);
+      if (!T) return LAPW1GPU_ERR_NOMEM;
+      rc = split_rect_gemm(c, k, set, k->nlo, k->nlo, ndf * nsl2, C2lo, k->nlo, Clo, k->nlo, T, k->nlo,
+                           c->slices_hns, a, &nl, 1);
+    }
     if (rc) return rc;
     CK(cudaEventRecord(c->auxj[set], a));
   }
@@ -1038,7 +1038,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     if (hns_fork) {
       CK(cudaStreamWaitEvent(s, c->auxj[set], 0));
       rc = split_hns_gemm(c, k, set, n, k->npad, K, Lop, Rop, d_hs, ldhs, c->slices_hns, s, &nl, hp,
-                          ev ? ev + 14 : nullptr, 1, 2);
+                          ev ? ev + 14 : nullptr, 0, 2);
     } else {
       rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), Lop, Rop, Clo, C2lo, s, &nl);
       if (rc) return rc;
@@ -1054,16 +1054,20 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     if (rc) return rc;
     if (k->nlo > 0) {
       nl++;
-      // T = C2^T CLM (nlo x nlo, K = NDF 25) by library ZGEMM, then its
+      // T = C2 CLM^T (nlo x nlo, K = NDF 25): in split precision from the
+      // auxiliary stream's tensor-core product, else by library ZGEMM; its
       // lower triangle into HS
       double2* T = (double2*)c->sbuf(set, "hnsLoT", sizeof(double2) * (size_t)k->nlo * k->nlo);
-      cublasHandle_t h = c->handle(set, s);
-      if (!T || !h) return LAPW1GPU_ERR_NOMEM;
-      const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-      if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, k->nlo, k->nlo, ndf * nsl2, &one, (const cuDoubleComplex*)C2lo,
-                      k->nlo, (const cuDoubleComplex*)Clo, k->nlo, &zero, (cuDoubleComplex*)T,
-                      k->nlo) != CUBLAS_STATUS_SUCCESS)
-        return LAPW1GPU_ERR_CUDA;
+      if (!T) return LAPW1GPU_ERR_NOMEM;
+      if (!hns_fork) {
+        cublasHandle_t h = c->handle(set, s);
+        if (!h) return LAPW1GPU_ERR_NOMEM;
+        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+        if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, k->nlo, k->nlo, ndf * nsl2, &one, (const cuDoubleComplex*)C2lo,
+                        k->nlo, (const cuDoubleComplex*)Clo, k->nlo, &zero, (cuDoubleComplex*)T,
+                        k->nlo) != CUBLAS_STATUS_SUCCESS)
+          return LAPW1GPU_ERR_CUDA;
+      }
       k_add_lower<<<dim3((k->nlo + 127) / 128, k->nlo), 128, 0, s>>>(nv, k->nlo, T, d_hs, ldhs, c->d_status);
     }
     CK(cudaGetLastError());
@@ -1231,9 +1235,11 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
     c->graphs.push_back({key, exec, nl});
     g = &c->graphs.back();
   }
+  const auto th0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(c->ev[0], c->stream));
   CK(cudaGraphLaunch(g->exec, c->stream));
   CK(cudaEventRecord(c->ev[6], c->stream));
+  const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
   int hstat = 0;
   CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1247,6 +1253,7 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
     st->ms_total = tot;
     for (int i = 0; i < nk; i++) st->flops_fp64_equiv += alg_flops(kps[i]);
     st->kernel_launches = g->launches;
+    st->ms_host = host_ms;
   }
   if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
   if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
@@ -1577,15 +1584,11 @@ int lapw1gpu_setup(lapw1gpu_context* c, const lapw1gpu_problem* p, double* hs, i
   return lapw1gpu_setup_stages(c, p, 7, hs, ldhs, hsdiag, st);
 }
 
-// Band-energy gradient (forces.cuh): rho = C f C^H and rhoE = C f eps C^H by
-// library ZGEMM, the PW x PW and LO parts by k_force_sph / k_force_lo, the
-// HNS part through its factors (four ZGEMMs and a per-atom reduction).
-int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_, int ldc, int nb, const double* d_occ,
-                    const double* d_eps, double* d_grad) {
-  if (!c || !k || k->ctx != c || !d_c_ || !d_occ || !d_eps || !d_grad || nb < 1 || ldc < k->n)
-    return LAPW1GPU_ERR_ARG;
-  if (!k->orbs.empty()) return LAPW1GPU_ERR_ARG;
-  CK(cudaSetDevice(c->device));
+// The adjoint of one k-point queued on the context's stream (no host
+// synchronisation): status bits go to c->d_status, which the caller clears.
+// timed: record the interval events of lapw1gpu_forces_stats.
+static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_, int ldc, int nb,
+                          const double* d_occ, const double* d_eps, double* d_grad, bool timed, int* nl_out) {
   const double2* C = reinterpret_cast<const double2*>(d_c_);
   cudaStream_t s = c->stream;
   DevProb P = k->P;
@@ -1603,8 +1606,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   if (!h) return LAPW1GPU_ERR_CUDA;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   int nlf = 0;  // kernels launched (a library product counts as one)
-  CK(cudaEventRecord(c->fev[0], s));
-  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  if (timed) CK(cudaEventRecord(c->fev[0], s));
   CK(cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * ndf, s));
   k_albl<<<dim3((k->nvpad + 127) / 128, nat), 128, 0, s>>>(P, c->d_status);
   k_phase<<<dim3((k->npad + 127) / 128, ndf), 128, 0, s>>>(P);
@@ -1632,8 +1634,9 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
     // written, not added (no zero fill): every lower-triangle element the
     // force kernels read is a product tile's element
     int nlr = 0;
-    int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
-    if (!rc) rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices, s, &nlr, nullptr, nullptr, 0, 3, 1);
+    int rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Cf, rho, n, c->slices_frc, s, &nlr, nullptr, nullptr, 0, 3, 1);
+    if (!rc)
+      rc = split_hns_gemm(c, k, 0, n, n, nb, Cn, Ce, rhoe, n, c->slices_frc, s, &nlr, nullptr, nullptr, 0, 3, 1);
     if (rc) return rc;
     nlf += nlr;
     rt = 1;
@@ -1646,7 +1649,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       return LAPW1GPU_ERR_CUDA;
     nlf += 2;
   }
-  CK(cudaEventRecord(c->fev[1], s));
+  if (timed) CK(cudaEventRecord(c->fev[1], s));
   int ntiles = 0;
   const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
   if (!tl) return LAPW1GPU_ERR_NOMEM;
@@ -1664,21 +1667,21 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
   double* bins = (double*)c->buf("frc_bins", sizeof(double) * 2 * nbox);
   if (!bins) return LAPW1GPU_ERR_NOMEM;
   CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
-  CK(cudaEventRecord(c->fev[2], s));
+  if (timed) CK(cudaEventRecord(c->fev[2], s));
   if (lt11)
     k_force_sph<FRC_LT, false><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
                                                                   d_grad, bins);
   else
     k_force_sph<SPH_LMAX, true><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
                                                                    d_grad, bins);
-  CK(cudaEventRecord(c->fev[3], s));
+  if (timed) CK(cudaEventRecord(c->fev[3], s));
   k_force_step<<<ndf, 256, 0, s>>>(P, k->tab, bins, d_grad);
   CK(cudaGetLastError());
   if (nlo > 0) {
     k_force_lo<<<dim3((n + 127) / 128, nlo), 128, 0, s>>>(P, k->d_locols, rho, rhoe, n, rt, d_grad);
     nlf++;
   }
-  CK(cudaEventRecord(c->fev[4], s));
+  if (timed) CK(cudaEventRecord(c->fev[4], s));
   CK(cudaGetLastError());
   if (!k->nohns) {
     const int nsl2 = (k->lnsmax + 1) * (k->lnsmax + 1);
@@ -1710,7 +1713,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
       k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
       int nly = 0;
-      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices, s, &nly, 1);
+      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices_frc, s, &nly, 1);
       if (rc) return rc;
       nlf += nly + 2;
     } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
@@ -1730,7 +1733,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
         if (!Lc) return LAPW1GPU_ERR_NOMEM;
         k_force_trans<<<dim3((nlo + 31) / 32, (Kc + 31) / 32), 256, 0, s>>>(Clo, nlo, Kc, nlo, 1, Lc, Kc);
         int nly = 0;
-        rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices, s,
+        rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices_frc, s,
                              &nly, 1);
         if (rc) return rc;
         nlf += nly + 1;
@@ -1755,19 +1758,130 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c_,
       CK(cudaGetLastError());
     }
   }
-  CK(cudaEventRecord(c->fev[5], s));
+  if (timed) CK(cudaEventRecord(c->fev[5], s));
+  *nl_out += nlf;
+  return LAPW1GPU_OK;
+}
+
+static int forces_check(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c, int ldc, int nb,
+                        const double* d_occ, const double* d_eps, const double* d_grad) {
+  if (!c || !k || k->ctx != c || !d_c || !d_occ || !d_eps || !d_grad || nb < 1 || ldc < k->n)
+    return LAPW1GPU_ERR_ARG;
+  if (!k->orbs.empty()) return LAPW1GPU_ERR_ARG;
+  return LAPW1GPU_OK;
+}
+
+// Band-energy gradient (forces.cuh): rho = C f C^H and rhoE = C f eps C^H by
+// library ZGEMM, the PW x PW and LO parts by k_force_sph / k_force_lo, the
+// HNS part through its factors (four ZGEMMs and a per-atom reduction).
+int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c, int ldc, int nb, const double* d_occ,
+                    const double* d_eps, double* d_grad) {
+  int rc = forces_check(c, k, d_c, ldc, nb, d_occ, d_eps, d_grad);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  int nl = 0;
+  rc = forces_enqueue(c, k, d_c, ldc, nb, d_occ, d_eps, d_grad, true, &nl);
+  if (rc) return rc;
   int hstat = 0;
   CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   c->last_status = hstat;
   c->status_pending = false;
-  c->last_launches = nlf;
+  c->last_launches = nl;
   for (int q = 0; q < 5; q++) cudaEventElapsedTime(&c->fms[q], c->fev[q], c->fev[q + 1]);
   cudaGetLastError();
   return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
 }
 
+// The adjoint of a k-point list queued back to back on the context's stream
+// (one host synchronisation and status read at the end), the companion of
+// lapw1gpu_setup_batch.
+int lapw1gpu_forces_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int nk, const double* const* d_c,
+                          const int* ldc, int nb, const double* d_occ, const double* const* d_eps,
+                          double* const* d_grad, double* ms_total) {
+  if (!c || !kps || nk < 1 || !d_c || !ldc || !d_eps || !d_grad) return LAPW1GPU_ERR_ARG;
+  for (int i = 0; i < nk; i++) {
+    const int rc = forces_check(c, kps[i], d_c[i], ldc[i], nb, d_occ, d_eps[i], d_grad[i]);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  CK(cudaEventRecord(c->ev[0], s));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+  int nl = 0;
+  for (int i = 0; i < nk; i++) {
+    const int rc = forces_enqueue(c, kps[i], d_c[i], ldc[i], nb, d_occ, d_eps[i], d_grad[i], false, &nl);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(c->ev[6], s));
+  int hstat = 0;
+  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  c->last_status = hstat;
+  c->status_pending = false;
+  c->last_launches = nl;
+  if (ms_total) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[6]);
+    *ms_total = t;
+  }
+  return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
+}
+
 }  // extern "C"
+
+// SECLR4 on the device (seclr4.F:149-345): the generalized problem from the
+// packed state, solved by the library (cuSOLVER zhegvdx: Cholesky of S,
+// reduction, tridiagonal divide and conquer, eigenvalues in (el, eu]).
+extern "C" int lapw1gpu_seclr4(lapw1gpu_context* c, const double* d_hs_, int ldhs, const double* d_hsdiag_, int n,
+                               double el, double eu, int nmax, double* d_eig, double* d_vec_, int ldv, int* nfound) {
+  if (!c || !d_hs_ || !d_hsdiag_ || n < 1 || ldhs < n || nmax < 1 || !d_eig || !nfound || (d_vec_ && ldv < n) ||
+      !(el < eu))
+    return LAPW1GPU_ERR_ARG;
+  *nfound = 0;
+  CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  if (!c->solver && cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  if (cusolverDnSetStream(c->solver, s) != CUSOLVER_STATUS_SUCCESS) return LAPW1GPU_ERR_CUDA;
+  const size_t nn = (size_t)n * n;
+  double2* H = (double2*)c->buf("sec_h", sizeof(double2) * nn);
+  double2* S = (double2*)c->buf("sec_s", sizeof(double2) * nn);
+  double* W = (double*)c->buf("sec_w", sizeof(double) * n);
+  int* info = (int*)c->buf("sec_info", sizeof(int));
+  if (!H || !S || !W || !info) return LAPW1GPU_ERR_NOMEM;
+  k_unpack_seclr<<<dim3((n + 127) / 128, n), 128, 0, s>>>(n, reinterpret_cast<const double2*>(d_hs_), ldhs,
+                                                         reinterpret_cast<const double2*>(d_hsdiag_), H, S);
+  CK(cudaGetLastError());
+  const cusolverEigMode_t jobz = d_vec_ ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+  int lwork = 0, meig = 0;
+  if (cusolverDnZhegvdx_bufferSize(c->solver, CUSOLVER_EIG_TYPE_1, jobz, CUSOLVER_EIG_RANGE_V, CUBLAS_FILL_MODE_LOWER,
+                                   n, (cuDoubleComplex*)H, n, (cuDoubleComplex*)S, n, el, eu, 0, 0, &meig, W,
+                                   &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return LAPW1GPU_ERR_CUDA;
+  double2* work = (double2*)c->buf("sec_work", sizeof(double2) * (size_t)std::max(1, lwork));
+  if (!work) return LAPW1GPU_ERR_NOMEM;
+  if (cusolverDnZhegvdx(c->solver, CUSOLVER_EIG_TYPE_1, jobz, CUSOLVER_EIG_RANGE_V, CUBLAS_FILL_MODE_LOWER, n,
+                        (cuDoubleComplex*)H, n, (cuDoubleComplex*)S, n, el, eu, 0, 0, &meig, W,
+                        (cuDoubleComplex*)work, lwork, info) != CUSOLVER_STATUS_SUCCESS)
+    return LAPW1GPU_ERR_CUDA;
+  int hinfo = 0;
+  CK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (hinfo != 0) return hinfo > n ? LAPW1GPU_ERR_NONFINITE : LAPW1GPU_ERR_RANGE;  // S not positive definite / no convergence
+  const int m = std::min(meig, nmax);
+  if (m > 0) {
+    CK(cudaMemcpyAsync(d_eig, W, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+    if (d_vec_)
+      CK(cudaMemcpy2DAsync(d_vec_, sizeof(double2) * ldv, H, sizeof(double2) * n, sizeof(double2) * n, m,
+                           cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  *nfound = m;
+  c->last_launches = 1;
+  return LAPW1GPU_OK;
+}
 
 // ---------------------------------------------------------------------
 // HNS without device allocation.

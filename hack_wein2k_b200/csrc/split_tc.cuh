@@ -573,10 +573,13 @@ static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
                            const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
                            int slices, cudaStream_t s, int* nlaunch, int ovw = 0) {
   switch (slices) {
+    case 2: return split_gemm_rect<2>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 3: return split_gemm_rect<3>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 8: return split_gemm_rect<8>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }

@@ -35,6 +35,8 @@ EXPORTS = [
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
     "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices", "lapw1gpu_test_wait_timeout",
     "lapw1gpu_last_launches", "lapw1gpu_host_register", "lapw1gpu_host_unregister", "lapw1gpu_forces_stats",
+    "lapw1gpu_forces_batch", "lapw1gpu_set_force_slices",
+    "lapw1gpu_seclr4",
 ]
 
 _lib = None
@@ -70,6 +72,9 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_finalize.argtypes = [vp]
     lib.lapw1gpu_set_precision.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_set_slices.argtypes = [vp, C.c_int, C.c_int]
+    lib.lapw1gpu_set_force_slices.argtypes = [vp, C.c_int]
+    lib.lapw1gpu_seclr4.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     lib.lapw1gpu_kpoint_upload.argtypes = [vp, C.POINTER(CProblem), C.POINTER(vp)]
     lib.lapw1gpu_kpoint_free.argtypes = [vp]
     lib.lapw1gpu_kpoint_run.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(CStats)]
@@ -92,6 +97,9 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_test_wait_timeout.argtypes = [vp, C.c_int]
     lib.lapw1gpu_last_launches.argtypes = [vp]
     lib.lapw1gpu_forces_stats.argtypes = [vp, C.POINTER(CStats)]
+    lib.lapw1gpu_forces_batch.argtypes = [vp, C.POINTER(vp), C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
+                                          C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                          C.POINTER(C.c_double)]
     lib.lapw1gpu_host_register.argtypes = [vp, C.c_void_p, C.c_size_t]
     lib.lapw1gpu_host_unregister.argtypes = [vp, C.c_void_p]
     _lib = lib
@@ -164,6 +172,10 @@ class Context:
         """split precision with separate slice counts (lapw1gpu_set_slices)"""
         _check("lapw1gpu_set_slices", self.lib.lapw1gpu_set_slices(self.h, slices_sph, slices_hns))
 
+    def set_force_slices(self, slices: int):
+        """int8 slices of the adjoint's products in split precision (lapw1gpu_set_force_slices)"""
+        _check("lapw1gpu_set_force_slices", self.lib.lapw1gpu_set_force_slices(self.h, slices))
+
     @property
     def stream_handle(self) -> int:
         return int(self.lib.lapw1gpu_stream(self.h) or 0)
@@ -229,6 +241,29 @@ class Context:
         _check("lapw1gpu_setup_batch",
                self.lib.lapw1gpu_setup_batch(self.h, karr, nk, stages, harr, larr, darr, C.byref(st)))
         return st.as_dict()
+
+    def forces_batch(self, kps, d_c_ptrs, ldc, nb: int, d_occ_ptr: int, d_eps_ptrs, d_grad_ptrs) -> float:
+        """lapw1gpu_forces_batch over resident k-points; returns the device
+        time of the whole list (ms)."""
+        nk = len(kps)
+        karr = (C.c_void_p * nk)(*[k.h.value if isinstance(k.h, C.c_void_p) else k.h for k in kps])
+        ms = C.c_double()
+        _check("lapw1gpu_forces_batch",
+               self.lib.lapw1gpu_forces_batch(self.h, karr, nk, (C.c_void_p * nk)(*d_c_ptrs), (C.c_int * nk)(*ldc),
+                                              nb, C.c_void_p(d_occ_ptr), (C.c_void_p * nk)(*d_eps_ptrs),
+                                              (C.c_void_p * nk)(*d_grad_ptrs), C.byref(ms)))
+        return ms.value
+
+    def seclr4(self, d_hs_ptr: int, ldhs: int, d_hsdiag_ptr: int, n: int, el: float, eu: float, nmax: int,
+               d_eig_ptr: int, d_vec_ptr: int = 0, ldv: int = 0) -> int:
+        """lapw1gpu_seclr4: eigenvalues (and eigenvectors) of the packed
+        state on the device; returns how many were found."""
+        nf = C.c_int()
+        _check("lapw1gpu_seclr4",
+               self.lib.lapw1gpu_seclr4(self.h, C.c_void_p(d_hs_ptr), ldhs, C.c_void_p(d_hsdiag_ptr), n, el, eu, nmax,
+                                        C.c_void_p(d_eig_ptr), C.c_void_p(d_vec_ptr) if d_vec_ptr else None,
+                                        ldv or n, C.byref(nf)))
+        return nf.value
 
     def tuning(self) -> dict:
         t = Tuning()

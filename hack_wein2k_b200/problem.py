@@ -48,7 +48,7 @@ class CStats(C.Structure):
     _fields_ = [(k, C.c_double) for k in (
         "ms_total", "ms_albl", "ms_spherical", "ms_lo", "ms_hns", "ms_horb",
         "ms_h2d", "ms_d2h", "flops_fp64_equiv", "kernel_launches", "ms_sph_main", "ms_hns_main",
-        "ms_k_albl", "ms_table", "ms_sph_slice")]
+        "ms_k_albl", "ms_table", "ms_sph_slice", "ms_host")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

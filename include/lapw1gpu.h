@@ -160,6 +160,7 @@ typedef struct lapw1gpu_stats {
   double ms_table;      /* K-c: the Theta/WARP table kernel k_table alone     */
   double ms_sph_slice;  /* K-a, split path: the two spherical operand slicers
                            (phases x AL/BL cut into int8 slices)             */
+  double ms_host;       /* batch: host time of enqueuing the graph launch   */
 } lapw1gpu_stats;
 
 typedef struct lapw1gpu_context lapw1gpu_context;
@@ -177,6 +178,10 @@ int lapw1gpu_set_precision(lapw1gpu_context* ctx, int prec, int slices);
  * for HNS (the non-spherical part is one to two orders of magnitude
  * smaller, so it tolerates one slice fewer at the same eigenvalue error) */
 int lapw1gpu_set_slices(lapw1gpu_context* ctx, int slices_sph, int slices_hns);
+/* int8 slices (4..8, default 6) of the adjoint's products in split
+ * precision (lapw1gpu_forces: the density matrices and the HNS
+ * projections); the force pair sums stay FP64 */
+int lapw1gpu_set_force_slices(lapw1gpu_context* ctx, int slices);
 
 /* One k-point's inputs resident in device memory (uploaded once; the
  * benchmark's resident-input path and the k-point batch driver use it). */
@@ -238,6 +243,20 @@ int lapw1gpu_last_launches(lapw1gpu_context* ctx);
 /* device status word of the last run (L1G_STATUS_* bits), 0 if clean; after
  * an asynchronous lapw1gpu_kpoint_run it waits for that run first */
 int lapw1gpu_last_status(lapw1gpu_context* ctx);
+
+/* SECLR4's generalized eigen-solve (seclr4.F:149-345) on the device, from
+ * the packed state the setup leaves: H x = e S x with H(i,j) = conj(HS(i,j))
+ * and S(i,j) = conj(HS(j,i)) for i > j (ZHCGST factors S**T), real
+ * diagonals from HS(i,i) and HSDIAG(i).  Eigenvalues in (el, eu], at most
+ * nmax, ascending, into d_eig (device, nmax doubles); their S-orthonormal
+ * eigenvectors into d_vec (device, n x nmax complex column-major, ldv >= n;
+ * NULL: eigenvalues only); *nfound (host) their count.  d_hs/d_hsdiag are
+ * read only.  The solver is the library's (cuSOLVER zhegvdx: Cholesky,
+ * reduction, divide and conquer), where the reference calls ZPOTRF, ZHCGST,
+ * ZHEEVX2 and ZTRSM.  A non-positive-definite S returns LAPW1GPU_ERR_NONFINITE.
+ * Synchronous. */
+int lapw1gpu_seclr4(lapw1gpu_context* ctx, const double* d_hs, int ldhs, const double* d_hsdiag, int n,
+                    double el, double eu, int nmax, double* d_eig, double* d_vec, int ldv, int* nfound);
 
 /* Build the nine HNS T blocks from the reference's gaunt lists: the sums of
  * hns.F:317-380 over LMSORT's grouping (lmsort.f:246-421: entries sorted by
@@ -329,6 +348,17 @@ int lapw1gpu_autotune(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp, double* d_hs,
 int lapw1gpu_forces(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp,
                     const double* d_c, int ldc, int nb, const double* d_occ,
                     const double* d_eps, double* d_grad);
+
+/* lapw1gpu_forces for a k-point list (the k-points of a lapw1gpu_setup_batch
+ * and their eigenvectors): kps[i], d_c[i] (ldc[i] >= n_i, nb columns),
+ * d_eps[i] (nb eigenvalues) and d_grad[i] (ndf x 3) per k-point, one
+ * occupation vector d_occ for all.  The k-points are queued back to back on
+ * the context's stream with one synchronisation at the end; ms_total
+ * (optional) gets the device time of the whole list.  Synchronous.  No
+ * counterpart in lapw1. */
+int lapw1gpu_forces_batch(lapw1gpu_context* ctx, lapw1gpu_kpoint* const* kps, int nk,
+                          const double* const* d_c, const int* ldc, int nb, const double* d_occ,
+                          const double* const* d_eps, double* const* d_grad, double* ms_total);
 
 /* Device times of the last lapw1gpu_forces call on the context, in the
  * fields of lapw1gpu_stats: ms_total the whole call, ms_albl the operands

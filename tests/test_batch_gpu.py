@@ -124,3 +124,34 @@ def test_autotune_keeps_results_exact(ctx, prec, slices):
     kp.free()
     ctx.set_tuning(hns_diag_b=512, split_group=16, sph_tc=1)
     ctx.set_precision(lapw1gpu.PREC_FP64)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [lapw1gpu.PREC_FP64, lapw1gpu.PREC_SPLIT])
+def test_forces_batch_equals_single_calls(ctx, prec):
+    """lapw1gpu_forces_batch queues the adjoint of uneven k-points back to
+    back; every gradient is the single call's to 1e-12 of its largest
+    component (the force kernels sum over pair tiles with atomic adds, whose
+    order varies from run to run)."""
+    from hack_wein2k_b200 import forces as FO
+    dev = torch.device("cuda", ctx.device)
+    probs = [synth.small_case(k) for k in ("lo", "apw", "ins", "gamma")]
+    nb = 6
+    occ = torch.ones(nb, dtype=torch.float64, device=dev)
+    setup = [FO.band_energy(ctx, p, occ) for p in probs]  # (E, eps, X, kp), FP64 setup
+    ctx.set_precision(prec, 5)
+    try:
+        ref = [FO.gradient(ctx, kp, X, occ, w).cpu().numpy() for (_, w, X, kp) in setup]
+        xs = [X.transpose(0, 1).contiguous() for (_, _, X, _) in setup]
+        ws = [w.contiguous() for (_, w, _, _) in setup]
+        gs = [torch.full((p.ndf, 3), np.nan, dtype=torch.float64, device=dev) for p in probs]
+        torch.cuda.synchronize()
+        ms = ctx.forces_batch([kp for (_, _, _, kp) in setup], [x.data_ptr() for x in xs], [p.n for p in probs],
+                              nb, occ.data_ptr(), [w.data_ptr() for w in ws], [g.data_ptr() for g in gs])
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+        for (_, _, _, kp) in setup:
+            kp.free()
+    assert ms > 0
+    for g, r in zip(gs, ref):
+        assert np.abs(g.cpu().numpy() - r).max() <= 1e-12 * np.abs(r).max()

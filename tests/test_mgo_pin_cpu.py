@@ -144,3 +144,32 @@ def test_eigenvalues_match_printed_through_the_oracle(case, block):
     e0 = np.array(case.eig[block]["eig"])
     assert len(w) == len(e0)
     assert np.abs(w - e0).max() <= TOL_EIG_RY, np.abs(w - e0).max()
+
+
+def test_vector_file_round_trip(case):
+    """case.vector as lapw1 writes it (inilpw.f:440-445, tapewf.F:44-59):
+    the header records of every atom, then per k-point the k line, the KZZ
+    of all HSROWS rows and each state's energy and conjugated eigenvector,
+    every record framed by its 4-byte length; read back unchanged."""
+    import io
+    import struct
+
+    from hack_wein2k_b200 import vector_file as VF
+    p = case.problem(0)
+    hs, hsd = O.setup(p)
+    H, S = hermitian_from_packed(hs, hsd)
+    w, Z = scipy.linalg.eigh(H, S)
+    sel = (w > case.in1.emin) & (w < case.in1.emax)
+    w, Z = w[sel], Z[:, sel]
+    buf = io.BytesIO()
+    VF.write_header(buf, p.e, p.elo)
+    VF.write_kpoint(buf, p.meta["k"], "1", p.kzz, w, Z, 1.0, "")
+    raw = buf.getvalue()
+    assert struct.unpack("<i", raw[:4])[0] == 8 * p.e.shape[1]          # E(1:LMAX) of atom 1
+    head, kps = VF.read_vector(io.BytesIO(raw), p.nat)
+    assert np.array_equal(head[0][0], p.e[0]) and np.array_equal(head[1][1], p.elo[1].reshape(-1))
+    (kp,) = kps
+    assert kp["kzz"].shape == (p.n, 3) and np.array_equal(kp["kzz"], p.kzz)
+    assert np.array_equal(kp["eig"], w) and np.array_equal(kp["z"], Z)
+    lines = VF.energy_lines(p.meta["k"], "1", p.n, w, 1.0)
+    assert len(lines) == 1 + len(w) and len(lines[0]) == 3 * 19 + 10 + 12 + 5 + 3
