@@ -961,7 +961,7 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
       double2* T = (double2*)c->sbuf(set, "hnsLoT", sizeof(double2) * (size_t)k->nlo * k->nlo);
       if (!T) return LAPW1GPU_ERR_NOMEM;
       rc = split_rect_gemm(c, k, set, k->nlo, k->nlo, ndf * nsl2, C2lo, k->nlo, Clo, k->nlo, T, k->nlo,
-                           c->slices_hns, a, &nl, 1);
+                           c->slices_hns, a, &nl, 1, "lorect");
     }
     if (rc) return rc;
     CK(cudaEventRecord(c->auxj[set], a));

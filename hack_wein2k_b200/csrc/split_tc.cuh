@@ -529,15 +529,16 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
 template <int S>
 static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
                            const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
-                           cudaStream_t s, int* nlaunch, int ovw) {
+                           cudaStream_t s, int* nlaunch, int ovw, const char* tag) {
   using Cf = split::Cfg<S>;
   const int Kcp = (Kc + 63) / 64 * 64;
   const int Kp = 2 * Kcp;
   const int npL = (npadL + 127) / 128 * 128, npR = (npadR + 127) / 128 * 128;
-  int8_t* A = (int8_t*)c->sbuf(set, "rectA", (size_t)S * npL * Kp);
-  int8_t* B = (int8_t*)c->sbuf(set, "rectB", (size_t)S * 2 * npR * Kp);
-  int* exA = (int*)c->sbuf(set, "rectExA", sizeof(int) * npL);
-  int* exB = (int*)c->sbuf(set, "rectExB", sizeof(int) * npR);
+  const std::string t(tag);
+  int8_t* A = (int8_t*)c->sbuf(set, (t + "A").c_str(), (size_t)S * npL * Kp);
+  int8_t* B = (int8_t*)c->sbuf(set, (t + "B").c_str(), (size_t)S * 2 * npR * Kp);
+  int* exA = (int*)c->sbuf(set, (t + "ExA").c_str(), sizeof(int) * npL);
+  int* exB = (int*)c->sbuf(set, (t + "ExB").c_str(), sizeof(int) * npR);
   if (!A || !B || !exA || !exB) return LAPW1GPU_ERR_NOMEM;
   if (cudaMemsetAsync(exA, 0x80, sizeof(int) * npL, s) != cudaSuccess ||
       cudaMemsetAsync(exB, 0x80, sizeof(int) * npR, s) != cudaSuccess)
@@ -569,17 +570,20 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
   return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
+// tag: the prefix of the scratch buffers (callers whose products differ
+// much in size keep separate ones, so that growing one never reallocates
+// a buffer that a captured batch uses)
 static int split_rect_gemm(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int m, int nr, int Kc,
                            const double2* Lop, int npadL, const double2* Rop, int npadR, double2* out, int ld,
-                           int slices, cudaStream_t s, int* nlaunch, int ovw = 0) {
+                           int slices, cudaStream_t s, int* nlaunch, int ovw = 0, const char* tag = "rect") {
   switch (slices) {
-    case 2: return split_gemm_rect<2>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 3: return split_gemm_rect<3>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
-    case 8: return split_gemm_rect<8>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw);
+    case 2: return split_gemm_rect<2>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 3: return split_gemm_rect<3>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 4: return split_gemm_rect<4>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 5: return split_gemm_rect<5>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 6: return split_gemm_rect<6>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 7: return split_gemm_rect<7>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
+    case 8: return split_gemm_rect<8>(c, k, set, m, nr, Kc, Lop, npadL, Rop, npadR, out, ld, s, nlaunch, ovw, tag);
     default: return LAPW1GPU_ERR_RANGE;
   }
 }
