@@ -577,6 +577,7 @@ def north_star(args):
 
     # ---- c1: the 40-atom single k-point (the line of the first build) ----
     c1 = c1_summary(ctx, torch, dev, stream) if not args.no_extras else None
+    c2 = c2_batch(ctx, torch, dev, stream) if not args.no_extras else None
 
     # ---- roofline of the dominant kernel (split arm, per k-point) ----
     clocks = clk.summary()
@@ -670,6 +671,8 @@ def north_star(args):
     }
     if c1 is not None:
         line["c1"] = c1
+    if c2 is not None:
+        line["c2_batch"] = c2
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -770,6 +773,44 @@ def c1_summary(ctx, torch, dev, stream):
             out[prec]["k_sph_tc_int8_tops"] = sph_tc_ops(p, 5) / (st["ms_sph_main"] * 1e-3) / 1e12
     kp.free()
     return out
+
+
+def c2_batch(ctx, torch, dev, stream):
+    """c2 (c1's cell at 64 k-points): the k-list set up as one batch (one
+    graph launch, concurrent chains tuned) against 64 single-k-point calls."""
+    from hack_wein2k_b200 import lapw1gpu, synth
+    ps = synth.config("c2")
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    ctx.set_slices(5, 4)
+    kps = [ctx.upload(q) for q in ps]
+    hs = [torch.empty((q.n, q.n), dtype=torch.complex128, device=dev) for q in ps]
+    hd = [torch.empty(q.n, dtype=torch.complex128, device=dev) for q in ps]
+    bargs = (kps, [t.data_ptr() for t in hs], [q.n for q in ps], [t.data_ptr() for t in hd])
+    tun = ctx.autotune(kps[0], hs[0].data_ptr(), ps[0].n, hd[0].data_ptr())
+    per_sets = {}
+    for sets in (1, 2, 3):
+        ctx.set_tuning(batch_sets=sets)
+        ctx.setup_batch(*bargs)  # eager pass + capture
+        per_sets[sets] = min(ctx.setup_batch(*bargs)["ms_total"] for _ in range(3)) / len(ps)
+    best = min(per_sets, key=per_sets.get)
+    ctx.set_tuning(batch_sets=best)
+
+    def singles():
+        for i, k in enumerate(kps):
+            k.run(hs[i].data_ptr(), ps[i].n, hd[i].data_ptr())
+
+    singles()
+    ms_single = min(_timed_loop(torch, stream, singles, 1) for _ in range(2)) / len(ps)
+    for k in kps:
+        k.free()
+    del hs, hd
+    torch.cuda.empty_cache()
+    return {"workload": "c2: c1's cell at 64 seeded k-points, split 5/4", "nk": len(ps),
+            "n_range": [min(q.n for q in ps), max(q.n for q in ps)],
+            "batch_ms_per_kpoint": per_sets[best], "batch_sets": best,
+            "batch_ms_per_kpoint_by_sets": per_sets, "single_calls_ms_per_kpoint": ms_single,
+            "gain": ms_single / per_sets[best],
+            "tuning": {k: v for k, v in tun.items() if k in ("split_group", "sph_tc", "sph_kblock")}}
 
 
 def fd_report(args):

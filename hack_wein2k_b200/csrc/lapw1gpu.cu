@@ -81,6 +81,7 @@ struct lapw1gpu_context {
   int hns_diag_b = 512;    // FP64 HNS: diagonal block of the blocked ZHER2M form
   int split_group = 16;    // split HNS: row tiles per rasterisation group
   int sph_tc = 1;          // split precision: spherical part on tcgen05 (1) or FP64 (0)
+  int sph_kb = 64;         // k_sph_tc: bytes of K per pipeline stage (64: deep ring, 128: two stages)
   int batch_sets = 2;      // concurrent k-point chains in a batch
   int test_never_wait = 0; // test hook: the spherical tensor kernel's consumer wait runs out
   int last_launches = 0;   // kernels launched by the last call (a library product counts as one)
@@ -779,15 +780,15 @@ static int hns_panels_zgemm(cublasHandle_t h, int n, int nv, int npad, int K, in
 }  // extern "C"
 
 // Spherical part on tcgen05 (sph_tc.cuh): slice the per-l operands, then
-// one CTA per (128 J, IT I) tile of the triangle.
-template <int S, int LS>
+// one CTA per (128 J, IT I) tile of the triangle; KB bytes of K per stage.
+template <int S, int LS, int KB>
 static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const DevProb& P, const SphCoef* coef,
                          const double2* tab, double2* hs, int ld, double2* hsdiag, cudaStream_t s, int* nl,
                          const cudaEvent_t* ev, HnsPipe* sp) {
-  using Cf = sphtc::Cfg<S>;
+  using Cf = sphtc::Cfg<S, KB>;
   const int nv = k->nv, L = k->ltop, Kc = 2 * k->ndf;
   // Kp: whole 32-byte MMA steps; the tensor map's K extent is Kp, so the
-  // last 64-byte TMA block of an odd step count reads zero fill past it
+  // last KB-byte TMA block reads zero fill past it
   const int Kcp = round_up(Kc, 16), Kp = 2 * Kcp;
   const int npA = round_up(nv, 128), npB = round_up(nv, Cf::IT);
   int8_t* A = (int8_t*)c->sbuf(set, "sphA", (size_t)S * L * npA * Kp);
@@ -805,8 +806,8 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   if (ev && cudaEventRecord(c->ev[21], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   *nl += 2;
   CUtensorMap ta, tb;
-  if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, 64) ||
-      l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N, 64))
+  if (l1g_tmap_3d(&ta, A, Kp, (uint64_t)L * npA, S, 128, KB) ||
+      l1g_tmap_3d(&tb, B, Kp, (uint64_t)L * 4 * npB, S, Cf::N, KB))
     return LAPW1GPU_ERR_CUDA;
   int ntile = 0;
   // I tiles outer: the CTAs resident at one time share few I tiles (B
@@ -820,7 +821,7 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
                                   if (bj * 128 <= bi * Cf::IT + Cf::IT - 1) t.push_back(make_int2(bj, bi));
                             });
   if (!dt) return LAPW1GPU_ERR_NOMEM;
-  if (!c->smem((const void*)sphtc::k_sph_tc<S, LS>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
+  if (!c->smem((const void*)sphtc::k_sph_tc<S, LS, KB>, Cf::SMEM)) return LAPW1GPU_ERR_CUDA;
   if (ev && cudaEventRecord(ev[0], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   // tiles are ordered by the I tile (column of S); per I tile bi the J tiles
   // bj with bj 128 <= bi IT + IT - 1, so a column group is a contiguous range
@@ -838,9 +839,10 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
     if (t1 > t0) {
       // persistent: one CTA per SM over the group's tiles
       const int grid = (int)std::min<long>(t1 - t0, c->nsm);
-      sphtc::k_sph_tc<S, LS><<<grid, Cf::THREADS, Cf::SMEM, s>>>(
-          ta, tb, P, dt + t0, (int)(t1 - t0), (Kp + 63) / 64, (Kp % 64) != 0, npA, npB, exA, exB, tab, k->tab, hs,
-          ld, hsdiag, c->d_status, c->test_never_wait);
+      const int nkb = (Kp + KB - 1) / KB, klast = (Kp - (nkb - 1) * KB) / 32;
+      sphtc::k_sph_tc<S, LS, KB><<<grid, Cf::THREADS, Cf::SMEM, s>>>(ta, tb, P, dt + t0, (int)(t1 - t0), nkb, klast,
+                                                                      npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag,
+                                                                      c->d_status, c->test_never_wait);
       *nl += 1;
     }
     if (sp && sp->col[g + 1] <= k->nv) {
@@ -873,20 +875,27 @@ static int sph_tc_dispatch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, con
                            const cudaEvent_t* ev, HnsPipe* sp) {
   const int Kp = 2 * round_up(2 * k->ndf, 16);
   const int mode = sph_level_mode(c->slices, Kp);
-#define SPH_CASE(SS)                                                                               \
-  case SS:                                                                                         \
-    return mode == 2   ? sph_tc_launch<SS, 2>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
-           : mode == 1 ? sph_tc_launch<SS, 1>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
-                       : sph_tc_launch<SS, 0>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp);
+  // 128-byte K blocks fit two stages up to 5 slices
+  const bool kb128 = c->sph_kb == 128 && c->slices <= 5;
+#define SPH_MODES(SS, KB)                                                                             \
+  return mode == 2   ? sph_tc_launch<SS, 2, KB>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
+         : mode == 1 ? sph_tc_launch<SS, 1, KB>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp) \
+                     : sph_tc_launch<SS, 0, KB>(c, k, set, P, coef, tab, hs, ld, hsdiag, s, nl, ev, sp);
   switch (c->slices) {
-    SPH_CASE(4)
-    SPH_CASE(5)
-    SPH_CASE(6)
-    SPH_CASE(7)
+    case 4:
+      if (kb128) SPH_MODES(4, 128)
+      SPH_MODES(4, 64)
+    case 5:
+      if (kb128) SPH_MODES(5, 128)
+      SPH_MODES(5, 64)
+    case 6:
+      SPH_MODES(6, 64)
+    case 7:
+      SPH_MODES(7, 64)
     default:
       return LAPW1GPU_ERR_RANGE;
   }
-#undef SPH_CASE
+#undef SPH_MODES
 }
 
 // algorithmic FP64-equivalent flops of the contractions
@@ -1197,7 +1206,7 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
   std::vector<uintptr_t> key = {(uintptr_t)nk,         (uintptr_t)stages,        (uintptr_t)c->prec,
                                 (uintptr_t)(c->slices * 16 + c->slices_hns), (uintptr_t)c->hns_diag_b,
                                 (uintptr_t)c->split_group,
-                                (uintptr_t)c->sph_tc,  (uintptr_t)c->batch_sets,
+                                (uintptr_t)c->sph_tc,  (uintptr_t)c->sph_kb, (uintptr_t)c->batch_sets,
                                 (uintptr_t)c->test_never_wait};
   for (int i = 0; i < nk; i++) {
     key.push_back((uintptr_t)kps[i]);
@@ -1267,6 +1276,7 @@ int lapw1gpu_get_tuning(lapw1gpu_context* c, lapw1gpu_tuning* t) {
   t->split_group = c->split_group;
   t->sph_tc = c->sph_tc;
   t->batch_sets = c->batch_sets;
+  t->sph_kblock = c->sph_kb;
   t->ms_best = 0.0;
   return LAPW1GPU_OK;
 }
@@ -1274,12 +1284,14 @@ int lapw1gpu_get_tuning(lapw1gpu_context* c, lapw1gpu_tuning* t) {
 int lapw1gpu_set_tuning(lapw1gpu_context* c, const lapw1gpu_tuning* t) {
   if (!c || !t) return LAPW1GPU_ERR_ARG;
   if (t->hns_diag_b < HNS_T || t->hns_diag_b % HNS_T || t->split_group < 1 || t->batch_sets < 1 ||
-      t->batch_sets > L1G_MAX_SETS || (t->sph_tc != 0 && t->sph_tc != 1))
+      t->batch_sets > L1G_MAX_SETS || (t->sph_tc != 0 && t->sph_tc != 1) ||
+      (t->sph_kblock != 64 && t->sph_kblock != 128))
     return LAPW1GPU_ERR_RANGE;
   c->hns_diag_b = t->hns_diag_b;
   c->split_group = t->split_group;
   c->sph_tc = t->sph_tc;
   c->batch_sets = t->batch_sets;
+  c->sph_kb = t->sph_kblock;
   return LAPW1GPU_OK;
 }
 
@@ -1326,6 +1338,9 @@ int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, in
     rc = tune(&c->hns_diag_b, {256, 512, 1024, 2048}, &ms);
   } else {
     if (sph_tc_supported(c->slices)) rc = tune(&c->sph_tc, {1, 0}, &ms);
+    // the K block (and with it the ring depth) of k_sph_tc: 128-byte blocks
+    // exist up to 5 slices
+    if (!rc && c->sph_tc && c->slices <= 5) rc = tune(&c->sph_kb, {64, 128}, &ms);
     if (!rc) rc = tune(&c->split_group, {4, 8, 16, 32}, &ms);
   }
   if (rc) return rc;

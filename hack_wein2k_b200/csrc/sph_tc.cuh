@@ -31,7 +31,7 @@
 
 namespace sphtc {
 
-using split::desc_sw64;
+using split::desc_kblock;
 using split::digit7;
 using split::digit_scale;
 using split::i2d_exact;
@@ -45,7 +45,10 @@ using split::tc_fence_after;
 using split::tc_fence_before;
 using split::tma_load_3d;
 
-template <int S>
+// KB: bytes of K per pipeline stage and row (64: 64-byte swizzled rows, a
+// deep ring; 128: 128-byte swizzled rows, half the TMA row requests per
+// byte, two stages) -- a tunable tile shape
+template <int S, int KB = 64>
 struct Cfg {
   // real columns per level of one accumulator buffer: 4 per I, at most 48
   // (12 I: three epilogue warp groups of 4 I)
@@ -57,15 +60,18 @@ struct Cfg {
   static constexpr int EG = IT / IPT;  // epilogue warp groups (4 warps each: the 4 TMEM lane quarters)
   static_assert(EG * IPT == IT, "I per tile must be a multiple of 4");
   static constexpr int EPI = 128 * EG;  // epilogue threads
-  // one pipeline stage: all S slices of a 64-byte K block of A (128 rows)
+  // one pipeline stage: all S slices of a KB-byte K block of A (128 rows)
   // and of B (N rows)
-  static constexpr int A_BYTES = S * 128 * 64;
-  static constexpr int B_BYTES = S * N * 64;
+  static_assert(KB == 64 || KB == 128, "K block of 64 or 128 bytes");
+  static constexpr int KSTEPS = KB / 32;  // 32-byte MMA K steps per stage
+  static constexpr int A_BYTES = S * 128 * KB;
+  static constexpr int B_BYTES = S * N * KB;
   static constexpr int STAGE = A_BYTES + B_BYTES;
   // per-tile exponent tables: eA - 12 per (l, J) and eB per (l, I, S|H), int16
   static constexpr int SCALE_BYTES = (SPH_LMAX * 128 + SPH_LMAX * 2 * IT) * 2;
   static constexpr int STAGES_FIT = (227 * 1024 - SCALE_BYTES - 1024) / STAGE;
   static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
+  static_assert(STAGES >= 2, "the ring needs two stages");
   static constexpr int SMEM = STAGES * STAGE + SCALE_BYTES + 1024;
   static constexpr int THREADS = EPI + 64;  // + the MMA warp and the TMA warp
 };
@@ -254,14 +260,14 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, co
 // stage ring and the two accumulator buffers run on counters that continue
 // across tiles, so the loads and MMAs of a tile's first l overlap the
 // previous tile's last epilogue, interstitial gather and HS writes.
-template <int S, int LS>
-__global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
+template <int S, int LS, int KB>
+__global__ void __launch_bounds__(Cfg<S, KB>::THREADS, 1)
     k_sph_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, DevProb P,
-             const int2* __restrict__ tiles, int ntile, int nkb, int khalf, int npA, int npB,
+             const int2* __restrict__ tiles, int ntile, int nkb, int klast, int npA, int npB,
              const int* __restrict__ exA, const int* __restrict__ exB, const double2* __restrict__ tab, TabDesc T,
              double2* __restrict__ hs, int ld, double2* __restrict__ hsdiag, int* __restrict__ status,
              int never_wait) {
-  using C = Cfg<S>;
+  using C = Cfg<S, KB>;
   constexpr int N = C::N, IT = C::IT, STAGES = C::STAGES, HALF = C::IPT, EPI = C::EPI;
   constexpr int MMA_WARP = 4 * C::EG, TMA_WARP = 4 * C::EG + 1;
   extern __shared__ uint8_t smem_raw[];
@@ -325,8 +331,8 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
           uint8_t* a = smem + st * C::STAGE;
           uint8_t* b = a + C::A_BYTES;
           mbar_expect_tx(&full[st], C::STAGE);
-          tma_load_3d(a, &tmA, &full[st], kb * 64, l * npA + j0, 0);
-          tma_load_3d(b, &tmB, &full[st], kb * 64, l * 4 * npB + 4 * i0, 0);
+          tma_load_3d(a, &tmA, &full[st], kb * KB, l * npA + j0, 0);
+          tma_load_3d(b, &tmB, &full[st], kb * KB, l * 4 * npB + 4 * i0, 0);
         }
       }
       if (!ok) atomicOr(status, L1G_STATUS_TIMEOUT);
@@ -370,17 +376,17 @@ __global__ void __launch_bounds__(Cfg<S>::THREADS, 1)
           // The S slices of B lie one after another in shared memory (one
           // (S N)-row K-major tile) and the level accumulators N columns
           // apart in TMEM, so A slice p times B slices 0..S-1-p is ONE MMA
-          // of width (S-p) N whose columns land on levels p..S-1.  When K
-          // is an odd number of 32-byte steps the last block holds one step
-          // (TMA zero-fills the rest; its MMA half is skipped).
-          const int nh = (khalf && kb == nkb - 1) ? 1 : 2;
+          // of width (S-p) N whose columns land on levels p..S-1.  The last
+          // block holds klast valid 32-byte steps (TMA zero-fills the rest;
+          // their MMAs are skipped).
+          const int nh = (kb == nkb - 1) ? klast : C::KSTEPS;
 #pragma unroll
           for (int p = 0; p < S; p++)
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
+            for (int h = 0; h < C::KSTEPS; h++) {
               if (h >= nh) continue;
-              const uint64_t ad = desc_sw64(a0 + p * 128 * 64 + h * 32);
-              const uint64_t bd = desc_sw64(b0 + h * 32);
+              const uint64_t ad = desc_kblock<KB>(a0 + p * 128 * KB + h * 32);
+              const uint64_t bd = desc_kblock<KB>(b0 + h * 32);
               const uint32_t acc = (kb > 0 || h > 0 || p > 0) ? 1u : 0u;
               const uint32_t d = tmem + (uint32_t)(buf * S * N + p * N);
               asm volatile(

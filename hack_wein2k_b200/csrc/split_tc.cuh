@@ -115,6 +115,22 @@ __device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
   d |= (uint64_t)4 << 61;              // SWIZZLE_64B
   return d;
 }
+// K-major operand tile, 128-byte swizzle: rows of 128 B, 8-row groups 1024 B
+// apart (the tile base 1024-byte aligned; a K step inside the row advances
+// the start address by 32 B, the swizzle acting on the absolute address)
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+  return d;
+}
+// the descriptor of a K block of KB bytes per row (64 or 128)
+template <int KB>
+__device__ __forceinline__ uint64_t desc_kblock(uint32_t saddr) {
+  return KB == 128 ? desc_sw128(saddr) : desc_sw64(saddr);
+}
 // instruction descriptor: D s32, A s8, B s8, both K-major, M x N
 __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
@@ -431,8 +447,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 l1g_encode_fn() {
 }
 
 // 3-D map over [S][rows][kp] int8 slice planes; a box is all S slices of
-// box_rows rows and `inner` bytes of K (64 with 64-byte swizzle, 32 with
-// 32-byte swizzle)
+// box_rows rows and `inner` bytes of K (128, 64 or 32: the swizzle of
+// that width)
 static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t rows, uint64_t S, uint32_t box_rows,
                        uint32_t inner = 64) {
   auto enc = l1g_encode_fn();
@@ -442,7 +458,10 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
   cuuint32_t box[3] = {inner, box_rows, (cuuint32_t)S};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, inner == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   inner == 128  ? CU_TENSOR_MAP_SWIZZLE_128B
+                   : inner == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                 : CU_TENSOR_MAP_SWIZZLE_64B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }

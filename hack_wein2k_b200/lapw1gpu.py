@@ -46,7 +46,7 @@ class Tuning(C.Structure):
     """ctypes mirror of `lapw1gpu_tuning`."""
 
     _fields_ = [("hns_diag_b", C.c_int), ("split_group", C.c_int), ("sph_tc", C.c_int),
-                ("batch_sets", C.c_int), ("ms_best", C.c_double)]
+                ("batch_sets", C.c_int), ("sph_kblock", C.c_int), ("ms_best", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

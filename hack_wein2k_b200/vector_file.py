@@ -11,6 +11,11 @@ lapw1 does, so that the rest of a WIEN2k run takes them unchanged:
                                    rows; per state I, E(I) and the
                                    conjugated eigenvector (complex build)
   energy_lines   tapewf.F:46,50    the formatted twin (case.energy)
+  write_nsh      atpar.f:112-115,345,563-570, forfhs.f:26-69
+                                   case.nsh (unit 71, read by lapw2's
+                                   force terms): per atom the Gaunt
+                                   factor x non-spherical radial integral
+                                   of every LQNS entry
 
 case.vector is a Fortran sequential unformatted file: every record is
 framed by its byte length as a 4-byte integer before and after (the
@@ -125,3 +130,74 @@ def read_vector(f: BinaryIO, nat: int):
             z[:, i] = np.conj(np.frombuffer(rec(), dtype="<c16"))
         kps.append(dict(k=(sx, sy, sz), kname=kname, weight=w, ipgr=ipgr, kzz=kzz, eig=eig, z=z))
     return head, kps
+
+
+def _nsh_pair(v) -> str:
+    return _e19(v.real) + _e19(v.imag)
+
+
+def write_nsh(f, rads, lomax: int = 3) -> None:
+    """case.nsh from the host ATPAR's per-atom Gaunt lists and radial
+    integrals (hack_wein2k_b200.atpar.AtomRadial): the header, then per
+    atom its ' .Atom' line, for every LQNS entry (l0, ll, lp, m, mm, mp)
+    the products GFAC x (uVu, dVd, uVd, dVu) and, when l0 or lp carries a
+    local orbital, GFAC x (loVu 21, loVu 12, loVlo 22, loVd 21, loVd 12),
+    and a closing line of zeros.  f: a text stream."""
+    f.write(" non-spherical Matrixelements x Gaunt-Coefficient (d=du/dE):\n"
+            " l0 ll lp m0 mm mp     uVu dVd\n"
+            "                       uVd dVu\n")
+    pad = " " * 18
+    zero = 0j
+    for ja, rad in enumerate(rads):
+        f.write(f"{ja + 1:3d} .Atom \n")
+        for (l0, ll, lp, lm1, m, mp, g) in rad.gaunts:
+            uvu, dvd, uvd = rad.vns[(l0, lm1, lp)]
+            dvu = rad.vns[(lp, lm1, l0)][2]
+            mm = rad.lm[lm1 - 1][1]
+            f.write(f"{l0:3d}{ll:3d}{lp:3d}{m:3d}{mm:3d}{mp:3d}" + _nsh_pair(g * uvu) + _nsh_pair(g * dvd) + "\n")
+            f.write(pad + _nsh_pair(g * uvd) + _nsh_pair(g * dvu) + "\n")
+            if l0 <= lomax or lp <= lomax:
+                t21 = t12 = t22 = d21 = d12 = zero
+                lo0 = l0 <= lomax and bool(rad.loor[l0])
+                if lo0:
+                    lv = rad.vnslo[(l0, lm1, lp)]
+                    t21, d21 = g * lv[0], g * lv[1]
+                if lp <= lomax and bool(rad.loor[lp]):
+                    lv = rad.vnslo[(lp, lm1, l0)]
+                    if lo0:
+                        t22 = g * rad.vnslo[(l0, lm1, lp)][2]
+                    t12, d12 = g * lv[0], g * lv[1]
+                f.write(pad + _nsh_pair(t21) + _nsh_pair(t12) + _nsh_pair(t22) + "\n")
+                f.write(pad + _nsh_pair(d21) + _nsh_pair(d12) + "\n")
+        f.write("".join(f"{0:3d}" for _ in range(6)) + _e19(0.0) * 4 + "\n" + pad + _e19(0.0) * 4 + "\n")
+
+
+def read_nsh(f):
+    """Parse a case.nsh written by write_nsh (or lapw1): {atom: [entry]},
+    entry = dict(idx=(l0, ll, lp, m, mm, mp), t=[tuu, tdd, tud, tdu],
+    lo=[tuu21, tuu12, tuu22, tud21, tdu12] or None).  lo lines follow an
+    entry exactly when l0 or lp is at most lomax (3)."""
+    lines = f.read().splitlines()[3:]
+    out, atom, i = {}, None, 0
+
+    def cvals(s, n):
+        return [complex(float(s[19 * (2 * k):19 * (2 * k + 1)]), float(s[19 * (2 * k + 1):19 * (2 * k + 2)]))
+                for k in range(n)]
+    while i < len(lines):
+        ln = lines[i]
+        if ln.strip().endswith(".Atom"):
+            atom = int(ln.split()[0])
+            out[atom] = []
+            i += 1
+            continue
+        idx = tuple(int(ln[3 * k:3 * k + 3]) for k in range(6))
+        t = cvals(ln[18:], 2) + cvals(lines[i + 1][18:], 2)
+        i += 2
+        if idx == (0,) * 6 and all(v == 0 for v in t):
+            continue
+        lo = None
+        if idx[0] <= 3 or idx[2] <= 3:
+            lo = cvals(lines[i][18:], 3) + cvals(lines[i + 1][18:], 2)
+            i += 2
+        out[atom].append(dict(idx=idx, t=t, lo=lo))
+    return out

@@ -323,6 +323,9 @@ typedef struct {
   int split_group;  /* split HNS: row tiles per L2 rasterisation group           */
   int sph_tc;       /* split: spherical part on tcgen05 (1) or FP64 (0)          */
   int batch_sets;   /* concurrent k-point chains in a batch (1..4)               */
+  int sph_kblock;   /* split: K bytes per k_sph_tc pipeline stage, 64 (four-deep
+                       ring of 64-byte swizzled rows) or 128 (two stages of
+                       128-byte rows; up to 5 slices, else 64 is used)        */
   double ms_best;   /* setup time of the tuned k-point with the choices, ms      */
 } lapw1gpu_tuning;
 int lapw1gpu_get_tuning(lapw1gpu_context* ctx, lapw1gpu_tuning* t);

@@ -116,6 +116,7 @@ def test_autotune_keeps_results_exact(ctx, prec, slices):
     t = ctx.autotune(kp, hs[0].data_ptr(), p.n, hd[0].data_ptr())
     assert t["hns_diag_b"] in (256, 512, 1024, 2048)
     assert t["split_group"] in (4, 8, 16, 32) and t["sph_tc"] in (0, 1) and t["ms_best"] > 0
+    assert t["sph_kblock"] in (64, 128)
     kp.run(hs[0].data_ptr(), p.n, hd[0].data_ptr(), stats=True)
     hs_o, hd_o = O.setup(p)
     err = rel_errors(_host(hs[0]), hd[0].cpu().numpy(), hs_o, hd_o)

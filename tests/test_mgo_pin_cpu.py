@@ -173,3 +173,31 @@ def test_vector_file_round_trip(case):
     assert np.array_equal(kp["eig"], w) and np.array_equal(kp["z"], Z)
     lines = VF.energy_lines(p.meta["k"], "1", p.n, w, 1.0)
     assert len(lines) == 1 + len(w) and len(lines[0]) == 3 * 19 + 10 + 12 + 5 + 3
+
+
+def test_nsh_file_round_trip(case):
+    """case.nsh as ATPAR/FORFHS write it for lapw2's forces (atpar.f:112,
+    345, 563-570; forfhs.f:26-69): one entry per LQNS Gaunt factor of each
+    atom, GFAC times the radial integrals, LO lines where l0 or lp <= LOMAX;
+    read back to the 12 printed digits.  The factors themselves are pinned
+    to lapw1's own print by the Gaunt/integral test above."""
+    import io
+
+    from hack_wein2k_b200 import vector_file as VF
+    buf = io.StringIO()
+    VF.write_nsh(buf, case.rads)
+    text = buf.getvalue()
+    assert text.splitlines()[0].startswith(" non-spherical Matrixelements x Gaunt-Coefficient")
+    got = VF.read_nsh(io.StringIO(text))
+    assert sorted(got) == [1, 2]
+    for ja, rad in enumerate(case.rads):
+        ents = got[ja + 1]
+        assert len(ents) == len(rad.gaunts) > 0
+        for e, (l0, ll, lp, lm1, m, mp, g) in zip(ents, rad.gaunts):
+            assert e["idx"] == (l0, ll, lp, m, rad.lm[lm1 - 1][1], mp)
+            uvu, dvd, uvd = rad.vns[(l0, lm1, lp)]
+            want = [g * uvu, g * dvd, g * uvd, g * rad.vns[(lp, lm1, l0)][2]]
+            assert all(abs(x - y) <= 1e-11 * max(1.0, abs(y)) for x, y in zip(e["t"], want)), (e, want)
+            assert (e["lo"] is not None) == (l0 <= 3 or lp <= 3)
+            if e["lo"] is not None and l0 <= 3 and rad.loor[l0]:
+                assert abs(e["lo"][0] - g * rad.vnslo[(l0, lm1, lp)][0]) <= 1e-11 * max(1.0, abs(e["lo"][0]))

@@ -181,3 +181,25 @@ def test_split_stages_compose(sctx, kind):
     finally:
         kp.free()
         sctx.set_precision(lapw1gpu.PREC_SPLIT, 7)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slices", [4, 5])
+@pytest.mark.parametrize("case", ["lo", "manyeq", "c1"])
+def test_sph_tc_kblock_shapes_agree(sctx, slices, case):
+    """k_sph_tc with 128-byte K blocks (two-stage ring) against the 64-byte
+    default: the level sums are exact int32 sums, so the two tile shapes
+    give the same bits; both within the slice count's bound of the oracle."""
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
+    p = synth.config("c1")[0] if case == "c1" else synth.small_case(case)
+    try:
+        sctx.set_tuning(sph_kblock=64)
+        hs64, hsd64 = sctx.setup(p)
+        sctx.set_tuning(sph_kblock=128)
+        hs128, hsd128 = sctx.setup(p)
+    finally:
+        sctx.set_tuning(sph_kblock=64)
+    assert np.array_equal(hs64, hs128) and np.array_equal(hsd64, hsd128)
+    hs_o, hsd_o = O.setup(p)
+    err = rel_errors(hs128, hsd128, hs_o, hsd_o)
+    assert err["S"] <= TOL_H[slices] and err["H"] <= TOL_H[slices], err
