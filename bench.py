@@ -269,15 +269,21 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- helpers
-def _timed_loop(torch, stream, fn, steps):
+def _timed_loop(torch, stream, fn, steps, nvtx=None):
+    """CUDA-event time of `steps` calls of fn on `stream`; nvtx: the name of
+    an NVTX range around the calls (a profiler can be limited to it)"""
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)
     e0.record(stream)
     for _ in range(steps):
         fn()
     e1.record(stream)
     torch.cuda.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
     return e0.elapsed_time(e1)
 
 
@@ -381,6 +387,7 @@ def north_star(args):
         else:
             ctx.set_precision(lapw1gpu.PREC_SPLIT, s_sph)
             ctx.set_slices(s_sph, s_hns)
+            ctx.set_force_slices(*args.force_slices)
 
     def bar():
         if dist is not None:
@@ -460,7 +467,7 @@ def north_star(args):
         step()
     bar()
     with ClockSampler(local) as clk:
-        ms = _timed_loop(torch, stream, step, args.steps)
+        ms = _timed_loop(torch, stream, step, args.steps, nvtx="timed")
     bar()
     ms = maxr(ms)
     ms_step = ms / args.steps
@@ -637,7 +644,8 @@ def north_star(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": f"int8 x{s_sph}/x{s_hns}/x6 slices (spherical/HNS/adjoint products) with f64 combine; "
+        "dtype": f"int8 x{s_sph}/x{s_hns}/x{args.force_slices[0]}/x{args.force_slices[1]} slices (spherical/HNS/"
+                 "adjoint density matrices/adjoint HNS projections) with f64 combine; "
                  "f64 force pair sums",
         "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD_C4, "kpoints_per_gpu": NK, "n": [q.n for q in ps], "nv0": p0.nv,
@@ -930,6 +938,9 @@ def main():
     ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--slices-hns", type=int, default=4,
                     help="int8 slices of HNS (the non-spherical part is 1-2 orders smaller than the spherical one)")
+    ap.add_argument("--force-slices", type=int, nargs=2, default=[6, 4], metavar=("RHO", "PROJ"),
+                    help="int8 slices of the adjoint's density matrices and of its HNS projections (the "
+                         "density matrices carry the force error; 4-slice projections leave it unchanged at c4)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["c4", "c1"], default="c4")
     ap.add_argument("--fd-components", type=int, default=3,

@@ -86,10 +86,12 @@ __device__ __forceinline__ FrcChunk frc_chunk(const DevProb& P, int t0) {
 }
 
 // dynamic shared memory: two stages of type rows (J: 1, I: 2 double2 per
-// row and l) and of phases, the per-warp force partials of a chunk's atoms
-// (8 per warp and component), and -4 pi KZZ of the tile's 64 rows
+// row and l) and of phases, two buffers of the per-warp force totals of a
+// chunk's atoms (one per warp and component), and -4 pi KZZ of the tile's
+// 64 rows
+#define FRC_WARPS (FRC_THREADS / 32)
 __host__ __device__ constexpr int frc_smem_bytes(int lt) {
-  return (2 * frc_tc(lt) * lt * SPH_T * 3 + 2 * 2 * FRC_MAXA * SPH_T) * 16 + FRC_MAXA * 3 * FRC_THREADS / 4 * 8 +
+  return (2 * frc_tc(lt) * lt * SPH_T * 3 + 2 * 2 * FRC_MAXA * SPH_T) * 16 + 2 * FRC_MAXA * 3 * FRC_WARPS * 8 +
          2 * SPH_T * 4 * 8;
 }
 
@@ -102,7 +104,9 @@ __host__ __device__ constexpr int frc_smem_bytes(int lt) {
 // Legendre weights, rho, rhoE and dK of the four pairs stay in registers
 // for all types.  The type rows (k_force_rows) and the phases of a chunk
 // are copied into shared memory by cp.async one chunk ahead (double
-// buffer), one warp per 32-row segment.
+// buffer), one warp per 32-row segment.  One block barrier per chunk: the
+// per-warp force totals of a chunk go to one of two buffers and are summed
+// over the warps (and added to F) after the next chunk's barrier.
 template <int LT, bool GUARD>
 __global__ void __launch_bounds__(FRC_THREADS, 1)
     k_force_sph(DevProb P, const int2* __restrict__ tiles, const double2* __restrict__ rowJ,
@@ -113,8 +117,8 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
   double2* sJ = sm2;                       // [2][TC][LT][SPH_T]
   double2* sI = sJ + 2 * TC * LT * SPH_T;  // [2][TC][LT][SPH_T][S, H]
   double2* sP = sI + 4 * TC * LT * SPH_T;  // [2][J, I][FRC_MAXA][SPH_T]
-  double* red = reinterpret_cast<double*>(sP + 4 * FRC_MAXA * SPH_T);  // [FRC_MAXA][3][8 warps x 8]
-  double* sK = red + FRC_MAXA * 3 * (FRC_THREADS / 4);                   // [J 0..31, I 32..63][4]
+  double* red = reinterpret_cast<double*>(sP + 4 * FRC_MAXA * SPH_T);  // [2][FRC_MAXA][3][warps]
+  double* sK = red + 2 * FRC_MAXA * 3 * FRC_WARPS;                       // [J 0..31, I 32..63][4]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int2 t = tiles[blockIdx.x];
   const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
@@ -203,18 +207,29 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
     }
   }
 
+  // sum over the warps of a staged chunk's per-warp totals (red buffer rb),
+  // one thread per (atom, component)
+  auto flush = [&](int rb, int a0, int na) {
+    if (tid < na * 3) {
+      const double* r = red + ((size_t)rb * FRC_MAXA * 3 + tid) * FRC_WARPS;
+      double sacc = 0.0;
+#pragma unroll
+      for (int w = 0; w < FRC_WARPS; w++) sacc += r[w];
+      atomicAdd(&F[(a0 + tid / 3) * 3 + tid % 3], sacc);
+    }
+  };
   int st = 0;
+  int pa0 = 0, pna = 0;  // atoms of the previous chunk, flushed after this chunk's barrier
   for (int t0 = 0; t0 < nat;) {
     const int t1 = t0 + ch.ntc;
+    frc_wait<0>();    // this thread's copies of the chunk (issued one chunk earlier)
+    __syncthreads();  // every thread's copies landed; every warp is past the previous chunk
     FrcChunk nx{0, 0, 1};
-    if (t1 < nat) {
+    if (t1 < nat) {  // into the stage the previous chunk read
       nx = frc_chunk<TC>(P, t1);
       stage(st ^ 1, t1, nx);
-      frc_wait<1>();
-    } else {
-      frc_wait<0>();
     }
-    __syncthreads();
+    flush(st ^ 1, pa0, pna);
     const double2* cJ = sJ + st * TC * LT * SPH_T;
     const double2* cI = sI + st * 2 * TC * LT * SPH_T;
     const double2* cPJ = sP + st * 2 * FRC_MAXA * SPH_T;
@@ -252,11 +267,12 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
         }
       }
     };
-    // this thread's share of one atom's force (phases fj of the J rows, fi
-    // of the I rows), reduced over the lanes that share lane & 7 (their I
-    // rows): lanes 0..7 hold the warp's 8 partials
-    auto fterm = [&](const double2(&fj)[2], const double2(&fi)[2], const double(&tS)[4], const double(&tH)[4],
-                     double(&fr)[3]) {
+    // one atom's force over the warp's pairs (phases fj of the J rows, fi
+    // of the I rows): returns, in lanes 0, 8 and 16, the warp's total of
+    // components 0, 1 and 2 (a transposed reduction: six shuffles for the
+    // three components)
+    auto fterm = [&](const double2(&fj)[2], const double2(&fi)[2], const double(&tS)[4],
+                     const double(&tH)[4]) -> double {
       double g[4];
 #pragma unroll
       for (int q = 0; q < 4; q++) {
@@ -276,25 +292,27 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
       const double2 kJ0 = k2[2 * jl0], kJ1 = k2[2 * (jl0 + 8)];
       const double zI0 = k2[2 * (SPH_T + il0) + 1].x, zI1 = k2[2 * (SPH_T + il0 + 4) + 1].x;
       const double zJ0 = k2[2 * jl0 + 1].x, zJ1 = k2[2 * (jl0 + 8) + 1].x;
-      fr[0] = fma(gi0, kI0.x, fma(gi1, kI1.x, -fma(gj0, kJ0.x, gj1 * kJ1.x)));
-      fr[1] = fma(gi0, kI0.y, fma(gi1, kI1.y, -fma(gj0, kJ0.y, gj1 * kJ1.y)));
-      fr[2] = fma(gi0, zI0, fma(gi1, zI1, -fma(gj0, zJ0, gj1 * zJ1)));
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], 16);
-        fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], 8);
-      }
+      const double f0 = fma(gi0, kI0.x, fma(gi1, kI1.x, -fma(gj0, kJ0.x, gj1 * kJ1.x)));
+      const double f1 = fma(gi0, kI0.y, fma(gi1, kI1.y, -fma(gj0, kJ0.y, gj1 * kJ1.y)));
+      const double f2 = fma(gi0, zI0, fma(gi1, zI1, -fma(gj0, zJ0, gj1 * zJ1)));
+      // lanes 0..15 keep components (0, 1), lanes 16..31 (2, none); then
+      // lanes with bit 3 clear keep the first, the others the second; then
+      // the sum over lane & 7
+      const bool lo16 = (lane & 16) == 0, lo8 = (lane & 8) == 0;
+      const double k0 = (lo16 ? f0 : f2) + __shfl_xor_sync(0xffffffffu, lo16 ? f2 : f0, 16);
+      const double k1 = (lo16 ? f1 : 0.0) + __shfl_xor_sync(0xffffffffu, lo16 ? 0.0 : f1, 16);
+      double v = (lo8 ? k0 : k1) + __shfl_xor_sync(0xffffffffu, lo8 ? k1 : k0, 8);
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 2);
+      v += __shfl_xor_sync(0xffffffffu, v, 1);
+      return v;
     };
-    // staged atom slot e of the chunk: partials into red[] for the chunk's end
+    // staged atom slot e of the chunk: the warp's totals into red buffer st
     auto fstaged = [&](int e, const double(&tS)[4], const double(&tH)[4]) {
       const int b = e * SPH_T;
       const double2 fj[2] = {cPJ[b + jl0], cPJ[b + jl0 + 8]}, fi[2] = {cPI[b + il0], cPI[b + il0 + 4]};
-      double fr[3];
-      fterm(fj, fi, tS, tH, fr);
-      if (lane < 8) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) red[(e * 3 + c) * (FRC_THREADS / 4) + warp * 8 + lane] = fr[c];
-      }
+      const double v = fterm(fj, fi, tS, tH);
+      if ((lane & 7) == 0 && lane < 24) red[(((size_t)st * FRC_MAXA + e) * 3 + (lane >> 3)) * FRC_WARPS + warp] = v;
     };
     if (ch.staged && ch.na == ch.ntc) {
       // one atom per type (slot tc): the force terms of type tc - 1 are
@@ -324,30 +342,20 @@ __global__ void __launch_bounds__(FRC_THREADS, 1)
           } else {
             const double2* pa = P.phase + (size_t)(ae + e) * P.npad;
             const double2 fj[2] = {pa[j0 + jl0], pa[j0 + jl0 + 8]}, fi[2] = {pa[i0 + il0], pa[i0 + il0 + 4]};
-            double fr[3];
-            fterm(fj, fi, tS, tH, fr);
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-#pragma unroll
-              for (int o = 4; o > 0; o >>= 1) fr[c] += __shfl_xor_sync(0xffffffffu, fr[c], o);
-              if (lane == 0) atomicAdd(&F[(ae + e) * 3 + c], fr[c]);
-            }
+            const double v = fterm(fj, fi, tS, tH);
+            if ((lane & 7) == 0 && lane < 24) atomicAdd(&F[(ae + e) * 3 + (lane >> 3)], v);
           }
         }
       }
     }
-    __syncthreads();
-    if (ch.staged)  // one warp per (atom, component): 64 partials
-      for (int q = warp; q < ch.na * 3; q += FRC_THREADS / 32) {
-        double sacc = red[q * (FRC_THREADS / 4) + lane] + red[q * (FRC_THREADS / 4) + 32 + lane];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
-        if (lane == 0) atomicAdd(&F[(a0c + q / 3) * 3 + q % 3], sacc);
-      }
+    pa0 = a0c;
+    pna = ch.staged ? ch.na : 0;
     t0 = t1;
     ch = nx;
     st ^= 1;
   }
+  __syncthreads();
+  flush(st ^ 1, pa0, pna);
 }
 
 // Step-function part of the spherical force: with B(dK) = sum over pairs

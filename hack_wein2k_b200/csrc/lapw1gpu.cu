@@ -74,7 +74,8 @@ struct lapw1gpu_context {
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 5;      // int8 slices of the spherical part (split precision)
   int slices_hns = 5;  // int8 slices of the HNS update
-  int slices_frc = 6;  // int8 slices of the adjoint's density matrices and projections
+  int slices_frc = 6;  // int8 slices of the adjoint's density matrices
+  int slices_prj = 6;  // and of its HNS projections
   cublasHandle_t blas[L1G_MAX_SETS] = {};  // library ZGEMMs, one handle (and workspace) per scratch set
   cusolverDnHandle_t solver = nullptr;      // the eigen-solve (lapw1gpu_seclr4)
   // tunables (lapw1gpu_autotune)
@@ -354,10 +355,13 @@ int lapw1gpu_set_precision(lapw1gpu_context* c, int prec, int slices) {
   return LAPW1GPU_OK;
 }
 
-int lapw1gpu_set_force_slices(lapw1gpu_context* c, int slices) {
+int lapw1gpu_set_force_slices(lapw1gpu_context* c, int slices_density, int slices_projection) {
   if (!c) return LAPW1GPU_ERR_ARG;
-  if (slices < 4 || slices > L1G_MAX_SLICES) return LAPW1GPU_ERR_RANGE;
-  c->slices_frc = slices;
+  if (slices_density < 4 || slices_density > L1G_MAX_SLICES || slices_projection < 4 ||
+      slices_projection > L1G_MAX_SLICES)
+    return LAPW1GPU_ERR_RANGE;
+  c->slices_frc = slices_density;
+  c->slices_prj = slices_projection;
   return LAPW1GPU_OK;
 }
 
@@ -1295,7 +1299,7 @@ int lapw1gpu_set_tuning(lapw1gpu_context* c, const lapw1gpu_tuning* t) {
   return LAPW1GPU_OK;
 }
 
-// Autotuner: every candidate of a tunable is timed on kp (best of two
+// Autotuner: every candidate of a tunable is timed on kp (best of three
 // runs, CUDA events around the whole stage sequence) with the others held,
 // tunables one after another; the fastest is kept.
 int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, int ldhs, double* d_hsdiag,
@@ -1303,7 +1307,7 @@ int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, in
   if (!c || !kp || !d_hs || !d_hsdiag || ldhs < kp->n || kp->ctx != c) return LAPW1GPU_ERR_ARG;
   auto time_once = [&](double* ms) -> int {
     double best = 1e30;
-    for (int r = 0; r < 2; r++) {
+    for (int r = 0; r < 3; r++) {
       lapw1gpu_stats st;
       int rc = lapw1gpu_kpoint_run(c, kp, 7, d_hs, ldhs, d_hsdiag, &st);
       if (rc) return rc;
@@ -1728,7 +1732,7 @@ static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double*
       k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
       k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
       int nly = 0;
-      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices_frc, s, &nly, 1);
+      rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices_prj, s, &nly, 1);
       if (rc) return rc;
       nlf += nly + 2;
     } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
@@ -1748,7 +1752,7 @@ static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double*
         if (!Lc) return LAPW1GPU_ERR_NOMEM;
         k_force_trans<<<dim3((nlo + 31) / 32, (Kc + 31) / 32), 256, 0, s>>>(Clo, nlo, Kc, nlo, 1, Lc, Kc);
         int nly = 0;
-        rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices_frc, s,
+        rc = split_rect_gemm(c, k, 0, Kc, 4 * nb, nlo, Lc, Kc, Gt + (size_t)nv * 4 * nb, 4 * nb, Yc, Kc, c->slices_prj, s,
                              &nly, 1);
         if (rc) return rc;
         nlf += nly + 1;

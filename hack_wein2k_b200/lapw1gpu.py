@@ -72,7 +72,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_finalize.argtypes = [vp]
     lib.lapw1gpu_set_precision.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_set_slices.argtypes = [vp, C.c_int, C.c_int]
-    lib.lapw1gpu_set_force_slices.argtypes = [vp, C.c_int]
+    lib.lapw1gpu_set_force_slices.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_seclr4.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     lib.lapw1gpu_kpoint_upload.argtypes = [vp, C.POINTER(CProblem), C.POINTER(vp)]
@@ -172,9 +172,11 @@ class Context:
         """split precision with separate slice counts (lapw1gpu_set_slices)"""
         _check("lapw1gpu_set_slices", self.lib.lapw1gpu_set_slices(self.h, slices_sph, slices_hns))
 
-    def set_force_slices(self, slices: int):
-        """int8 slices of the adjoint's products in split precision (lapw1gpu_set_force_slices)"""
-        _check("lapw1gpu_set_force_slices", self.lib.lapw1gpu_set_force_slices(self.h, slices))
+    def set_force_slices(self, slices: int, slices_projection: Optional[int] = None):
+        """int8 slices of the adjoint's density matrices and of its HNS
+        projections in split precision (lapw1gpu_set_force_slices)"""
+        sp = slices if slices_projection is None else slices_projection
+        _check("lapw1gpu_set_force_slices", self.lib.lapw1gpu_set_force_slices(self.h, slices, sp))
 
     @property
     def stream_handle(self) -> int:

@@ -178,10 +178,11 @@ int lapw1gpu_set_precision(lapw1gpu_context* ctx, int prec, int slices);
  * for HNS (the non-spherical part is one to two orders of magnitude
  * smaller, so it tolerates one slice fewer at the same eigenvalue error) */
 int lapw1gpu_set_slices(lapw1gpu_context* ctx, int slices_sph, int slices_hns);
-/* int8 slices (4..8, default 6) of the adjoint's products in split
- * precision (lapw1gpu_forces: the density matrices and the HNS
- * projections); the force pair sums stay FP64 */
-int lapw1gpu_set_force_slices(lapw1gpu_context* ctx, int slices);
+/* int8 slices (4..8 each, default 6 and 6) of the adjoint's products in
+ * split precision (lapw1gpu_forces): the density matrices rho, rhoE and
+ * the HNS projections Y = R^H (G c); the force pair sums stay FP64 */
+int lapw1gpu_set_force_slices(lapw1gpu_context* ctx, int slices_density,
+                              int slices_projection);
 
 /* One k-point's inputs resident in device memory (uploaded once; the
  * benchmark's resident-input path and the k-point batch driver use it). */

@@ -7,7 +7,8 @@
   * c4 k-point 0 (RKmax 8, N = 12726): the FP64 HAMILT stage on sampled
     column blocks, and the HNS stage of three atoms (the other atom types'
     non-spherical T blocks zeroed), against the oracle at 1e-12;
-  * c3 forces: the adjoint (FP64 and split) against central differences of
+  * c3 forces: the adjoint (FP64, split, split with 4-slice HNS
+    projections) against central differences of
     the band energy of the lowest 400 bands with step 1e-4 bohr, on 12
     components, within 1e-4 Ry/bohr.
 The oracle runs its ZHER2M blocks on OpenBLAS zgemm here (the same sums in
@@ -126,10 +127,13 @@ def c3_forces(ctx):
     ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
     try:
         gsp = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+        ctx.set_force_slices(6, 4)  # the benchmark's setting: 4-slice HNS projections
+        gsp4 = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
     finally:
+        ctx.set_force_slices(6, 6)
         ctx.set_precision(lapw1gpu.PREC_FP64)
     kp.free()
-    return p, occ, g64, gsp
+    return p, occ, g64, (gsp, gsp4)
 
 
 @pytest.mark.gpu
@@ -138,7 +142,7 @@ def c3_forces(ctx):
 def test_c3_forces_match_central_differences(ctx, c3_forces, ac):
     """dE/dR of the adjoint against (E(R + h) - E(R - h)) / 2h, h = 1e-4
     bohr, through the FP64 setup and the device eigen-solve."""
-    p, occ, g64, gsp = c3_forces
+    p, occ, g64, (gsp, gsp4) = c3_forces
     a, c = ac
     bk = np.asarray(p.bkzz, dtype=np.float64).reshape(3, 3)
     h = 1.0e-4 * bk[c, c] / (2.0 * np.pi)  # lattice step of the orthorhombic cell
@@ -146,3 +150,4 @@ def test_c3_forces_match_central_differences(ctx, c3_forces, ac):
     to_cart = bk[c, c] / (2.0 * np.pi)
     assert abs(fd - g64[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, g64[a, c] * to_cart)
     assert abs(fd - gsp[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gsp[a, c] * to_cart)
+    assert abs(fd - gsp4[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gsp4[a, c] * to_cart)
