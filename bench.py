@@ -476,6 +476,13 @@ def north_star(args):
     g0_split = grads[0].cpu().numpy()
     # parts of the split step: the batched setup alone, the forces alone
     ms_setup_split = min(ctx.setup_batch(*bargs)["ms_total"] for _ in range(3)) / NK
+
+    def singles():  # the same k-points as 16 lapw1gpu_kpoint_run calls
+        for i, k in enumerate(kps):
+            k.run(hs[i].data_ptr(), ps[i].n, hd[i].data_ptr())
+
+    singles()
+    ms_setup_singles = _timed_loop(torch, stream, singles, 1) / NK
     ms_forces_split = min(forces_all()[1] for _ in range(2)) / NK
     fst_split = []
     for i, q in enumerate(ps[:4]):
@@ -654,6 +661,7 @@ def north_star(args):
                    "l2": "inputs larger than L2: each k-point's HS is 2.6 GB (126 MB L2)"},
         "kpoints_per_s": 1e3 / value,
         "setup": {"split_ms_per_kpoint": ms_setup_split, "fp64_ms_per_kpoint": ms_setup_fp64,
+                  "split_single_calls_ms_per_kpoint": ms_setup_singles,
                   "speedup": ms_setup_fp64 / ms_setup_split,
                   "split_fp64_equiv_tflops": (16.0 * p0.n ** 2 * p0.ltop ** 2 + 8.0 * p0.n ** 2 * 25) * p0.ndf
                   / (ms_setup_split * 1e-3) / 1e12},

@@ -82,7 +82,7 @@ struct lapw1gpu_context {
   int hns_diag_b = 512;    // FP64 HNS: diagonal block of the blocked ZHER2M form
   int split_group = 16;    // split HNS: row tiles per rasterisation group
   int sph_tc = 1;          // split precision: spherical part on tcgen05 (1) or FP64 (0)
-  int sph_kb = 64;         // k_sph_tc: bytes of K per pipeline stage (64: deep ring, 128: two stages)
+  int sph_kb = 128;        // k_sph_tc: bytes of K per pipeline stage (64: deep ring, 128: two stages)
   int batch_sets = 2;      // concurrent k-point chains in a batch
   int test_never_wait = 0; // test hook: the spherical tensor kernel's consumer wait runs out
   int last_launches = 0;   // kernels launched by the last call (a library product counts as one)

@@ -326,7 +326,8 @@ typedef struct {
   int batch_sets;   /* concurrent k-point chains in a batch (1..4)               */
   int sph_kblock;   /* split: K bytes per k_sph_tc pipeline stage, 64 (four-deep
                        ring of 64-byte swizzled rows) or 128 (two stages of
-                       128-byte rows; up to 5 slices, else 64 is used)        */
+                       128-byte rows; up to 5 slices, else 64 is used;
+                       the default)                                           */
   double ms_best;   /* setup time of the tuned k-point with the choices, ms      */
 } lapw1gpu_tuning;
 int lapw1gpu_get_tuning(lapw1gpu_context* ctx, lapw1gpu_tuning* t);

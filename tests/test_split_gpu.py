@@ -187,18 +187,20 @@ def test_split_stages_compose(sctx, kind):
 @pytest.mark.parametrize("slices", [4, 5])
 @pytest.mark.parametrize("case", ["lo", "manyeq", "c1"])
 def test_sph_tc_kblock_shapes_agree(sctx, slices, case):
-    """k_sph_tc with 128-byte K blocks (two-stage ring) against the 64-byte
-    default: the level sums are exact int32 sums, so the two tile shapes
-    give the same bits; both within the slice count's bound of the oracle."""
+    """k_sph_tc with 128-byte K blocks (two-stage ring, the default) against
+    64-byte ones (four-stage ring): the level sums are exact int32 sums, so
+    the two tile shapes give the same bits; both within the slice count's
+    bound of the oracle."""
     sctx.set_precision(lapw1gpu.PREC_SPLIT, slices)
     p = synth.config("c1")[0] if case == "c1" else synth.small_case(case)
+    kb0 = sctx.tuning()["sph_kblock"]
     try:
         sctx.set_tuning(sph_kblock=64)
         hs64, hsd64 = sctx.setup(p)
         sctx.set_tuning(sph_kblock=128)
         hs128, hsd128 = sctx.setup(p)
     finally:
-        sctx.set_tuning(sph_kblock=64)
+        sctx.set_tuning(sph_kblock=kb0)
     assert np.array_equal(hs64, hs128) and np.array_equal(hsd64, hsd128)
     hs_o, hsd_o = O.setup(p)
     err = rel_errors(hs128, hsd128, hs_o, hsd_o)
