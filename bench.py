@@ -10,7 +10,9 @@ LO per atom for l <= 2, 16 seeded k-points per GPU.  One step = the
 calkpt.F:153-185 setup of all 16 k-points in split precision as ONE
 captured batch launch (lapw1gpu_setup_batch: int8 Ozaki slices on tcgen05,
 5 slices spherical / 4 HNS, FP64 combine) plus the adjoint forces of the
-lowest 400 bands at each of the 16 k-points (lapw1gpu_forces).  The
+lowest 400 bands at each of the 16 k-points (lapw1gpu_forces_batch; int8
+slice products with 6 slices for the density matrices and 4 for the HNS
+projections, FP64 pair sums).  The
 eigenvectors come from the device eigen-solve of each k-point's split
 matrices before timing (the eigen-solve is not part of the step, as SECLR4
 is not part of the setup).  With N GPUs each rank takes its own 16 k-points
@@ -622,13 +624,16 @@ def north_star(args):
         kd[name] = {"bound": bnd, "work_per_launch": w, "ms": t, "achieved": a, "unit": unit, "peak": pk,
                     "frac": a / pk if a else None}
     dom = max((k for k in kern if kern[k][0] != "hbm"), key=lambda k: kern[k][2])
-    traffic = None
+    tr4 = {}
     tj = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tj):
         try:
-            traffic = json.load(open(tj)).get("c4", {}).get(dom)
+            tr4 = json.load(open(tj)).get("c4", {})
         except Exception:
-            traffic = None
+            tr4 = {}
+    for name in kd:  # DRAM bytes per launch from the ncu captures (profiles/traffic.json)
+        kd[name]["traffic"] = tr4.get(name)
+    traffic = tr4.get(dom)
     dm = kd[dom]
     roofline = {"kernel": dom, "bound": dm["bound"], "achieved": dm["achieved"], "peak": dm["peak"],
                 "unit": dm["unit"], "frac": dm["frac"], "traffic": traffic,

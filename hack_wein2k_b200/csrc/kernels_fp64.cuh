@@ -440,8 +440,13 @@ __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restr
   const int nv = P.nv;
   const int I = nv + c.nnlo - 1;  // 0-based row/column of this LO
   int J = blockIdx.x * blockDim.x + threadIdx.x;
-  if (J > I) return;
   const int jn = c.jn, l = c.l, jlo = c.jlo, jeqo = c.jeqo, mo1 = c.mo1, mult = P.mult[jn];
+  // the LO row's Y_lm per equivalent atom, shared by the block (I is the
+  // block's), in chunks of LO_YCH atoms
+  constexpr int LO_YCH = 16;
+  __shared__ double2 syi[LO_YCH][16];
+  const bool active = J <= I;
+  if (!active && (blockIdx.x * blockDim.x) > I) return;  // the whole block is past the row (block-uniform)
   const double pi = 3.141592653589793238462643;
   const double r = P.rmt[jn], r2 = r * r;
   const double pi4r2v = 4.0 * pi * sqrt(P.vi) * r * r;
@@ -471,21 +476,30 @@ __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restr
     any_lo |= inlo[jlop];
   }
   double2 S = cmk(0.0, 0.0), H = cmk(0.0, 0.0);
-  if (J < nv || any_lo) {
+  const bool work = active && (J < nv || any_lo);
+  {
     double alj = 0.0, blj = 0.0;
-    if (J < nv) {
+    if (work && J < nv) {
       size_t oo = ((size_t)jn * P.ltop + l) * P.nvpad + J;
       alj = P.al[oo];
       blj = P.bl[oo];
     }
     for (int jeq = 0; jeq < mult; jeq++) {
+      if (jeq % LO_YCH == 0) {  // block-uniform: the next chunk's Y_lm of the LO row
+        __syncthreads();
+        const int q = threadIdx.x;
+        if (q < LO_YCH && jeq + q < mult)
+          dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * (c.a0 + jeq + q), P.rotloc + 9 * jn, l, syi[q]);
+        __syncthreads();
+      }
+      if (!work) continue;
       const int a = c.a0 + jeq;
       const double* ra = P.pos + 3 * a;
       double s = ra[0] * (double)(P.kzz[3 * I] - P.kzz[3 * J]) + ra[1] * (double)(P.kzz[3 * I + 1] - P.kzz[3 * J + 1]) +
                  ra[2] * (double)(P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
       const double2 ph = cconj(cexp2pi(s));
-      double2 yi[16], yj[16];
-      dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yi);
+      double2 yj[16];
+      const double2* yi = syi[jeq % LO_YCH];
       dev_ylm_row<3>(P.xk[J], P.yk[J], P.zk[J], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yj);
       for (int mo2 = -l; mo2 <= l; mo2++) {
         const int lm = l * (l + 1) + mo2;
@@ -532,6 +546,7 @@ __global__ void k_lo(DevProb P, const LoCol* __restrict__ cols, double2* __restr
     }
   }
 #undef LOV
+  if (!active) return;
   if (J == I) {
     hs[(size_t)I * ld + I] = H;
     hsdiag[I] = S;

@@ -1239,7 +1239,11 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
       return rc ? rc : LAPW1GPU_ERR_CUDA;
     }
     cudaGraphExec_t exec = nullptr;
-    e = cudaGraphInstantiate(&exec, graph, 0);
+    // the kernel nodes keep the priorities of the streams they were captured
+    // from (chains high, the HNS operand streams low), so that the
+    // persistent spherical kernel's CTAs are placed before the side work, as
+    // in eager runs; a graph uses them only when instantiated with this flag
+    e = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -1299,58 +1303,61 @@ int lapw1gpu_set_tuning(lapw1gpu_context* c, const lapw1gpu_tuning* t) {
   return LAPW1GPU_OK;
 }
 
-// Autotuner: every candidate of a tunable is timed on kp (best of three
-// runs, CUDA events around the whole stage sequence) with the others held,
-// tunables one after another; the fastest is kept.
+// Autotuner: the candidates of a tunable are timed on kp with the others
+// held, tunables one after another; the fastest is kept.  Each candidate's
+// time is its best of three runs, the runs of the candidates interleaved
+// (round r runs every candidate once) so that a drift of the clocks over
+// the tuning favours none of them, and it is the time of the kernel the
+// tunable shapes where there is one (the spherical tensor-core kernel for
+// its K block, the HNS products for their L2 grouping), else of the whole
+// stage sequence (CUDA events).
 int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, int ldhs, double* d_hsdiag,
                       lapw1gpu_tuning* out) {
   if (!c || !kp || !d_hs || !d_hsdiag || ldhs < kp->n || kp->ctx != c) return LAPW1GPU_ERR_ARG;
-  auto time_once = [&](double* ms) -> int {
-    double best = 1e30;
-    for (int r = 0; r < 3; r++) {
-      lapw1gpu_stats st;
-      int rc = lapw1gpu_kpoint_run(c, kp, 7, d_hs, ldhs, d_hsdiag, &st);
-      if (rc) return rc;
-      best = std::min(best, st.ms_total);
-    }
-    *ms = best;
+  enum { T_TOTAL, T_SPH, T_HNS };
+  auto tune = [&](int* knob, const std::vector<int>& cand, int what) -> int {
+    const int v0 = *knob;
+    std::vector<double> t(cand.size(), 1e30);
+    for (int r = 0; r < 3; r++)
+      for (size_t q = 0; q < cand.size(); q++) {
+        *knob = cand[q];
+        lapw1gpu_stats st;
+        int rc = lapw1gpu_kpoint_run(c, kp, 7, d_hs, ldhs, d_hsdiag, &st);
+        if (rc) {
+          *knob = v0;
+          return rc;
+        }
+        const double m = what == T_SPH ? st.ms_sph_main : what == T_HNS ? st.ms_hns_main : st.ms_total;
+        t[q] = std::min(t[q], m > 0.0 ? m : st.ms_total);
+      }
+    size_t b = 0;
+    for (size_t q = 1; q < cand.size(); q++)
+      if (t[q] < t[b]) b = q;
+    *knob = cand[b];
     return LAPW1GPU_OK;
   };
-  auto tune = [&](int* knob, const std::vector<int>& cand, double* best_ms) -> int {
-    int best = *knob;
-    double bm = 1e30;
-    for (int v : cand) {
-      *knob = v;
-      double ms;
-      int rc = time_once(&ms);
-      if (rc) {
-        *knob = best;
-        return rc;
-      }
-      if (ms < bm) {
-        bm = ms;
-        best = v;
-      }
-    }
-    *knob = best;
-    *best_ms = bm;
-    return LAPW1GPU_OK;
-  };
-  double ms = 0.0;
   int rc = LAPW1GPU_OK;
   if (c->prec == LAPW1GPU_PREC_FP64) {
-    rc = tune(&c->hns_diag_b, {256, 512, 1024, 2048}, &ms);
+    rc = tune(&c->hns_diag_b, {256, 512, 1024, 2048}, T_TOTAL);
   } else {
-    if (sph_tc_supported(c->slices)) rc = tune(&c->sph_tc, {1, 0}, &ms);
+    if (sph_tc_supported(c->slices)) rc = tune(&c->sph_tc, {1, 0}, T_TOTAL);
     // the K block (and with it the ring depth) of k_sph_tc: 128-byte blocks
     // exist up to 5 slices
-    if (!rc && c->sph_tc && c->slices <= 5) rc = tune(&c->sph_kb, {64, 128}, &ms);
-    if (!rc) rc = tune(&c->split_group, {4, 8, 16, 32}, &ms);
+    if (!rc && c->sph_tc && c->slices <= 5) rc = tune(&c->sph_kb, {64, 128}, T_SPH);
+    if (!rc) rc = tune(&c->split_group, {4, 8, 16, 32}, T_HNS);
+  }
+  if (rc) return rc;
+  // the setup time with the final choices
+  double total_best = 1e30;
+  for (int r = 0; r < 2 && !rc; r++) {
+    lapw1gpu_stats st;
+    rc = lapw1gpu_kpoint_run(c, kp, 7, d_hs, ldhs, d_hsdiag, &st);
+    if (!rc) total_best = std::min(total_best, st.ms_total);
   }
   if (rc) return rc;
   if (out) {
     lapw1gpu_get_tuning(c, out);
-    out->ms_best = ms;
+    out->ms_best = total_best;
   }
   return LAPW1GPU_OK;
 }
