@@ -718,13 +718,18 @@ def c3_fd_component(ctx, torch, dev, p, nb, a, c, h_bohr=1.0e-4):
     import dataclasses
     bk = np.asarray(p.bkzz, dtype=np.float64).reshape(3, 3)
     h = h_bohr * bk[c, c] / (2.0 * np.pi)  # lattice step of the orthorhombic cell
+    from hack_wein2k_b200.forces import _setup_device
+    from hack_wein2k_b200.seclr import eigenvalues, hermitian_from_packed_device
     vals = []
     for sgn in (1.0, -1.0):
         pos = np.array(p.pos, dtype=np.float64, copy=True)
         pos[a, c] += sgn * h
-        E, _, _, kp, _ = _c3_band_energy(ctx, torch, dev, dataclasses.replace(p, pos=pos), nb)
+        kp, hs, hd = _setup_device(ctx, dataclasses.replace(p, pos=pos))
+        H, S = hermitian_from_packed_device(hs, hd)
+        del hs, hd
+        vals.append(float(eigenvalues(H, S, nb).sum()))  # the band energy, unit occupations
+        del H, S
         kp.free()
-        vals.append(E)
     return (vals[0] - vals[1]) / (2.0 * h)
 
 
@@ -762,7 +767,8 @@ def c3_accuracy(ctx, torch, dev, n_fd):
     for a, c in comps:
         d = c3_fd_component(ctx, torch, dev, p3, nb, a, c)
         err = abs(d - res["fp64"][1][a, c]) * bk[c, c] / (2.0 * np.pi)  # Ry/bohr
-        fd.append({"atom": a, "comp": c, "fd_minus_adjoint_ry_bohr": err,
+        err_sp = abs(d - res["split"][1][a, c]) * bk[c, c] / (2.0 * np.pi)
+        fd.append({"atom": a, "comp": c, "fd_minus_adjoint_ry_bohr": err, "fd_minus_split_adjoint_ry_bohr": err_sp,
                    "force_ry_bohr": float(-res["fp64"][1][a, c] * bk[c, c] / (2.0 * np.pi))})
     out["central_fd_1e-4_bohr"] = fd
     return out
@@ -836,7 +842,8 @@ def c2_batch(ctx, torch, dev, stream):
 
 def fd_report(args):
     """Central differences (step 1e-4 bohr) of the c3 band energy along all
-    3 NDF coordinates against the FP64 adjoint: one JSON line."""
+    3 NDF coordinates against the FP64 adjoint and the split one: one JSON
+    line.  The energies come from the eigenvalue-only solve."""
     import torch
 
     from hack_wein2k_b200 import forces as FO
@@ -847,20 +854,35 @@ def fd_report(args):
     nb = NBANDS
     E, w, X, kp, occ = _c3_band_energy(ctx, torch, dev, p3, nb)
     g = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+    # the split adjoint (bench.py's slice counts) on the same eigenvectors
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, args.slices)
+    ctx.set_slices(args.slices, args.slices_hns)
+    ctx.set_force_slices(*args.force_slices)
+    gs = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+    ctx.set_precision(lapw1gpu.PREC_FP64)
     kp.free()
+    del X
+    torch.cuda.empty_cache()
     bk = np.asarray(p3.bkzz, dtype=np.float64).reshape(3, 3)
     errs = np.zeros((p3.ndf, 3))
+    errs_sp = np.zeros((p3.ndf, 3))
     t0 = time.time()
     for a in range(p3.ndf):
         for c in range(3):
             d = c3_fd_component(ctx, torch, dev, p3, nb, a, c)
             errs[a, c] = abs(d - g[a, c]) * bk[c, c] / (2.0 * np.pi)
+            errs_sp[a, c] = abs(d - gs[a, c]) * bk[c, c] / (2.0 * np.pi)
     F = FO.cartesian_forces(p3, g)
-    print(json.dumps({"workload": f"c3: 100-atom cell 20^3 bohr, RKmax 6, N {p3.n}, {nb} bands, FP64 path",
+    print(json.dumps({"workload": f"c3: 100-atom cell 20^3 bohr, RKmax 6, N {p3.n}, {nb} bands; central "
+                                  "differences of the FP64 setup's band energy",
                       "components": int(errs.size), "step_bohr": 1e-4,
-                      "max_abs_err_ry_bohr": float(errs.max()), "mean_abs_err_ry_bohr": float(errs.mean()),
-                      "max_force_ry_bohr": float(np.abs(F).max()), "seconds": time.time() - t0,
-                      "worst": [int(x) for x in np.unravel_index(np.argmax(errs), errs.shape)]}), flush=True)
+                      "fp64_adjoint": {"max_abs_err_ry_bohr": float(errs.max()),
+                                       "mean_abs_err_ry_bohr": float(errs.mean()),
+                                       "worst": [int(x) for x in np.unravel_index(np.argmax(errs), errs.shape)]},
+                      "split_adjoint": {"slices": [args.slices, args.slices_hns] + list(args.force_slices),
+                                        "max_abs_err_ry_bohr": float(errs_sp.max()),
+                                        "mean_abs_err_ry_bohr": float(errs_sp.mean())},
+                      "max_force_ry_bohr": float(np.abs(F).max()), "seconds": time.time() - t0}), flush=True)
     ctx.close()
     return 0
 

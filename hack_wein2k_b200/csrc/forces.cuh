@@ -406,6 +406,7 @@ __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const doub
   const LoCol c = cols[blockIdx.y];
   const int nv = P.nv;
   const int I = nv + c.nnlo - 1;
+  if ((int)(blockIdx.x * blockDim.x) >= I) return;  // no pair J < I in the block (block-uniform)
   const int J = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int jn = c.jn, l = c.l, jlo = c.jlo, jeqo = c.jeqo, mo1 = c.mo1, mult = P.mult[jn];
@@ -451,16 +452,27 @@ __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const doub
       blj = P.bl[oo];
     }
   }
+  // the LO row's Y_lm per equivalent atom, shared by the block (I is the
+  // block's), in chunks of FRC_YCH atoms
+  constexpr int FRC_YCH = 16;
+  __shared__ double2 syi[FRC_YCH][16];
   for (int jeq = 0; jeq < mult; jeq++) {
     const int a = c.a0 + jeq;
+    if (jeq % FRC_YCH == 0) {  // block-uniform
+      __syncthreads();
+      const int q = threadIdx.x;
+      if (q < FRC_YCH && jeq + q < mult)
+        dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * (a + q), P.rotloc + 9 * jn, l, syi[q]);
+      __syncthreads();
+    }
     double2 S = cmk(0.0, 0.0), H = cmk(0.0, 0.0);
     if (act) {
       const double* ra = P.pos + 3 * a;
       double s = ra[0] * (double)(P.kzz[3 * I] - P.kzz[3 * J]) + ra[1] * (double)(P.kzz[3 * I + 1] - P.kzz[3 * J + 1]) +
                  ra[2] * (double)(P.kzz[3 * I + 2] - P.kzz[3 * J + 2]);
       const double2 ph = cconj(cexp2pi(s));
-      double2 yi[16], yj[16];
-      dev_ylm_row<3>(P.xk[I], P.yk[I], P.zk[I], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yi);
+      double2 yj[16];
+      const double2* yi = syi[jeq % FRC_YCH];
       dev_ylm_row<3>(P.xk[J], P.yk[J], P.zk[J], P.rotij + 9 * a, P.rotloc + 9 * jn, l, yj);
       for (int mo2 = -l; mo2 <= l; mo2++) {
         const int lm = l * (l + 1) + mo2;
@@ -571,16 +583,20 @@ __global__ void k_force_weight(int n, int nb, const double2* __restrict__ C, int
 // Z = T Y per atom: the product L^T (G c) through the small T of each atom
 // instead of a second N x K GEMM, because L = M conj(R) (+ the CLM terms of
 // the LO rows).  FRC_ZCOLS columns of Y per block: the atom type's T blocks
-// and the columns' Y entries of the atom are staged in shared memory once.  Y: [col][K] (k = (a*2 + r)*nsl2 + b), Yc, Zc: [col][Kc]
+// and the columns' Y entries of the atom are staged in shared memory once;
+// lane = column (the T entries a warp reads are one broadcast word, the
+// columns' Y rows lie 3 NSL2 = 75 double2 apart: odd, so a warp's 16-byte
+// reads do not conflict) and each thread keeps the NSL2 outputs of one T
+// row (r) of its column in registers.  Y: [col][K] (k = (a*2 + r)*nsl2 + b), Yc, Zc: [col][Kc]
 // (k = a*nsl2 + lm), col < ncol = 4 nb.
 //   zc = 0: Z[a][(r, lm)] = sum_b T_(r,A)[lm][b] Y_A[b] + T_(r,B)[lm][b] Y_B[b]
 //           (+ T_(r,C)[lm][b] Yc[b] with LOs), with (A, B, C) = (TUU, TDU,
 //           TUU21) for r = 0 and (TUD, TDD, TUD21) for r = 1;
 //   zc = 1: Zc[a][lm] = sum_b TUU12[lm][b] Y_A[b] + TDU12[lm][b] Y_B[b] +
 //           TUU22[lm][b] Yc[b]: the CLM row of T applied to Y over all rows.
-#define FRC_ZCOLS 32
+#define FRC_ZCOLS 128
 #define FRC_ZSMEM ((6 * L1G_NSL2 * L1G_NSL2 + FRC_ZCOLS * 3 * L1G_NSL2) * 16)
-__global__ void __launch_bounds__(256) k_force_hns_z(int zc, int nsl2, int K, int Kc, int ncol,
+__global__ void __launch_bounds__(256, 1) k_force_hns_z(int zc, int nsl2, int K, int Kc, int ncol,
                                                      const int* __restrict__ atype, const double2* __restrict__ tns,
                                                      const double2* __restrict__ Y, const double2* __restrict__ Yc,
                                                      double2* __restrict__ Z, double2* __restrict__ Zc) {
@@ -605,22 +621,39 @@ __global__ void __launch_bounds__(256) k_force_hns_z(int zc, int nsl2, int K, in
     sY[(cl * 3 + part) * L1G_NSL2 + b] = v;
   }
   __syncthreads();
-  const int nout = zc ? nsl2 : 2 * nsl2;
-  for (int i = tid; i < nc * nout; i += blockDim.x) {
-    const int cl = i / nout, ko = i % nout;
-    const int ro = zc ? 0 : ko / nsl2, lm = zc ? ko : ko % nsl2;
-    const double2* tA = sT + ((3 * ro) * L1G_NSL2 + lm) * L1G_NSL2;  // blocks (A, B, C) of row ro
-    const double2* y = sY + cl * 3 * L1G_NSL2;
-    double2 z = cmk(0.0, 0.0);
-    for (int b = 0; b < nsl2; b++) {
-      z = cadd(z, cmul(tA[b], y[b]));
-      z = cadd(z, cmul(tA[L1G_NSL2 * L1G_NSL2 + b], y[L1G_NSL2 + b]));
-      z = cadd(z, cmul(tA[2 * L1G_NSL2 * L1G_NSL2 + b], y[2 * L1G_NSL2 + b]));  // zero without LOs
+  // warp w: columns 32 (w % 4) + lane, outputs: zc = 0 the row r = w / 4
+  // (lm = 0 .. nsl2-1), zc = 1 the lm half w / 4 of the single row
+  const int lane = tid & 31, w = tid >> 5, cl = (w & 3) * 32 + lane, oh = w >> 2;
+  const int half = (nsl2 + 1) / 2;
+  const int ro = zc ? 0 : oh, lm0 = (zc && oh) ? half : 0, nlm = zc ? (oh ? nsl2 - half : half) : nsl2;
+  const double2* tR = sT + (3 * ro) * L1G_NSL2 * L1G_NSL2;    // blocks (A, B, C) of row ro
+  const double2* y = sY + (size_t)min(cl, nc - 1) * 3 * L1G_NSL2;  // columns past nc: computed, not stored
+  double2 z[L1G_NSL2];
+#pragma unroll
+  for (int q = 0; q < L1G_NSL2; q++) z[q] = cmk(0.0, 0.0);
+  for (int b = 0; b < nsl2; b++) {
+    const double2 yA = y[b], yB = y[L1G_NSL2 + b], yC = y[2 * L1G_NSL2 + b];  // yC zero without LOs
+#pragma unroll
+    for (int q = 0; q < L1G_NSL2; q++) {
+      if (q < nlm) {
+        const double2* t = tR + (lm0 + q) * L1G_NSL2 + b;
+        z[q] = cadd(z[q], cmul(t[0], yA));
+        z[q] = cadd(z[q], cmul(t[L1G_NSL2 * L1G_NSL2], yB));
+        z[q] = cadd(z[q], cmul(t[2 * L1G_NSL2 * L1G_NSL2], yC));
+      }
     }
-    if (zc)
-      Zc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + lm] = z;
-    else
-      Z[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + ko] = z;
+  }
+  if (cl < nc) {
+#pragma unroll
+    for (int q = 0; q < L1G_NSL2; q++) {
+      if (q < nlm) {
+        const int lm = lm0 + q;
+        if (zc)
+          Zc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + lm] = z[q];
+        else
+          Z[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + ro * nsl2 + lm] = z[q];
+      }
+    }
   }
 }
 

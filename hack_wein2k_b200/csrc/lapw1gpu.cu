@@ -18,11 +18,27 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "kernels_fp64.cuh"
 #include "forces.cuh"
+
+// The last failing CUDA call of this thread, for lapw1gpu_last_error
+static thread_local char g_last_error[192];
+static void l1g_note_error(const char* what, long code, const char* file, int line) {
+  const char* base = strrchr(file, '/');
+  snprintf(g_last_error, sizeof(g_last_error), "%s:%d: %s (%ld)", base ? base + 1 : file, line, what, code);
+}
+// the launch status after kernel launches, noted when it is an error
+static int l1g_launch_status(const char* file, int line) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return LAPW1GPU_OK;
+  l1g_note_error(cudaGetErrorName(e), (long)e, file, line);
+  return LAPW1GPU_ERR_CUDA;
+}
+
 
 #define L1G_VERSION "lapw1gpu 0.1 (sm_100a)"
 
@@ -94,19 +110,31 @@ struct lapw1gpu_context {
     int launches = 0;
   };
   std::vector<Graph> graphs;  // captured batches
-  std::map<const void*, int> smem_attr;  // kernels whose dynamic shared memory limit is raised
   std::vector<void*> host_pinned;        // caller buffers page-locked by lapw1gpu_host_register
 
-  // raise a kernel's dynamic shared-memory limit once per context (not a
-  // stream operation, and kept out of captured sequences)
+  // raise a kernel's dynamic shared-memory limit (not a stream operation,
+  // and kept out of captured sequences).  The limit belongs to the kernel
+  // on the device, not to a context, so the record of what was set is
+  // process-wide and the limit only ever grows: a second context (or a
+  // second library user) asking for less must not lower it under a size
+  // that another context's queued launches rely on.
   bool smem(const void* fn, int bytes) {
-    auto it = smem_attr.find(fn);
-    if (it != smem_attr.end() && it->second >= bytes) return true;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> raised;  // (device, kernel) -> limit set there
+    static std::map<const void*, int> widest;                  // kernel -> largest limit set anywhere
+    std::lock_guard<std::mutex> lock(mu);
+    int& cur = raised[std::make_pair(device, fn)];
+    if (cur >= bytes) return true;
+    int& wide = widest[fn];
+    const int want = std::max(bytes, wide);  // never below a limit set before, on any device
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, want);
+    if (e != cudaSuccess) {
+      l1g_note_error(cudaGetErrorName(e), (long)e, __FILE__, __LINE__);
       cudaGetLastError();
       return false;
     }
-    smem_attr[fn] = bytes;
+    cur = want;
+    wide = want;
     return true;
   }
 
@@ -208,13 +236,14 @@ static const int2* kp_tiles(lapw1gpu_kpoint* k, const std::string& key, int* cou
 
 namespace {
 
-#define CK(x)                                 \
-  do {                                        \
-    cudaError_t _e = (x);                     \
-    if (_e != cudaSuccess) {                  \
-      cudaGetLastError();                     \
-      return LAPW1GPU_ERR_CUDA;               \
-    }                                         \
+#define CK(x)                                           \
+  do {                                                  \
+    cudaError_t _e = (x);                               \
+    if (_e != cudaSuccess) {                            \
+      l1g_note_error(cudaGetErrorName(_e), _e, __FILE__, __LINE__); \
+      cudaGetLastError();                               \
+      return LAPW1GPU_ERR_CUDA;                         \
+    }                                                   \
   } while (0)
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
@@ -263,6 +292,8 @@ int validate(const lapw1gpu_problem* p) {
 extern "C" {
 
 const char* lapw1gpu_version(void) { return L1G_VERSION; }
+
+const char* lapw1gpu_last_error(void) { return g_last_error; }
 
 int lapw1gpu_init(int device, lapw1gpu_context** out) {
   if (!out) return LAPW1GPU_ERR_ARG;
@@ -719,7 +750,7 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
   k_hns_alm<<<dim3((P.npad + 127) / 128, P.ndf), 128, 0, s>>>(P, lor, nlor, Rop, Clo);
   if (!Lop) {
     *nl += 1;
-    return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+    return l1g_launch_status(__FILE__, __LINE__);
   }
   if (c ? !c->smem((const void*)k_hns_tmul, TMUL_SMEM)
         : cudaFuncSetAttribute(k_hns_tmul, cudaFuncAttributeMaxDynamicSharedMemorySize, TMUL_SMEM) != cudaSuccess)
@@ -736,7 +767,7 @@ static int launch_hns_ops(lapw1gpu_context* c, const DevProb& P, const double2* 
                                                                                            C2lo, 0);
     *nl += 1;
   }
-  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  return l1g_launch_status(__FILE__, __LINE__);
 }
 
 // The FP64 HNS update in the blocked form of ZHER2M (zher2m.f:69-80):
@@ -804,9 +835,12 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
   if (sl_smem > 200 * 1024) return LAPW1GPU_ERR_RANGE;
   if (!c->smem((const void*)sphtc::k_sph_slice<S>, sl_smem)) return LAPW1GPU_ERR_CUDA;
   if (ev && cudaEventRecord(c->ev[20], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
+  if (int rc = l1g_launch_status(__FILE__, __LINE__)) return rc;
   sphtc::k_sph_slice<S><<<dim3(npA / 32, L), 256, sl_smem, s>>>(P, coef, 0, Kcp, npA, A, exA, c->d_status);
+  if (int rc = l1g_launch_status(__FILE__, __LINE__)) return rc;
   sphtc::k_sph_slice<S><<<dim3((2 * npB + 31) / 32, L), 256, sl_smem, s>>>(P, coef, 1, Kcp, 2 * npB, B, exB,
                                                                            c->d_status);
+  if (int rc = l1g_launch_status(__FILE__, __LINE__)) return rc;
   if (ev && cudaEventRecord(c->ev[21], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
   *nl += 2;
   CUtensorMap ta, tb;
@@ -847,6 +881,14 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
       sphtc::k_sph_tc<S, LS, KB><<<grid, Cf::THREADS, Cf::SMEM, s>>>(ta, tb, P, dt + t0, (int)(t1 - t0), nkb, klast,
                                                                       npA, npB, exA, exB, tab, k->tab, hs, ld, hsdiag,
                                                                       c->d_status, c->test_never_wait);
+      const cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) {
+        char what[160];
+        snprintf(what, sizeof(what), "%s launching k_sph_tc<%d,%d,%d> grid %d block %d smem %d", cudaGetErrorName(le),
+                 S, LS, KB, grid, Cf::THREADS, Cf::SMEM);
+        l1g_note_error(what, (long)le, __FILE__, __LINE__);
+        return LAPW1GPU_ERR_CUDA;
+      }
       *nl += 1;
     }
     if (sp && sp->col[g + 1] <= k->nv) {
@@ -855,7 +897,7 @@ static int sph_tc_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, const
     }
   }
   if (ev && cudaEventRecord(ev[1], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
-  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  return l1g_launch_status(__FILE__, __LINE__);
 }
 
 // Exactness of the level sums (|slice| <= 64; level d sums d+1 products of
@@ -990,9 +1032,11 @@ static int kpoint_run_impl(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, 
     nl++;
     if (ev) CK(cudaEventRecord(ev[18], s));
     k_table<<<(unsigned)((ntab + 127) / 128), 128, 0, s>>>(P, k->tab, k->d_warp, tab);
+    if (int rc = l1g_launch_status(__FILE__, __LINE__)) return rc;
     if (ev) CK(cudaEventRecord(ev[19], s));
     nl++;
     k_sph_coef<<<nat, 32, 0, s>>>(P, coef);
+    if (int rc = l1g_launch_status(__FILE__, __LINE__)) return rc;
     // column groups of the spherical contraction (the caller's boundaries)
     HnsPipe* sp = (hp && hp->fixed && hp->groups > 0) ? hp : nullptr;
     if (c->prec == LAPW1GPU_PREC_SPLIT && c->sph_tc && sph_tc_supported(c->slices)) {

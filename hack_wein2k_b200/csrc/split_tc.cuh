@@ -463,6 +463,7 @@ static int l1g_tmap_3d(CUtensorMap* m, const void* base, uint64_t kp, uint64_t r
                    : inner == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
                                  : CU_TENSOR_MAP_SWIZZLE_64B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) l1g_note_error("cuTensorMapEncodeTiled", (long)r, __FILE__, __LINE__);
   return r == CUDA_SUCCESS ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
 }
 
@@ -495,7 +496,7 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
     split::k_slice_rows<S><<<gs, 256, 0, s>>>(Rop, Kc, Kcp, npad, np, 1, 0, exB, B, c->d_status);
     *nlaunch += 4;
   }
-  if (!(phase & 2)) return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  if (!(phase & 2)) return l1g_launch_status(__FILE__, __LINE__);
   CUtensorMap ta, tb;
   if (l1g_tmap_3d(&ta, A, Kp, np, S, 128) || l1g_tmap_3d(&tb, B, Kp, 2 * (uint64_t)np, S, Cf::N))
     return LAPW1GPU_ERR_CUDA;
@@ -539,7 +540,7 @@ static int split_gemm_launch(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, i
     }
   }
   if (ev && cudaEventRecord(ev[1], s) != cudaSuccess) return LAPW1GPU_ERR_CUDA;
-  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  return l1g_launch_status(__FILE__, __LINE__);
 }
 
 // Rectangular product out(i, j) += sum_k L(i, k) R(j, k), i < m, j < nr,
@@ -586,7 +587,7 @@ static int split_gemm_rect(lapw1gpu_context* c, lapw1gpu_kpoint* k, int set, int
   split::k_split_gemm<S><<<(unsigned)ntile, SPLIT_THREADS, Cf::SMEM, s>>>(ta, tb, dt, Kp / 64, m, nr, ovw ? 3 : 1,
                                                                            exA, exB, out, ld, c->d_status);
   *nlaunch += 1;
-  return cudaGetLastError() == cudaSuccess ? LAPW1GPU_OK : LAPW1GPU_ERR_CUDA;
+  return l1g_launch_status(__FILE__, __LINE__);
 }
 
 // tag: the prefix of the scratch buffers (callers whose products differ

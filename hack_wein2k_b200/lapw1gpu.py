@@ -31,7 +31,7 @@ STATUS = {
 EXPORTS = [
     "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
-    "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version",
+    "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version", "lapw1gpu_last_error",
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
     "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices", "lapw1gpu_test_wait_timeout",
     "lapw1gpu_last_launches", "lapw1gpu_host_register", "lapw1gpu_host_unregister", "lapw1gpu_forces_stats",
@@ -85,6 +85,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_stream.restype = vp
     lib.lapw1gpu_last_status.argtypes = [vp]
     lib.lapw1gpu_version.restype = C.c_char_p
+    lib.lapw1gpu_last_error.restype = C.c_char_p
     lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
                                             dp, dp, dp, ip, dp]
     lib.lapw1gpu_hns_noalloc.argtypes = [C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
@@ -108,7 +109,10 @@ def load(path: Optional[str] = None):
 
 def _check(where: str, rc: int):
     if rc != 0:
-        raise Lapw1GpuError(where, rc)
+        err = Lapw1GpuError(where, rc)
+        if rc == 3 and _lib is not None:  # the failing CUDA call, for the message
+            err.args = (f"{err.args[0]} [{_lib.lapw1gpu_last_error().decode()}]",)
+        raise err
 
 
 def _dp(a: np.ndarray):

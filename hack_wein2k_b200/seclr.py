@@ -46,3 +46,15 @@ def solve(H: torch.Tensor, S: torch.Tensor, el: float = -1e70, eu: float = 1e70,
         w, V = w[:nmax], V[:, :nmax]
     X = torch.linalg.solve_triangular(L.conj().transpose(0, 1), V, upper=True)    # back-transform
     return w, X
+
+
+def eigenvalues(H: torch.Tensor, S: torch.Tensor, nmax: Optional[int] = None) -> torch.Tensor:
+    """The ascending eigenvalues of H x = e S x (the lowest nmax), without
+    eigenvectors: the same reduction as `solve`, then the eigenvalue-only
+    Hermitian solver."""
+    L = torch.linalg.cholesky(S)
+    Y = torch.linalg.solve_triangular(L, H, upper=False)
+    A = torch.linalg.solve_triangular(L, Y.conj().transpose(0, 1), upper=False)
+    A = 0.5 * (A + A.conj().transpose(0, 1))
+    w = torch.linalg.eigvalsh(A)
+    return w if nmax is None else w[:nmax]

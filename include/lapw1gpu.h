@@ -375,6 +375,10 @@ int lapw1gpu_forces_stats(lapw1gpu_context* ctx, lapw1gpu_stats* st);
 
 /* version string of the library */
 const char* lapw1gpu_version(void);
+/* The CUDA call that made this thread's latest LAPW1GPU_ERR_CUDA ("file:line:
+ * error name (code)"), or "" before any: a diagnostic for the caller's log.
+ * No counterpart in the reference. */
+const char* lapw1gpu_last_error(void);
 
 #ifdef __cplusplus
 }

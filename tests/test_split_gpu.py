@@ -205,3 +205,24 @@ def test_sph_tc_kblock_shapes_agree(sctx, slices, case):
     hs_o, hsd_o = O.setup(p)
     err = rel_errors(hs128, hsd128, hs_o, hsd_o)
     assert err["S"] <= TOL_H[slices] and err["H"] <= TOL_H[slices], err
+
+
+@pytest.mark.gpu
+def test_second_context_keeps_kernel_limits(sctx):
+    """A kernel's dynamic shared-memory limit belongs to the kernel on the
+    device: a second context that runs a small problem after the first ran
+    a large one must not lower it under what the first context's next,
+    medium problem needs (the split slicer's shared memory grows with the
+    atom count)."""
+    sctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    other = lapw1gpu.Context(0, prec=lapw1gpu.PREC_SPLIT, slices=5)
+    try:
+        sctx.setup(synth.config("c1")[0])
+        other.setup(synth.small_case("lo"))
+        p = synth.small_case("manyeq")
+        hs, hsd = sctx.setup(p)
+    finally:
+        other.close()
+    hs_o, hsd_o = O.setup(p)
+    err = rel_errors(hs, hsd, hs_o, hsd_o)
+    assert err["S"] <= TOL_H[5] and err["H"] <= TOL_H[5], err
