@@ -3,7 +3,7 @@ lapw1's radial set-up (ATPAR) and eigenvalues from the reference's shipped
 MgO runs.
 
 The WIEN2k tree ships complete MgO SCF runs under
-SRC_elast/example-MgO/elast/{eos,rhomb} whose last cycle wrote the spherical
+SRC_elast/example-MgO/elast/{eos,rhomb,tetra} whose last cycle wrote the spherical
 (case.vsp) and non-spherical (case.vns) potentials that its lapw1 read, and
 whose lapw1 printed (case.output1_*).  The input files are kept as text
 (the case-file readers of hack_wein2k_b200.case_files parse them in the
@@ -106,10 +106,10 @@ def parse_eigenvalues(paths):
 
 def main(ref):
     base = os.path.join(ref, "SRC_elast", "example-MgO", "elast")
-    out = {"source": "SRC_elast/example-MgO/elast/{eos,rhomb} of the reference tree: the input files case.struct, "
+    out = {"source": "SRC_elast/example-MgO/elast/{eos,rhomb,tetra} of the reference tree: the input files case.struct, "
                      "case.in1, case.klist, case.vsp, case.vns as text, and numbers printed by its lapw1 in "
                      "case.output1_*", "cases": {}}
-    for case in ("eos", "rhomb"):
+    for case in ("eos", "rhomb", "tetra"):
         d = os.path.join(base, case)
         files = {ext: open(os.path.join(d, case + "." + ext)).read() for ext in ("struct", "in1", "klist", "vsp", "vns")}
         st = parse_struct(os.path.join(d, case + ".struct"))

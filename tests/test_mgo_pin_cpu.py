@@ -1,7 +1,7 @@
 """End-to-end pin of the H/S setup against the reference's own MgO runs (CPU).
 
 tests/golden/mgo_atpar.json holds the input files of the reference's
-shipped MgO SCF runs (SRC_elast/example-MgO/elast/{eos,rhomb}: case.struct,
+shipped MgO SCF runs (SRC_elast/example-MgO/elast/{eos,rhomb,tetra}: case.struct,
 case.in1, case.klist and the case.vsp / case.vns potentials of the cycle
 whose lapw1 output is kept) and the numbers that lapw1 printed:
   * the searched energy parameters, the POTENTIAL PARAMETERS table
@@ -61,7 +61,11 @@ class Case:
                                     tns=tns, name=f"{self.name}-k{block}")
 
 
-@pytest.fixture(scope="module", params=["eos", "rhomb"])
+# per run: lattice, symmetry operations, LM terms of the potential per atom, k-points
+RUNS = {"eos": ("F", 48, 4, 165), "rhomb": ("R", 12, 6, 489), "tetra": ("F", 16, 5, 405)}
+
+
+@pytest.fixture(scope="module", params=sorted(RUNS))
 def case(request):
     return Case(request.param)
 
@@ -70,14 +74,15 @@ def test_case_file_readers(case):
     st = case.struct
     assert len(st.atoms) == 2 and [a.name for a in st.atoms] == ["Mg", "O"]
     assert all(a.jrj == 781 and abs(a.rmt - 1.7) < 1e-12 for a in st.atoms)
-    assert st.lattic == ("F" if case.name == "eos" else "R")
-    assert len(st.imat) == (48 if case.name == "eos" else 12)
+    lattic, nsym, nlm, nk = RUNS[case.name]
+    assert st.lattic == lattic
+    assert len(st.imat) == nsym
     assert case.in1.rkmax == 8.0 and case.in1.lmax == 10 and case.in1.lnsmax == 4
     assert (case.in1.emin, case.in1.emax) == (-7.0, 1.5)
     assert all(len(v) == 781 for v in case.vsp)
-    assert [len(x) for x in case.vns.lm] == ([4, 4] if case.name == "eos" else [6, 6])
+    assert [len(x) for x in case.vns.lm] == [nlm, nlm]
     assert len(case.vns.potk) > 50 and case.vns.potk[0][:3] == (0, 0, 0)
-    assert len(case.klist) == (165 if case.name == "eos" else 489)
+    assert len(case.klist) == nk
 
 
 def test_energy_search_matches_printed(case):

@@ -20,7 +20,7 @@ from tests.test_mgo_pin_cpu import TOL_EIG_RY, Case
 BLOCKS = [0, 3, 60]
 
 
-@pytest.fixture(scope="module", params=["eos", "rhomb"])
+@pytest.fixture(scope="module", params=["eos", "rhomb", "tetra"])
 def mgo(request):
     return Case(request.param)
 
