@@ -521,13 +521,20 @@ __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const doub
     const double uim = H.x * rj.y - H.y * rj.x;  // Im(conj(H) rho(J,I))
     const double vim = S.x * re.y - S.y * re.x;  // Im(conj(S) rhoE(J,I))
     const double g = act ? -2.0 * (uim - vim) : 0.0;
+    // the block's sum (every block of a column belongs to one atom): warp
+    // sums, then one atomic per component and block
+    __shared__ double wsum[4][3];  // blockDim.x = 128: 4 warps
 #pragma unroll
     for (int cc = 0; cc < 3; cc++) {
       double v = g * dxc[cc];
 #pragma unroll
       for (int o2 = 16; o2 > 0; o2 >>= 1) v += __shfl_down_sync(0xffffffffu, v, o2);
-      if (lane == 0) atomicAdd(&F[a * 3 + cc], v);
+      if (lane == 0) wsum[threadIdx.x >> 5][cc] = v;
     }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicAdd(&F[a * 3 + threadIdx.x], wsum[0][threadIdx.x] + wsum[1][threadIdx.x] +
+                                                          wsum[2][threadIdx.x] + wsum[3][threadIdx.x]);
+    __syncthreads();  // wsum is rewritten by the next equivalent atom
   }
 #undef LOV
 }
@@ -607,19 +614,24 @@ __global__ void __launch_bounds__(256, 1) k_force_hns_z(int zc, int nsl2, int K,
   const int nc = min(FRC_ZCOLS, ncol - c0);
   const double2* T = tns + (size_t)atype[a] * LAPW1GPU_NTNS * L1G_NSL2 * L1G_NSL2;
   const int nb = zc ? 3 : 6, b0 = zc ? 6 : 0;  // T blocks used
+  // staging by cp.async (every copy in flight at once; the block has one
+  // wave of work after it)
   for (int i = tid; i < nb * nsl2 * nsl2; i += blockDim.x) {
     const int blk = i / (nsl2 * nsl2), r = i % (nsl2 * nsl2), lm = r / nsl2, b = r % nsl2;
-    sT[(blk * L1G_NSL2 + lm) * L1G_NSL2 + b] = T[((size_t)(b0 + blk) * L1G_NSL2 + lm) * L1G_NSL2 + b];
+    frc_cp16(&sT[(blk * L1G_NSL2 + lm) * L1G_NSL2 + b], &T[((size_t)(b0 + blk) * L1G_NSL2 + lm) * L1G_NSL2 + b]);
   }
   for (int i = tid; i < nc * 3 * nsl2; i += blockDim.x) {
     const int cl = i / (3 * nsl2), r = i % (3 * nsl2), part = r / nsl2, b = r % nsl2;
-    double2 v = cmk(0.0, 0.0);
+    double2* dst = &sY[(cl * 3 + part) * L1G_NSL2 + b];
     if (part < 2)
-      v = Y[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + part * nsl2 + b];
+      frc_cp16(dst, &Y[(size_t)(c0 + cl) * K + (size_t)a * 2 * nsl2 + part * nsl2 + b]);
     else if (Yc)
-      v = Yc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + b];
-    sY[(cl * 3 + part) * L1G_NSL2 + b] = v;
+      frc_cp16(dst, &Yc[(size_t)(c0 + cl) * Kc + (size_t)a * nsl2 + b]);
+    else
+      *dst = cmk(0.0, 0.0);
   }
+  frc_commit();
+  frc_wait<0>();
   __syncthreads();
   // warp w: columns 32 (w % 4) + lane, outputs: zc = 0 the row r = w / 4
   // (lm = 0 .. nsl2-1), zc = 1 the lm half w / 4 of the single row
