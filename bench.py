@@ -360,7 +360,7 @@ def kc_bytes(p):
 
 
 # ---------------------------------------------------------------- the c4 line
-def north_star(args):
+def c4_step_line(args):
     import torch
 
     from hack_wein2k_b200 import forces as FO
@@ -591,7 +591,7 @@ def north_star(args):
     torch.cuda.empty_cache()
     acc3 = c3_accuracy(ctx, torch, dev, args.fd_components) if not args.no_extras else None
 
-    # ---- c1: the 40-atom single k-point (the line of the first build) ----
+    # ---- c1: the 40-atom single k-point ----
     c1 = c1_summary(ctx, torch, dev, stream) if not args.no_extras else None
     c2 = c2_batch(ctx, torch, dev, stream) if not args.no_extras else None
 
@@ -889,7 +889,7 @@ def fd_report(args):
 
 # ---------------------------------------------------------------- the c1 line
 def single_c1(args):
-    """The 40-atom c1 single-k-point setup (split vs FP64), the first build's line."""
+    """The 40-atom c1 single-k-point setup (split vs FP64) as its own line."""
     import torch
 
     from hack_wein2k_b200 import lapw1gpu, synth
@@ -993,7 +993,7 @@ def main():
         return fd_report(args)
     if args.workload == "c1":
         return single_c1(args)
-    return north_star(args)
+    return c4_step_line(args)
 
 
 if __name__ == "__main__":
