@@ -628,6 +628,17 @@ __global__ void k_hns_alm(DevProb P, const LoRange* __restrict__ lor, int nlor, 
   }
 }
 
+// 16-byte global -> shared copy that bypasses registers (cp.async), so that
+// a block's staging has all its loads in flight at once
+__device__ __forceinline__ void l1g_cp16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void l1g_cp_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 #define TMUL_I 64        // columns (basis rows i) per work item
 #define TMUL_ROWS 10     // rows of L per thread (one warp: 10 rows x 64 columns)
 #define TMUL_WARPS 5     // 5 x 10 >= 2 NSL2 = 50 rows
@@ -660,15 +671,19 @@ __global__ void __launch_bounds__(32 * TMUL_WARPS, 2) k_hns_tmul(int npad, int n
         const int row = idx / K, col = idx % K;
         const int ro = row / nsl2, la = row % nsl2, r = col / nsl2, b = col % nsl2;
         const int blk = ro == 0 ? (r == 0 ? 0 : 1) : (r == 0 ? 3 : 4);  // TUU TDU / TUD TDD
-        sM[idx] = T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b];
+        l1g_cp16(&sM[idx], &T[((size_t)blk * L1G_NSL2 + la) * L1G_NSL2 + b]);
       }
       staged = a;
     }
     const double2* R = Rop + (size_t)a * K * npad;
     for (int idx = tid; idx < K * TMUL_I; idx += 32 * TMUL_WARPS) {
       const int k = idx / TMUL_I, c = idx % TMUL_I;
-      sR[idx] = (i0 + c < npad) ? R[(size_t)k * npad + i0 + c] : make_double2(0.0, 0.0);
+      if (i0 + c < npad)
+        l1g_cp16(&sR[idx], &R[(size_t)k * npad + i0 + c]);
+      else
+        sR[idx] = make_double2(0.0, 0.0);
     }
+    l1g_cp_wait_all();
     __syncthreads();
     const int r0 = w * TMUL_ROWS;
     if (r0 < K) {  // warp-uniform
