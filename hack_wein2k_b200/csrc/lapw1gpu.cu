@@ -1348,7 +1348,8 @@ int lapw1gpu_set_tuning(lapw1gpu_context* c, const lapw1gpu_tuning* t) {
 }
 
 // Autotuner: the candidates of a tunable are timed on kp with the others
-// held, tunables one after another; the fastest is kept.  Each candidate's
+// held, tunables one after another; the fastest is kept if it beats the
+// value held before by more than 2%.  Each candidate's
 // time is its best of three runs, the runs of the candidates interleaved
 // (round r runs every candidate once) so that a drift of the clocks over
 // the tuning favours none of them, and it is the time of the kernel the
@@ -1377,6 +1378,10 @@ int lapw1gpu_autotune(lapw1gpu_context* c, lapw1gpu_kpoint* kp, double* d_hs, in
     size_t b = 0;
     for (size_t q = 1; q < cand.size(); q++)
       if (t[q] < t[b]) b = q;
+    // the value held before tuning stays unless another beats it by more
+    // than 2% (short timings of about a second in all drift by a few %)
+    for (size_t q = 0; q < cand.size(); q++)
+      if (cand[q] == v0 && t[b] > 0.98 * t[q]) b = q;
     *knob = cand[b];
     return LAPW1GPU_OK;
   };
