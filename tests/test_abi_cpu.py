@@ -45,6 +45,18 @@ def test_init_without_device_reports_nodevice():
     assert not h.value
 
 
+def test_last_error_is_an_empty_string_before_any_cuda_failure():
+    """lapw1gpu_last_error names the CUDA call behind a LAPW1GPU_ERR_CUDA;
+    in a fresh thread that has had none it is the empty string."""
+    import threading
+    lib = lapw1gpu.load()
+    out = []
+    t = threading.Thread(target=lambda: out.append(lib.lapw1gpu_last_error()))
+    t.start()
+    t.join()
+    assert out == [b""]
+
+
 def test_problem_struct_layout_matches_header():
     """Field order of the ctypes mirror follows the C struct."""
     from hack_wein2k_b200.problem import CProblem
