@@ -87,6 +87,16 @@ struct lapw1gpu_context {
   int* d_status = nullptr;
   int last_status = 0;
   bool status_pending = false;  // an asynchronous run has not been read back
+  // a setup queued by lapw1gpu_setup_async, ended by lapw1gpu_setup_wait
+  struct lapw1gpu_kpoint* async_k = nullptr;  // its uploaded inputs (freed by the wait)
+  int* h_async_status = nullptr;              // mapped host word: its status word
+  int* h_async_status_dev = nullptr;          //   (the device view of it)
+  int* h_status = nullptr;                    // mapped host word: the status of a synchronous call
+  int* h_status_dev = nullptr;
+  cudaEvent_t async_done = nullptr;           // its kernels and status copy (main stream)
+  bool async_copies = false;                  // HS copies queued on the copy stream (ev[11] ends them)
+  int async_nl = 0;
+  bool async_pending = false;
   int prec = LAPW1GPU_PREC_FP64;
   int slices = 5;      // int8 slices of the spherical part (split precision)
   int slices_hns = 5;  // int8 slices of the HNS update
@@ -246,6 +256,27 @@ namespace {
     }                                                   \
   } while (0)
 
+// one thread stores the device status word into a mapped host word
+__global__ void k_status_out(const int* __restrict__ d, int* h) { *(volatile int*)h = *d; }
+
+// The status word after the work queued on s: through the mapped host word
+// (no copy engine), else by a copy.  Synchronises s; counts its launch in *nl.
+static int read_status(lapw1gpu_context* c, cudaStream_t s, int* out, int* nl = nullptr) {
+  if (c->h_status) {
+    k_status_out<<<1, 1, 0, s>>>(c->d_status, c->h_status_dev);
+    CK(cudaGetLastError());
+    if (nl) ++*nl;
+    CK(cudaStreamSynchronize(s));
+    *out = *(volatile int*)c->h_status;
+    return LAPW1GPU_OK;
+  }
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *out = h;
+  return LAPW1GPU_OK;
+}
+
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 // validation of the caller's problem (the checks the reference makes by
@@ -335,6 +366,26 @@ int lapw1gpu_init(int device, lapw1gpu_context** out) {
     cudaEventCreateWithFlags(&c->auxf[i], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->auxj[i], cudaEventDisableTiming);
   }
+  cudaEventCreateWithFlags(&c->async_done, cudaEventDisableTiming);
+  // status words read back through mapped host memory (a one-thread kernel
+  // stores them), not by copies, which would queue behind a running
+  // lapw1gpu_setup_async's HS copies on the copy engines
+  for (int** w : {&c->h_async_status, &c->h_status}) {
+    if (cudaHostAlloc(w, sizeof(int), cudaHostAllocMapped) != cudaSuccess) {
+      cudaGetLastError();
+      *w = nullptr;
+    }
+  }
+  if (c->h_async_status && cudaHostGetDevicePointer(&c->h_async_status_dev, c->h_async_status, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeHost(c->h_async_status);
+    c->h_async_status = nullptr;
+  }
+  if (c->h_status && cudaHostGetDevicePointer(&c->h_status_dev, c->h_status, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeHost(c->h_status);
+    c->h_status = nullptr;
+  }
   if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     delete c;
@@ -357,6 +408,10 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   for (auto& kv : c->bufs)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   for (auto& kv : c->tiles) cudaFree(kv.second.first);
+  if (c->async_pending && c->async_k) lapw1gpu_kpoint_free(c->async_k);
+  if (c->h_async_status) cudaFreeHost(c->h_async_status);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->async_done) cudaEventDestroy(c->async_done);
   if (c->d_status) cudaFree(c->d_status);
   for (auto& e : c->ev) cudaEventDestroy(e);
   for (auto& e : c->fev) cudaEventDestroy(e);
@@ -459,9 +514,7 @@ int lapw1gpu_last_status(lapw1gpu_context* c) {
   if (!c) return 0;
   if (c->status_pending) {  // the last run was asynchronous: wait for it and read its status
     int hstat = 0;
-    if (cudaSetDevice(c->device) == cudaSuccess &&
-        cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
-        cudaStreamSynchronize(c->stream) == cudaSuccess)
+    if (cudaSetDevice(c->device) == cudaSuccess && read_status(c, c->stream, &hstat) == LAPW1GPU_OK)
       c->last_status = hstat;
     c->status_pending = false;
   }
@@ -1213,12 +1266,12 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* c, lapw1gpu_kpoint* k, int stages, dou
   c->status_pending = !st;
   if (st) {
     int hstat = 0;
-    CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    if (int rc2 = read_status(c, s, &hstat, &nl)) return rc2;
+    c->last_launches = nl;
     c->last_status = hstat;
     fill_stats(c, k, nl, st);
-    if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
     if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+    if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
     if (hstat) return LAPW1GPU_ERR_RANGE;
   }
   return LAPW1GPU_OK;
@@ -1302,22 +1355,23 @@ int lapw1gpu_setup_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int n
   CK(cudaEventRecord(c->ev[6], c->stream));
   const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
   int hstat = 0;
-  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  int nl = g->launches;
+  if (int rc2 = read_status(c, c->stream, &hstat, &nl)) return rc2;
   c->last_status = hstat;
   c->status_pending = false;
-  c->last_launches = g->launches;
+  c->last_launches = nl;
   if (st) {
     memset(st, 0, sizeof(*st));
     float tot = 0.f;
     cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]);
     st->ms_total = tot;
     for (int i = 0; i < nk; i++) st->flops_fp64_equiv += alg_flops(kps[i]);
-    st->kernel_launches = g->launches;
+    st->kernel_launches = nl;
     st->ms_host = host_ms;
   }
-  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+  // a timed-out wait leaves elements unwritten, which later finite checks see
   if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
   if (hstat) return LAPW1GPU_ERR_RANGE;
   return LAPW1GPU_OK;
 }
@@ -1442,9 +1496,15 @@ static int hns_granule(const lapw1gpu_context* c) {
 // columns [c0, c0+w), the rows above c0 as soon as HAMILT ends; the rest of
 // each panel follows the last stage.
 #define L1G_D2H_PANEL 256
-int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs_, int ldhs,
-                          double* hsdiag_, lapw1gpu_stats* st) {
+// The host-buffer setup.  async: return once everything is queued, the
+// copies of HS/HSDIAG left running on the copy stream and the status word
+// copied into page-locked memory behind the kernels (lapw1gpu_setup_wait
+// ends it); else wait for all of it.
+static int setup_host_impl(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs_, int ldhs,
+                           double* hsdiag_, lapw1gpu_stats* st, bool async) {
   if (!c || !p || !hs_ || !hsdiag_ || ldhs < p->n) return LAPW1GPU_ERR_ARG;
+  if (c->async_pending) return LAPW1GPU_ERR_ARG;  // one queued setup at a time
+  if (async && !c->h_async_status) return LAPW1GPU_ERR_NOMEM;
   CK(cudaSetDevice(c->device));
   double2* hs = reinterpret_cast<double2*>(hs_);
   double2* hsdiag = reinterpret_cast<double2*>(hsdiag_);
@@ -1528,7 +1588,7 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
           rc = LAPW1GPU_ERR_CUDA;
       }
       CK(cudaEventRecord(ecp, cs));
-      CK(cudaStreamWaitEvent(s, ecp, 0));
+      if (!async) CK(cudaStreamWaitEvent(s, ecp, 0));
     } else if (overlap) {
       // c->ev[3] marks the end of HAMILT (+ LO columns) on s
       CK(cudaStreamWaitEvent(cs, c->ev[3], 0));
@@ -1554,14 +1614,24 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
                               w, cudaMemcpyDeviceToHost, s) != cudaSuccess)
           rc = LAPW1GPU_ERR_CUDA;
       }
-      CK(cudaStreamWaitEvent(s, ecp, 0));
+      if (!async) CK(cudaStreamWaitEvent(s, ecp, 0));
+    }
+    if (async && rc == LAPW1GPU_OK) {
+      CK(cudaEventRecord(e3, s));
+      k_status_out<<<1, 1, 0, s>>>(c->d_status, c->h_async_status_dev);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(c->async_done, s));
+      c->async_k = k;
+      c->async_copies = grouped || overlap;
+      c->async_nl = nl + 1;
+      c->async_pending = true;
+      return LAPW1GPU_OK;
     }
   }
   CK(cudaEventRecord(e3, s));
   int hstat = 0;
-  if (cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    rc = rc ? rc : LAPW1GPU_ERR_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+  if (read_status(c, s, &hstat, &nl) != LAPW1GPU_OK) rc = rc ? rc : LAPW1GPU_ERR_CUDA;
+  c->last_launches = nl;
   c->last_status = hstat;
   c->status_pending = false;
   if (st && rc == LAPW1GPU_OK) {
@@ -1574,8 +1644,47 @@ int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int st
   }
   lapw1gpu_kpoint_free(k);
   if (rc) return rc;
-  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+  // a timed-out wait leaves elements unwritten, which later finite checks see
   if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
+  if (hstat) return LAPW1GPU_ERR_RANGE;
+  return LAPW1GPU_OK;
+}
+
+int lapw1gpu_setup_stages(lapw1gpu_context* c, const lapw1gpu_problem* p, int stages, double* hs, int ldhs,
+                          double* hsdiag, lapw1gpu_stats* st) {
+  return setup_host_impl(c, p, stages, hs, ldhs, hsdiag, st, false);
+}
+
+int lapw1gpu_setup_async(lapw1gpu_context* c, const lapw1gpu_problem* p, double* hs, int ldhs, double* hsdiag) {
+  return setup_host_impl(c, p, 7, hs, ldhs, hsdiag, nullptr, true);
+}
+
+int lapw1gpu_setup_wait(lapw1gpu_context* c, lapw1gpu_stats* st) {
+  if (!c || !c->async_pending) return LAPW1GPU_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  int rc = LAPW1GPU_OK;
+  if (cudaEventSynchronize(c->async_done) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+  if (c->async_copies && cudaEventSynchronize(c->ev[11]) != cudaSuccess) rc = LAPW1GPU_ERR_CUDA;
+  if (rc) cudaGetLastError();
+  const int hstat = *c->h_async_status;
+  c->last_status = hstat;
+  c->status_pending = false;
+  c->last_launches = c->async_nl;
+  if (st && rc == LAPW1GPU_OK) {
+    fill_stats(c, c->async_k, c->async_nl, st);
+    float a = 0.f;
+    cudaEventElapsedTime(&a, c->ev[7], c->ev[8]);
+    st->ms_h2d = a;
+    st->ms_d2h = 0.0;  // the copies run behind later work on the copy stream
+  }
+  lapw1gpu_kpoint_free(c->async_k);
+  c->async_k = nullptr;
+  c->async_pending = false;
+  if (rc) return rc;
+  // a timed-out wait leaves elements unwritten, which later finite checks see
+  if (hstat & L1G_STATUS_TIMEOUT) return LAPW1GPU_ERR_TIMEOUT;
+  if (hstat & L1G_STATUS_NONFINITE) return LAPW1GPU_ERR_NONFINITE;
   if (hstat) return LAPW1GPU_ERR_RANGE;
   return LAPW1GPU_OK;
 }
@@ -1860,8 +1969,7 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c, 
   rc = forces_enqueue(c, k, d_c, ldc, nb, d_occ, d_eps, d_grad, true, &nl);
   if (rc) return rc;
   int hstat = 0;
-  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  if (int rc2 = read_status(c, s, &hstat, &nl)) return rc2;
   c->last_status = hstat;
   c->status_pending = false;
   c->last_launches = nl;
@@ -1892,8 +2000,7 @@ int lapw1gpu_forces_batch(lapw1gpu_context* c, lapw1gpu_kpoint* const* kps, int 
   }
   CK(cudaEventRecord(c->ev[6], s));
   int hstat = 0;
-  CK(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  if (int rc2 = read_status(c, s, &hstat, &nl)) return rc2;
   c->last_status = hstat;
   c->status_pending = false;
   c->last_launches = nl;

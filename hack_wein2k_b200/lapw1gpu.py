@@ -32,6 +32,7 @@ EXPORTS = [
     "lapw1gpu_init", "lapw1gpu_finalize", "lapw1gpu_set_precision", "lapw1gpu_kpoint_upload",
     "lapw1gpu_kpoint_free", "lapw1gpu_kpoint_run", "lapw1gpu_setup", "lapw1gpu_setup_stages",
     "lapw1gpu_stream", "lapw1gpu_last_status", "lapw1gpu_tns_from_gaunt", "lapw1gpu_version", "lapw1gpu_last_error",
+    "lapw1gpu_setup_async", "lapw1gpu_setup_wait",
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
     "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices", "lapw1gpu_test_wait_timeout",
     "lapw1gpu_last_launches", "lapw1gpu_host_register", "lapw1gpu_host_unregister", "lapw1gpu_forces_stats",
@@ -85,6 +86,8 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_stream.restype = vp
     lib.lapw1gpu_last_status.argtypes = [vp]
     lib.lapw1gpu_version.restype = C.c_char_p
+    lib.lapw1gpu_setup_async.argtypes = [vp, C.POINTER(CProblem), C.c_void_p, C.c_int, C.c_void_p]
+    lib.lapw1gpu_setup_wait.argtypes = [vp, C.POINTER(CStats)]
     lib.lapw1gpu_last_error.restype = C.c_char_p
     lib.lapw1gpu_tns_from_gaunt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, dp,
                                             dp, dp, dp, ip, dp]
@@ -231,6 +234,25 @@ class Context:
         if stats:
             return hs, hsdiag, st.as_dict()
         return hs, hsdiag
+
+    def setup_async(self, prob: Problem, hs: np.ndarray, hsdiag: np.ndarray) -> None:
+        """lapw1gpu_setup_async into host buffers (HS Fortran-ordered); the
+        problem's arrays and the buffers are held until setup_wait."""
+        n = prob.n
+        assert hs.flags.f_contiguous and hs.dtype == np.complex128 and hs.shape[0] >= n
+        cp = prob.to_c()
+        rc = self.lib.lapw1gpu_setup_async(self.h, C.byref(cp), hs.ctypes.data, hs.shape[0], hsdiag.ctypes.data)
+        _check("lapw1gpu_setup_async", rc)
+        self._async_keep = (cp, hs, hsdiag)
+
+    def setup_wait(self, stats: bool = False):
+        """lapw1gpu_setup_wait: (HS, HSDIAG[, stats]) of the queued setup."""
+        st = CStats()
+        rc = self.lib.lapw1gpu_setup_wait(self.h, C.byref(st))
+        keep, self._async_keep = getattr(self, "_async_keep", None), None
+        _check("lapw1gpu_setup_wait", rc)
+        hs, hsdiag = keep[1], keep[2]
+        return (hs, hsdiag, st.as_dict()) if stats else (hs, hsdiag)
 
     def upload(self, prob: Problem) -> KPoint:
         return KPoint(self, prob)

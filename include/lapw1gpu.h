@@ -206,6 +206,20 @@ int lapw1gpu_kpoint_run(lapw1gpu_context* ctx, lapw1gpu_kpoint* kp, int stages,
  * Synchronous: returns when hs/hsdiag hold the result. */
 int lapw1gpu_setup(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
                    double* hs, int ldhs, double* hsdiag, lapw1gpu_stats* st);
+/* lapw1gpu_setup without the wait: returns once the setup's kernels and
+ * the copies of HS/HSDIAG into the caller's buffers are queued.  The copies
+ * run on the context's copy stream behind the kernels that produce each
+ * column group, so later device work on the context's stream (the device
+ * eigen-solve, lapw1gpu_forces of a resident k-point) overlaps them.
+ * lapw1gpu_setup_wait ends it: it waits for the kernels and the copies and
+ * returns the status lapw1gpu_setup would have returned (st optional).
+ * Until then hs, hsdiag and the problem's host arrays stay valid and
+ * unchanged, and no other lapw1gpu_setup* call is made on the context
+ * (they return LAPW1GPU_ERR_ARG).  No counterpart in the reference (its
+ * CALKPT is sequential). */
+int lapw1gpu_setup_async(lapw1gpu_context* ctx, const lapw1gpu_problem* p,
+                         double* hs, int ldhs, double* hsdiag);
+int lapw1gpu_setup_wait(lapw1gpu_context* ctx, lapw1gpu_stats* st);
 
 /* lapw1gpu_setup restricted to the given stages (parity tests of each
  * reference routine). */

@@ -156,3 +156,37 @@ def test_forces_batch_equals_single_calls(ctx, prec):
     assert ms > 0
     for g, r in zip(gs, ref):
         assert np.abs(g.cpu().numpy() - r).max() <= 1e-12 * np.abs(r).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [lapw1gpu.PREC_FP64, lapw1gpu.PREC_SPLIT])
+def test_setup_async_with_forces_in_between(ctx, prec):
+    """lapw1gpu_setup_async, then lapw1gpu_forces of another, resident
+    k-point while the HS copies run, then lapw1gpu_setup_wait: the host HS
+    and HSDIAG equal the synchronous setup's bit for bit, and the forces
+    equal a call made alone (up to the order of their atomic sums)."""
+    from hack_wein2k_b200 import forces as FO
+    dev = torch.device("cuda", ctx.device)
+    ctx.set_precision(prec, 5)
+    try:
+        occ = torch.ones(8, dtype=torch.float64, device=dev)
+        _, w, X, kp = FO.band_energy(ctx, synth.small_case("lo"), occ)
+        g_alone = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+        p = synth.config("c0")[0]
+        hs_s, hd_s = ctx.setup(p)
+        n = p.n
+        hs = np.zeros((n, n), dtype=np.complex128, order="F")
+        hd = np.zeros(n, dtype=np.complex128)
+        Xc = X.transpose(0, 1).contiguous()
+        g = torch.empty_like(torch.from_numpy(g_alone)).to(dev)
+        torch.cuda.synchronize(dev)
+        ctx.setup_async(p, hs, hd)
+        kp.forces(Xc.data_ptr(), X.shape[0], X.shape[1], occ.data_ptr(), w.contiguous().data_ptr(), g.data_ptr())
+        hs_a, hd_a = ctx.setup_wait()
+        kp.free()
+    finally:
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    assert hs_a is hs and hd_a is hd
+    assert np.array_equal(hs, hs_s) and np.array_equal(hd, hd_s)
+    g = g.cpu().numpy()
+    assert np.abs(g - g_alone).max() <= 1e-12 * np.abs(g_alone).max()
