@@ -314,12 +314,26 @@ def _sph_pairs(p):
     return p.nv * (p.nv - 1) / 2.0
 
 
-def force_sph_flops(p):
+def force_sph_flops(p, block=None):
     """FP64 flops of k_force_sph (FMA = 2): per plane-wave pair J < I and
     atom type, the l = 0 term (6) and 10 per further l (two 2-vector dot
     products weighted into the S and H sums); per pair and atom 21 (phase
-    product, the two imaginary parts, the pair term and its dK weighting)."""
-    return _sph_pairs(p) * (p.nat * (6.0 + 10.0 * (p.ltop - 1)) + 21.0 * p.ndf)
+    product, the two imaginary parts, the pair term and its dK weighting).
+    With the spherical projections (block rows per block) the kernel takes
+    the pairs inside a block only."""
+    if block:
+        pairs = sum(min(block, p.nv - r0) * (min(block, p.nv - r0) - 1) / 2.0 for r0 in range(0, p.nv, block))
+    else:
+        pairs = _sph_pairs(p)
+    return pairs * (p.nat * (6.0 + 10.0 * (p.ltop - 1)) + 21.0 * p.ndf)
+
+
+def force_proj_ops(p, nb, S):
+    """int8 ops of the adjoint's spherical projections: output K x 4 nb
+    complex (K = 2 NDF ltop^2 real-harmonic rows), inner NV complex, 8 real
+    ops per complex multiply-add, S(S+1)/2 slice products"""
+    K = 2.0 * p.ndf * p.ltop ** 2
+    return 8.0 * K * 4.0 * nb * p.nv * (S * (S + 1) / 2.0)
 
 
 def sph_tc_ops(p, S):
@@ -390,6 +404,7 @@ def c4_step_line(args):
             ctx.set_precision(lapw1gpu.PREC_SPLIT, s_sph)
             ctx.set_slices(s_sph, s_hns)
             ctx.set_force_slices(*args.force_slices)
+            ctx.set_force_projection(*args.force_projection)
 
     def bar():
         if dist is not None:
@@ -491,6 +506,10 @@ def c4_step_line(args):
         kps[i].forces(Xc[i].data_ptr(), q.n, NBANDS, occ.data_ptr(), W[i].data_ptr(), grads[i].data_ptr())
         fst_split.append(ctx.forces_stats())
     ms_fsph_split = float(np.mean([f["ms_sph_main"] for f in fst_split]))
+    ms_fproj_split = float(np.mean([f["ms_sph_slice"] for f in fst_split]))
+    fproj_on = ms_fproj_split > 0.0
+    fproj_s = args.force_projection[0] if args.force_projection[0] > 0 else 6
+    fproj_b = args.force_projection[1] if fproj_on else None
     # per-kernel times of one split k-point (stats pass)
     st_k = kps[0].run(hs[0].data_ptr(), ps[0].n, hd[0].data_ptr(), stats=True)
 
@@ -617,7 +636,8 @@ def c4_step_line(args):
     hbm = peaks.get("hbm_gbs", 6650.0)
     albl_b, slicer_b = ka_bytes(p0, s_sph)
     kern = {
-        "k_force_sph (adjoint pair sums, FP64)": ("fp64", force_sph_flops(p0), ms_fsph_split, "TFLOP/s", fp64_peak),
+        "k_force_sph (adjoint pair sums, FP64)": ("fp64", force_sph_flops(p0, fproj_b), ms_fsph_split, "TFLOP/s",
+                                                  fp64_peak),
         "k_sph_tc (K-b, tcgen05 int8)": ("tensor", sph_tc_ops(p0, s_sph), st_k["ms_sph_main"], "TOP/s", int8_peak),
         "k_split_gemm (K-ns, tcgen05 int8)": ("tensor", split_gemm_ops(p0, s_hns), st_k["ms_hns_main"], "TOP/s",
                                               int8_peak),
@@ -625,6 +645,10 @@ def c4_step_line(args):
         "k_sph_slice x2 (K-a, split operands)": ("hbm", slicer_b, st_k["ms_sph_slice"], "GB/s", hbm),
         "k_table (K-c)": ("hbm", kc_bytes(p0), st_k["ms_table"], "GB/s", hbm),
     }
+
+    if fproj_on:
+        kern["k_split_gemm (adjoint spherical projections, tcgen05 int8, with their operand slicing)"] = (
+            "tensor", force_proj_ops(p0, NBANDS, fproj_s), ms_fproj_split, "TOP/s", int8_peak)
 
     def rate(w, t, unit):
         if t <= 0:
@@ -646,6 +670,9 @@ def c4_step_line(args):
             tr4 = {}
     for name in kd:  # DRAM bytes per launch from the ncu captures (profiles/traffic.json)
         kd[name]["traffic"] = tr4.get(name)
+    fs = "k_force_sph (adjoint pair sums, FP64)"
+    if fproj_on and kd[fs]["traffic"]:  # the capture covers every pair; with projections it takes the block pairs
+        kd[fs]["traffic"] *= force_sph_flops(p0, fproj_b) / force_sph_flops(p0)
     traffic = tr4.get(dom)
     dm = kd[dom]
     roofline = {"kernel": dom, "bound": dm["bound"], "achieved": dm["achieved"], "peak": dm["peak"],
@@ -669,9 +696,10 @@ def c4_step_line(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": f"int8 x{s_sph}/x{s_hns}/x{args.force_slices[0]}/x{args.force_slices[1]} slices (spherical/HNS/"
-                 "adjoint density matrices/adjoint HNS projections) with f64 combine; "
-                 "f64 force pair sums",
+        "dtype": f"int8 x{s_sph}/x{s_hns}/x{args.force_slices[0]}/x{args.force_slices[1]}"
+                 + (f"/x{fproj_s}" if fproj_on else "") + " slices (spherical/HNS/adjoint density matrices/"
+                 "adjoint HNS projections" + ("/adjoint spherical projections" if fproj_on else "")
+                 + ") with f64 combine; f64 force pair sums" + (" inside row blocks" if fproj_on else ""),
         "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD_C4, "kpoints_per_gpu": NK, "n": [q.n for q in ps], "nv0": p0.nv,
                    "nlo": p0.nlo, "atoms": p0.ndf, "bands": NBANDS, "lmax": p0.ltop - 1, "lmax_ns": p0.lnsmax,
@@ -686,7 +714,9 @@ def c4_step_line(args):
         "forces": {"split_ms_per_kpoint": ms_forces_split, "fp64_ms_per_kpoint": ms_forces_fp64,
                    "split_forces_per_s": 3 * p0.ndf / (ms_forces_split * 1e-3),
                    "fp64_forces_per_s": 3 * p0.ndf / (ms_forces_fp64 * 1e-3),
-                   "k_force_sph_ms": ms_fsph_split, "stats_k0": fst_split[0]},
+                   "k_force_sph_ms": ms_fsph_split, "projection_products_ms": ms_fproj_split,
+                   "projections": ({"slices": fproj_s, "block_rows": args.force_projection[1]} if fproj_on
+                                   else None), "stats_k0": fst_split[0]},
         "fp64_path": {"ms_per_kpoint": ms64 / NK, "speedup_split_over_fp64": (ms64 / NK) / value,
                       "tuning": tun_fp64},
         "tuning": tun_split,
@@ -990,6 +1020,9 @@ def main():
     ap.add_argument("--force-slices", type=int, nargs=2, default=[6, 4], metavar=("RHO", "PROJ"),
                     help="int8 slices of the adjoint's density matrices and of its HNS projections (the "
                          "density matrices carry the force error; 4-slice projections leave it unchanged at c4)")
+    ap.add_argument("--force-projection", type=int, nargs=2, default=[-1, 1024], metavar=("SLICES", "BLOCK"),
+                    help="the adjoint's spherical pairs of different BLOCK-row blocks as int8 slice projections "
+                         "(lapw1gpu_set_force_projection; -1: 6 slices from 6 blocks, 0: the FP64 pair kernel)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["c4", "c1"], default="c4")
     ap.add_argument("--fd-components", type=int, default=3,

@@ -400,6 +400,208 @@ __global__ void __launch_bounds__(256) k_force_step(DevProb P, TabDesc T, const 
   if (threadIdx.x < 3) atomicAdd(&F[a * 3 + threadIdx.x], red[threadIdx.x][0]);
 }
 
+// ---------------------------------------------------------------------
+// The spherical pair sums as projections (split precision).
+//
+// By the addition theorem (2l+1) P_l(u.v) = sum_m Z_lm(u) Z_lm(v) for the
+// real spherical harmonics Z_lm scaled as below, so the type term of a pair
+// factors into row vectors: tH(I,J) = sum_(l,m) sum_(alpha,beta)
+// A^alpha_J Z_lm(J) M^(alpha beta)_l A^beta_I Z_lm(I) with A = (al, bl),
+// M_H = vif (mAA mAB / mBA mBB), M_S = vif diag(1, chn).  With y_b(I) =
+// conj(phase_a(I)) c_b(I), conj(phase_J) phase_I rho(J,I) = sum_b f_b y_b(J)
+// conj(y_b(I)), and with kappa = 2 pi KZZ the pair weight -4 pi (KZZ_I -
+// KZZ_J) = -2 (kappa_I - kappa_J), so that the PW x PW part of atom a's
+// gradient over pairs J < I with J in a set Jset and I in a set Iset is
+//   -2 sum_(l,m,alpha,beta,b) M^(alpha beta)_l (f_b | f_b eps_b) Im(
+//       Pj_alpha conj(Yk_beta) - Pk_alpha conj(Y_beta))
+// where P = sum_(J in Jset) A^alpha Z_lm conj(phase_a) (c, kappa c)(J) and Y
+// the same over Iset.  J < I is a triangle, not a product of two sets: the
+// PW rows are cut into blocks of B rows; the pairs of two different blocks
+// are the projections of block p (Y) against the sum of the projections of
+// the blocks before it (the prefix P), the pairs inside a block go through
+// k_force_sph on the diagonal tiles.  The projections are int8 slice
+// products (k_split_gemm) of the left operand of k_force_rsph with (G c)^T.
+// Rows whose |k| is 0 use the direction z (their al, bl vanish for l > 0).
+// The pair kernel uses P_l = x P_(l-1) for |x| >= 0.9999999 (hamilt.F's
+// UTOP branch); the projections use P_l itself (the same value at |x| = 1).
+
+// Z_lm(u) for the unit vector u, lm = l l + l + m: m = 0: N_l0 Q_l0(uz);
+// m > 0 and m < 0: sqrt(2) N_l|m| Q_l|m|(uz) times Re and Im of (ux + i uy)^|m|,
+// with P_l^m = (1 - uz^2)^(m/2) Q_lm (no Condon-Shortley phase; Q_mm =
+// (2m-1)!!, Q_(m+1)m = (2m+1) uz Q_mm, then the three-term recursion in l)
+// and N_lm = sqrt((2l+1) (l-m)!/(l+m)!), so that sum_m Z_lm(u) Z_lm(v) =
+// (2l+1) P_l(u.v).
+__device__ double frc_zlm(double ux, double uy, double uz, int l, int m) {
+  const int am = m < 0 ? -m : m;
+  double q0 = 1.0;
+  for (int k = 1; k <= am; k++) q0 *= (double)(2 * k - 1);
+  double q = q0;
+  if (l > am) {
+    double qm2 = q0, qm1 = (double)(2 * am + 1) * uz * q0;
+    for (int ll = am + 2; ll <= l; ll++) {
+      const double qn = ((double)(2 * ll - 1) * uz * qm1 - (double)(ll + am - 1) * qm2) / (double)(ll - am);
+      qm2 = qm1;
+      qm1 = qn;
+    }
+    q = qm1;
+  }
+  double fr = 1.0;
+  for (int k = l - am + 1; k <= l + am; k++) fr /= (double)k;
+  const double nrm = sqrt((double)(2 * l + 1) * fr);
+  if (am == 0) return nrm * q;
+  double cr = 1.0, ci = 0.0;
+  for (int k = 0; k < am; k++) {
+    const double tr = cr * ux - ci * uy;
+    ci = cr * uy + ci * ux;
+    cr = tr;
+  }
+  return 1.4142135623730951 * nrm * q * (m > 0 ? cr : ci);
+}
+
+__device__ __forceinline__ int frc_lof(int lm) {
+  int l = (int)sqrt((double)lm);
+  while (l * l > lm) l--;
+  while ((l + 1) * (l + 1) <= lm) l++;
+  return l;
+}
+
+// Left operand of the projections, k-major: row I < NV of Lt (stride ld)
+// holds, at r = (a 2 + alpha) ltop^2 + lm, A^alpha_(t l)(I) Z_lm(k_I)
+// conj(phase_a(I)) for atom a of type t (alpha 0: al, 1: bl).  One block
+// per row.
+__global__ void __launch_bounds__(256) k_force_rsph(DevProb P, double2* __restrict__ Lt, int ld) {
+  __shared__ double z[L1G_MAXL * L1G_MAXL];
+  __shared__ unsigned char lof[L1G_MAXL * L1G_MAXL];
+  const int I = blockIdx.x;
+  const int L2 = P.ltop * P.ltop;
+  if ((int)threadIdx.x < L2) {
+    double ux = 0.0, uy = 0.0, uz = 1.0;
+    const double r = P.rk[I];
+    if (r > 0.0) {
+      ux = P.xk[I] / r;
+      uy = P.yk[I] / r;
+      uz = P.zk[I] / r;
+    }
+    const int lm = threadIdx.x, l = frc_lof(lm);
+    z[lm] = frc_zlm(ux, uy, uz, l, lm - l * l - l);
+    lof[lm] = (unsigned char)l;
+  }
+  __syncthreads();
+  const int per = 2 * L2, K = P.ndf * per;
+  double2* out = Lt + (size_t)I * ld;
+  for (int r = threadIdx.x; r < K; r += blockDim.x) {
+    const int a = r / per, rem = r - a * per, alpha = rem >= L2 ? 1 : 0, lm = rem - alpha * L2;
+    const size_t o = ((size_t)P.atype[a] * P.ltop + lof[lm]) * P.nvpad + I;
+    const double v = (alpha ? P.bl[o] : P.al[o]) * z[lm];
+    const double2 ph = P.phase[(size_t)a * P.npad + I];
+    out[r] = cmk(v * ph.x, -v * ph.y);
+  }
+}
+
+// One block of rows against the prefix: Y and Pre are K x 4nb column-major
+// (stride ld; column g nb + b: g = 0 the plain projection of band b, g =
+// 1..3 the kappa_g-weighted one), rows r = (a 2 + alpha) ltop^2 + lm.
+// Adds block p's cross-block pair sums to F and, with update, Pre += Y.
+// One block per (atom, FRC_PB bands); thread = lm, both alpha rows.
+#define FRC_PB 8
+// the default (lapw1gpu_set_force_projection slices -1): 6 slices (at 5 the
+// c1 adjoint's error grew from 2.5e-8 to 1.2e-5 of its largest component),
+// on when the PW rows span 6 blocks (at c1, 4.5 blocks of 1024 rows, the
+// projections took 6.97 ms against 6.09 for the pair kernel alone; at c4,
+// 11.6 blocks, 57.3 against 73.7 ms for the whole adjoint)
+#define L1G_FSP_SLICES 6
+#define L1G_FSP_MIN_BLOCKS 6
+__global__ void __launch_bounds__(128) k_force_pre(DevProb P, const SphCoef* __restrict__ coef,
+                                                   const double2* __restrict__ Y, double2* __restrict__ Pre, int ld,
+                                                   int nb, const double* __restrict__ f,
+                                                   const double* __restrict__ eps, int update,
+                                                   double* __restrict__ F) {
+  __shared__ double red[4][3];
+  const int a = blockIdx.x, b0 = blockIdx.y * FRC_PB, b1 = min(nb, b0 + FRC_PB);
+  const int L2 = P.ltop * P.ltop, t = P.atype[a];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int lm = threadIdx.x; lm < L2; lm += blockDim.x) {
+    const SphCoef cf = coef[t * P.ltop + frc_lof(lm)];
+    const double hAA = cf.vif * cf.mAA, hAB = cf.vif * cf.mAB, hBA = cf.vif * cf.mBA, hBB = cf.vif * cf.mBB;
+    const double sAA = cf.vif, sBB = cf.vif * cf.chn;
+    const size_t r0 = (size_t)a * 2 * L2 + lm, r1 = r0 + L2;
+    for (int b = b0; b < b1; b++) {
+      double2 p[2][4], y[2][4];
+#pragma unroll
+      for (int g = 0; g < 4; g++) {
+        const size_t o = (size_t)(g * nb + b) * ld;
+        p[0][g] = Pre[o + r0];
+        p[1][g] = Pre[o + r1];
+        y[0][g] = Y[o + r0];
+        y[1][g] = Y[o + r1];
+      }
+      const double fb = f[b], fe = f[b] * eps[b];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double X[2][2];
+#pragma unroll
+        for (int al = 0; al < 2; al++)
+#pragma unroll
+          for (int be = 0; be < 2; be++) {
+            // Im(p conj(y)) = p.y y.x - p.x y.y
+            const double2 p0 = p[al][0], pk = p[al][c + 1], y0 = y[be][0], yk = y[be][c + 1];
+            X[al][be] = fma(p0.y, yk.x, -(p0.x * yk.y)) - fma(pk.y, y0.x, -(pk.x * y0.y));
+          }
+        const double tH = fma(hAA, X[0][0], fma(hAB, X[0][1], fma(hBA, X[1][0], hBB * X[1][1])));
+        const double tS = fma(sAA, X[0][0], sBB * X[1][1]);
+        acc[c] = fma(-2.0, fma(fb, tH, -(fe * tS)), acc[c]);
+      }
+      if (update) {
+#pragma unroll
+        for (int g = 0; g < 4; g++) {
+          const size_t o = (size_t)(g * nb + b) * ld;
+          Pre[o + r0] = cadd(p[0][g], y[0][g]);
+          Pre[o + r1] = cadd(p[1][g], y[1][g]);
+        }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
+    atomicAdd(&F[a * 3 + threadIdx.x], v);
+  }
+}
+
+// The step-function bins of k_force_sph alone, for the tiles whose pairs
+// the projections cover (same thread-to-pair map, same bins).
+__global__ void __launch_bounds__(FRC_THREADS) k_force_bins(DevProb P, const int2* __restrict__ tiles, TabDesc T,
+                                                            const double2* __restrict__ rho,
+                                                            const double2* __restrict__ rhoe, int ldr, int rt,
+                                                            double* __restrict__ bins) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int2 t = tiles[blockIdx.x];
+  const int i0 = t.x * SPH_T, j0 = t.y * SPH_T;
+  const int nv = P.nv;
+  const int jl0 = (warp & 1) * 16 + (lane & 7), il0 = (warp >> 1) * 8 + (lane >> 3);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int J = j0 + jl0 + 8 * (q >> 1), I = i0 + il0 + 4 * (q & 1);
+    if (!(J < nv && I < nv && J < I)) continue;
+    const double2 rj = rt ? cconj(rho[(size_t)J * ldr + I]) : rho[(size_t)I * ldr + J];
+    const double2 re = rt ? cconj(rhoe[(size_t)J * ldr + I]) : rhoe[(size_t)I * ldr + J];
+    const int d0 = P.kzz[3 * I] - P.kzz[3 * J], d1 = P.kzz[3 * I + 1] - P.kzz[3 * J + 1],
+              d2 = P.kzz[3 * I + 2] - P.kzz[3 * J + 2];
+    const size_t b = (((size_t)(d2 + T.d3) * (2 * T.d2 + 1)) + (d1 + T.d2)) * (2 * T.d1 + 1) + (d0 + T.d1);
+    const double x2q = P.xk[J] * P.xk[I] + P.yk[J] * P.yk[I] + P.zk[J] * P.zk[I];
+    atomicAdd(&bins[2 * b], x2q * rj.x - re.x);
+    atomicAdd(&bins[2 * b + 1], x2q * rj.y - re.y);
+  }
+}
+
 // local-orbital columns: k_lo's terms per equivalent atom, reduced per warp
 __global__ void k_force_lo(DevProb P, const LoCol* __restrict__ cols, const double2* __restrict__ rho,
                            const double2* __restrict__ rhoe, int ldr, int rt, double* __restrict__ F) {

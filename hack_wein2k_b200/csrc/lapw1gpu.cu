@@ -77,8 +77,13 @@ struct lapw1gpu_context {
   cudaEvent_t ev[22] = {};  // 0-6 stages, 7-11 host copies, 12-15 main contraction kernels,
                             // 16-21 k_albl, k_table, the spherical slicers
   cudaEvent_t fork = nullptr, join[L1G_MAX_SETS] = {};
-  cudaEvent_t fev[6] = {};  // the last forces call: start, density matrices, k_force_sph, LO columns, end
-  float fms[5] = {};        // its intervals (ms), read by lapw1gpu_forces_stats
+  cudaEvent_t fev[7] = {};  // the last forces call: start, density matrices, k_force_sph, LO columns, end;
+                            // [6] the end of the spherical projections
+  float fms[7] = {};        // its intervals (ms), read by lapw1gpu_forces_stats; [5] the projections,
+                            // [6] their products (the split_rect_gemm calls)
+  bool fproj_last = false;  // the last forces call formed spherical projections
+  std::vector<cudaEvent_t> fpev;  // timed forces call: around each projection product
+  int fpev_used = 0;
   // per scratch set: the stream that prepares the split HNS operands while
   // the spherical stage runs, and its fork/join events
   cudaStream_t aux[L1G_MAX_SETS] = {};
@@ -102,6 +107,9 @@ struct lapw1gpu_context {
   int slices_hns = 5;  // int8 slices of the HNS update
   int slices_frc = 6;  // int8 slices of the adjoint's density matrices
   int slices_prj = 6;  // and of its HNS projections
+  int slices_fsp = -1;   // and of its spherical projections (0: the FP64 pair kernel for every pair;
+                         // -1: L1G_FSP_SLICES slices when NV spans L1G_FSP_MIN_BLOCKS blocks)
+  int fsp_block = 1024;  // PW rows per block of the spherical projections
   cublasHandle_t blas[L1G_MAX_SETS] = {};  // library ZGEMMs, one handle (and workspace) per scratch set
   cusolverDnHandle_t solver = nullptr;      // the eigen-solve (lapw1gpu_seclr4)
   // tunables (lapw1gpu_autotune)
@@ -415,6 +423,7 @@ int lapw1gpu_finalize(lapw1gpu_context* c) {
   if (c->d_status) cudaFree(c->d_status);
   for (auto& e : c->ev) cudaEventDestroy(e);
   for (auto& e : c->fev) cudaEventDestroy(e);
+  for (auto& e : c->fpev) cudaEventDestroy(e);
   cudaEventDestroy(c->fork);
   for (auto& e : c->hns_ev) cudaEventDestroy(e);
   for (auto& e : c->sph_ev) cudaEventDestroy(e);
@@ -451,6 +460,16 @@ int lapw1gpu_set_force_slices(lapw1gpu_context* c, int slices_density, int slice
   return LAPW1GPU_OK;
 }
 
+int lapw1gpu_set_force_projection(lapw1gpu_context* c, int slices, int block_rows) {
+  if (!c) return LAPW1GPU_ERR_ARG;
+  if ((slices > 0 && (slices < 4 || slices > L1G_MAX_SLICES)) || slices < -1 || block_rows < 64 ||
+      block_rows % SPH_T)
+    return LAPW1GPU_ERR_RANGE;
+  c->slices_fsp = slices;
+  c->fsp_block = block_rows;
+  return LAPW1GPU_OK;
+}
+
 int lapw1gpu_set_slices(lapw1gpu_context* c, int slices_sph, int slices_hns) {
   if (!c) return LAPW1GPU_ERR_ARG;
   if (slices_sph < 2 || slices_sph > L1G_MAX_SLICES || slices_hns < 2 || slices_hns > L1G_MAX_SLICES)
@@ -469,7 +488,9 @@ int lapw1gpu_forces_stats(lapw1gpu_context* c, lapw1gpu_stats* st) {
   memset(st, 0, sizeof(*st));
   st->ms_albl = c->fms[0];      // operands and the density matrices
   st->ms_spherical = c->fms[1] + c->fms[2];
-  st->ms_sph_main = c->fms[2];  // k_force_sph
+  st->ms_sph_main = c->fms[2] - c->fms[5];  // k_force_sph
+  st->ms_sph_slice = c->fms[6];               // the products of the spherical projections
+  st->ms_table = c->fms[5] - c->fms[6];       // and their other kernels (operand, prefix, bins)
   st->ms_lo = c->fms[3];        // the step-function sums and the LO columns
   st->ms_hns = c->fms[4];       // the HNS part
   st->ms_total = c->fms[0] + c->fms[1] + c->fms[2] + c->fms[3] + c->fms[4];
@@ -1834,8 +1855,46 @@ static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double*
     nlf += 2;
   }
   if (timed) CK(cudaEventRecord(c->fev[1], s));
+  // G c (k_force_gscale) and, in split precision, its k-major copy (G c)^T:
+  // the right operand of the spherical and of the HNS projections
+  double2* GC = nullptr;
+  double2* Gt = nullptr;
+  auto make_gc = [&](bool with_gt) -> int {
+    if (!GC) {
+      GC = (double2*)c->buf("frc_gc", sizeof(double2) * (size_t)4 * nb * n);
+      if (!GC) return LAPW1GPU_ERR_NOMEM;
+      k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
+      nlf++;
+    }
+    if (with_gt && !Gt) {
+      Gt = (double2*)c->buf("frc_gt", sizeof(double2) * (size_t)n * 4 * nb);
+      if (!Gt) return LAPW1GPU_ERR_NOMEM;
+      k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
+      nlf++;
+    }
+    return l1g_launch_status(__FILE__, __LINE__);
+  };
+  // split precision: the spherical pairs of two different row blocks as
+  // projections (forces.cuh), the pairs inside a block on k_force_sph
+  const int fB = c->fsp_block;
+  const int fS = c->slices_fsp < 0 ? L1G_FSP_SLICES : c->slices_fsp;
+  const bool fproj = split_rho && fS > 0 && nv > fB && (c->slices_fsp > 0 || nv >= L1G_FSP_MIN_BLOCKS * fB);
+  if (timed) {
+    c->fproj_last = fproj;
+    c->fpev_used = 0;
+  }
   int ntiles = 0;
-  const int2* tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
+  const int2* tl = nullptr;
+  if (fproj) {
+    tl = kp_tiles(k, "fsp_in:" + std::to_string(nv) + ":" + std::to_string(fB), &ntiles, [&](std::vector<int2>& t) {
+      const int nt = (nv + SPH_T - 1) / SPH_T;
+      for (int bi = 0; bi < nt; bi++)
+        for (int bj = 0; bj <= bi; bj++)
+          if ((bi * SPH_T) / fB == (bj * SPH_T) / fB) t.push_back(make_int2(bi, bj));
+    });
+  } else {
+    tl = tiles_tri(k, "sph", nv, SPH_T, &ntiles);
+  }
   if (!tl) return LAPW1GPU_ERR_NOMEM;
   const size_t nrow = (size_t)nat * ltop * k->nvpad;
   double2* rowJ = (double2*)c->buf("frc_rowj", sizeof(double2) * nrow);
@@ -1852,6 +1911,55 @@ static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double*
   if (!bins) return LAPW1GPU_ERR_NOMEM;
   CK(cudaMemsetAsync(bins, 0, sizeof(double) * 2 * nbox, s));
   if (timed) CK(cudaEventRecord(c->fev[2], s));
+  if (fproj) {
+    const int L2 = ltop * ltop, Ks = ndf * 2 * L2, nblk = (nv + fB - 1) / fB;
+    double2* Ls = (double2*)c->buf("frc_ls", sizeof(double2) * (size_t)nv * Ks);
+    double2* Pre = (double2*)c->buf("frc_pre", sizeof(double2) * (size_t)Ks * 4 * nb);
+    double2* Yp = (double2*)c->buf("frc_yp", sizeof(double2) * (size_t)Ks * 4 * nb);
+    if (!Ls || !Pre || !Yp) return LAPW1GPU_ERR_NOMEM;
+    if (int rc = make_gc(true)) return rc;
+    k_force_rsph<<<nv, 256, 0, s>>>(P, Ls, Ks);
+    nlf++;
+    for (int pb = 0; pb < nblk; pb++) {
+      const int r0 = pb * fB, kc = std::min(fB, nv - r0);
+      int nly = 0;
+      if (timed) {
+        while ((int)c->fpev.size() < 2 * (pb + 1)) {
+          cudaEvent_t e;
+          CK(cudaEventCreate(&e));
+          c->fpev.push_back(e);
+        }
+        CK(cudaEventRecord(c->fpev[2 * pb], s));
+      }
+      // block 0 is the first prefix; later blocks are contracted with it
+      int rc = split_rect_gemm(c, k, 0, Ks, 4 * nb, kc, Ls + (size_t)r0 * Ks, Ks, Gt + (size_t)r0 * 4 * nb, 4 * nb,
+                               pb == 0 ? Pre : Yp, Ks, fS, s, &nly, 1, "fsp");
+      if (rc) return rc;
+      if (timed) {
+        CK(cudaEventRecord(c->fpev[2 * pb + 1], s));
+        c->fpev_used = 2 * (pb + 1);
+      }
+      nlf += nly;
+      if (pb > 0) {
+        k_force_pre<<<dim3(ndf, (nb + FRC_PB - 1) / FRC_PB), 128, 0, s>>>(P, coef, Yp, Pre, Ks, nb, d_occ, d_eps,
+                                                                          pb + 1 < nblk ? 1 : 0, d_grad);
+        nlf++;
+      }
+    }
+    int nto = 0;
+    const int2* to = kp_tiles(k, "fsp_out:" + std::to_string(nv) + ":" + std::to_string(fB), &nto,
+                              [&](std::vector<int2>& t) {
+                                const int nt = (nv + SPH_T - 1) / SPH_T;
+                                for (int bi = 0; bi < nt; bi++)
+                                  for (int bj = 0; bj <= bi; bj++)
+                                    if ((bi * SPH_T) / fB != (bj * SPH_T) / fB) t.push_back(make_int2(bi, bj));
+                              });
+    if (!to) return LAPW1GPU_ERR_NOMEM;
+    k_force_bins<<<nto, FRC_THREADS, 0, s>>>(P, to, k->tab, rho, rhoe, n, rt, bins);
+    nlf++;
+    CK(cudaGetLastError());
+    if (timed) CK(cudaEventRecord(c->fev[6], s));
+  }
   if (lt11)
     k_force_sph<FRC_LT, false><<<ntiles, FRC_THREADS, fsmem, s>>>(P, tl, rowJ, rowI, k->tab, rho, rhoe, n, rt,
                                                                   d_grad, bins);
@@ -1873,33 +1981,28 @@ static int forces_enqueue(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double*
     double2* Rop = (double2*)c->buf("hnsR", sizeof(double2) * (size_t)K * k->npad);
     size_t nloc = (size_t)Kc * std::max(1, nlo);
     double2* Clo = (double2*)c->buf("hnsClo", sizeof(double2) * nloc);
-    double2* GC = (double2*)c->buf("frc_gc", sizeof(double2) * (size_t)4 * nb * n);
     double2* Y = (double2*)c->buf("frc_y", sizeof(double2) * (size_t)4 * nb * K);
     double2* Z = (double2*)c->buf("frc_z", sizeof(double2) * (size_t)4 * nb * K);
-    if (!Rop || !Clo || !GC || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
+    if (!Rop || !Clo || !Y || !Z) return LAPW1GPU_ERR_NOMEM;
     int nl = 0;
     // R and CLM only: the adjoint applies T to Y = R^H (G c), not L = M conj(R)
     int rc = launch_hns_ops(c, P, k->d_tns, k->d_loranges, (int)k->loranges.size(), nullptr, Rop, Clo, nullptr, s,
                             &nl);
     if (rc) return rc;
-    k_force_gscale<<<dim3((n + 127) / 128, nb), 128, 0, s>>>(n, nb, P.kzz, C, ldc, GC);
-    nlf += nl + 1;
-    CK(cudaGetLastError());
+    nlf += nl;
+    if ((rc = make_gc(split_rho))) return rc;
     // Y = R^H (G c): K x 4nb (rows of R beyond n unused); Yc = CLM^H (G c)
     // over the LO rows; Z = T (Y; Yc) per atom.  Split precision: Y and Yc
     // as int8 slice products, from k-major copies conj(R)^T, conj(CLM)^T
     // and (G c)^T
-    double2* Gt = nullptr;
     if (split_rho) {
       double2* Lt = (double2*)c->buf("frc_rt", sizeof(double2) * (size_t)n * K);
-      Gt = (double2*)c->buf("frc_gt", sizeof(double2) * (size_t)n * 4 * nb);
-      if (!Lt || !Gt) return LAPW1GPU_ERR_NOMEM;
+      if (!Lt) return LAPW1GPU_ERR_NOMEM;
       k_force_trans<<<dim3((n + 31) / 32, (K + 31) / 32), 256, 0, s>>>(Rop, k->npad, K, n, 1, Lt, K);
-      k_force_trans<<<dim3((n + 31) / 32, (4 * nb + 31) / 32), 256, 0, s>>>(GC, n, 4 * nb, n, 0, Gt, 4 * nb);
       int nly = 0;
       rc = split_rect_gemm(c, k, 0, K, 4 * nb, n, Lt, K, Gt, 4 * nb, Y, K, c->slices_prj, s, &nly, 1);
       if (rc) return rc;
-      nlf += nly + 2;
+      nlf += nly + 1;
     } else if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, K, 4 * nb, n, &one, (const cuDoubleComplex*)Rop, k->npad,
                            (const cuDoubleComplex*)GC, n, &zero, (cuDoubleComplex*)Y, K) != CUBLAS_STATUS_SUCCESS) {
       return LAPW1GPU_ERR_CUDA;
@@ -1974,6 +2077,15 @@ int lapw1gpu_forces(lapw1gpu_context* c, lapw1gpu_kpoint* k, const double* d_c, 
   c->status_pending = false;
   c->last_launches = nl;
   for (int q = 0; q < 5; q++) cudaEventElapsedTime(&c->fms[q], c->fev[q], c->fev[q + 1]);
+  c->fms[5] = c->fms[6] = 0.f;
+  if (c->fproj_last) {
+    cudaEventElapsedTime(&c->fms[5], c->fev[2], c->fev[6]);
+    for (int q = 0; q + 1 < c->fpev_used; q += 2) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, c->fpev[q], c->fpev[q + 1]);
+      c->fms[6] += t;
+    }
+  }
   cudaGetLastError();
   return hstat ? LAPW1GPU_ERR_RANGE : LAPW1GPU_OK;
 }

@@ -36,7 +36,7 @@ EXPORTS = [
     "lapw1gpu_hns_noalloc", "lapw1gpu_forces", "lapw1gpu_setup_batch", "lapw1gpu_get_tuning",
     "lapw1gpu_set_tuning", "lapw1gpu_autotune", "lapw1gpu_set_slices", "lapw1gpu_test_wait_timeout",
     "lapw1gpu_last_launches", "lapw1gpu_host_register", "lapw1gpu_host_unregister", "lapw1gpu_forces_stats",
-    "lapw1gpu_forces_batch", "lapw1gpu_set_force_slices",
+    "lapw1gpu_forces_batch", "lapw1gpu_set_force_slices", "lapw1gpu_set_force_projection",
     "lapw1gpu_seclr4",
 ]
 
@@ -74,6 +74,7 @@ def load(path: Optional[str] = None):
     lib.lapw1gpu_set_precision.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_set_slices.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_set_force_slices.argtypes = [vp, C.c_int, C.c_int]
+    lib.lapw1gpu_set_force_projection.argtypes = [vp, C.c_int, C.c_int]
     lib.lapw1gpu_seclr4.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     lib.lapw1gpu_kpoint_upload.argtypes = [vp, C.POINTER(CProblem), C.POINTER(vp)]
@@ -184,6 +185,14 @@ class Context:
         projections in split precision (lapw1gpu_set_force_slices)"""
         sp = slices if slices_projection is None else slices_projection
         _check("lapw1gpu_set_force_slices", self.lib.lapw1gpu_set_force_slices(self.h, slices, sp))
+
+    def set_force_projection(self, slices: int, block_rows: int = 1024):
+        """split precision: the adjoint's spherical pairs of different blocks
+        of block_rows PW rows as int8 slice projections (slices 4..8; 0: the
+        FP64 pair kernel for every pair; -1: 6 slices from 6 blocks of rows)
+        (lapw1gpu_set_force_projection)"""
+        _check("lapw1gpu_set_force_projection",
+               self.lib.lapw1gpu_set_force_projection(self.h, slices, block_rows))
 
     @property
     def stream_handle(self) -> int:

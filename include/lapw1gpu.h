@@ -183,6 +183,16 @@ int lapw1gpu_set_slices(lapw1gpu_context* ctx, int slices_sph, int slices_hns);
  * the HNS projections Y = R^H (G c); the force pair sums stay FP64 */
 int lapw1gpu_set_force_slices(lapw1gpu_context* ctx, int slices_density,
                               int slices_projection);
+/* Spherical pair sums of the adjoint in split precision as projections:
+ * slices = 0 keeps the FP64 pair kernel for every PW x PW pair; 4..8 forms
+ * the pairs of two different blocks of block_rows PW rows (a multiple of
+ * 32, at least 64) from int8 slice products of the rows' real-harmonic
+ * expansion (addition theorem) with (G c)^T, block by block against the
+ * running sum of the blocks before; the pairs inside a block stay on the
+ * FP64 pair kernel.  slices = -1 (the default, with 1024-row blocks): 6
+ * slices when the PW rows span at least 6 blocks, else the pair kernel. */
+int lapw1gpu_set_force_projection(lapw1gpu_context* ctx, int slices,
+                                  int block_rows);
 
 /* One k-point's inputs resident in device memory (uploaded once; the
  * benchmark's resident-input path and the k-point batch driver use it). */
@@ -382,7 +392,10 @@ int lapw1gpu_forces_batch(lapw1gpu_context* ctx, lapw1gpu_kpoint* const* kps, in
 /* Device times of the last lapw1gpu_forces call on the context, in the
  * fields of lapw1gpu_stats: ms_total the whole call, ms_albl the operands
  * and the density matrices, ms_spherical the plane-wave pair sums with
- * ms_sph_main the pair kernel k_force_sph alone, ms_lo the step-function
+ * ms_sph_main the pair kernel k_force_sph alone, ms_sph_slice the int8
+ * products of the spherical projections with their operand slicing and
+ * ms_table the projections' other kernels (both 0 without them), ms_lo the
+ * step-function
  * sums and the local-orbital columns, ms_hns the non-spherical part,
  * kernel_launches its launches.  No counterpart in the reference. */
 int lapw1gpu_forces_stats(lapw1gpu_context* ctx, lapw1gpu_stats* st);

@@ -67,6 +67,45 @@ def test_split_density_matrices_match_fp64(ctx, kind):
     assert np.abs(gs - g64).max() <= 1e-8 * scale, (gs, g64)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", KINDS + ["manyeq"])
+def test_spherical_projections_match_fp64(ctx, kind):
+    """lapw1gpu_set_force_projection: the spherical pairs of two different
+    64-row blocks as int8 slice projections (6 slices) against the running
+    sum of the earlier blocks, the pairs inside a block on the FP64 pair
+    kernel.  Same eigenvectors: the gradient agrees with the FP64 adjoint
+    to 1e-8 of its largest component ("gamma" has a zero k-vector row,
+    "apw" rows without bl, "manyeq" 17 equivalent atoms of one type)."""
+    p = synth.small_case(kind, rkmax=2.5) if kind == "manyeq" else synth.small_case(kind)
+    w, _ = FR.eigh(p)
+    nb, _ = FR.gapped_nb(w)
+    dev = torch.device("cuda", ctx.device)
+    occ = _occ(p, nb).to(dev)
+    E, eps, X, kp = FO.band_energy(ctx, p, occ)
+    g64 = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    ctx.set_precision(lapw1gpu.PREC_SPLIT, 5)
+    ctx.set_force_projection(6, 64)
+    try:
+        gp = FO.gradient(ctx, kp, X, occ, eps).cpu().numpy()
+    finally:
+        ctx.set_force_projection(-1, 1024)
+        ctx.set_precision(lapw1gpu.PREC_FP64)
+    kp.free()
+    scale = np.abs(g64).max()
+    assert scale > 0
+    assert np.abs(gp - g64).max() <= 1e-8 * scale, (gp, g64)
+
+
+@pytest.mark.gpu
+def test_force_projection_arguments(ctx):
+    """The block must be a multiple of 32 rows, at least 64; slices -1, 0 or 4..8."""
+    for bad in [(6, 48), (6, 100), (3, 1024), (9, 1024), (-2, 1024)]:
+        with pytest.raises(lapw1gpu.Lapw1GpuError) as e:
+            ctx.set_force_projection(*bad)
+        assert e.value.code == 7  # LAPW1GPU_ERR_RANGE
+    ctx.set_force_projection(-1, 1024)
+
+
 @pytest.fixture(scope="module")
 def manyeq_ref():
     p = synth.small_case("manyeq", rkmax=2.5)

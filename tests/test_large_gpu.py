@@ -129,11 +129,16 @@ def c3_forces(ctx):
         gsp = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
         ctx.set_force_slices(6, 4)  # the benchmark's setting: 4-slice HNS projections
         gsp4 = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
+        # and the spherical pairs of different 1024-row blocks as 6-slice
+        # projections (automatic from 6 blocks; c3 spans 5.4, so forced here)
+        ctx.set_force_projection(6, 1024)
+        gproj = FO.gradient(ctx, kp, X, occ, w).cpu().numpy()
     finally:
+        ctx.set_force_projection(-1, 1024)
         ctx.set_force_slices(6, 6)
         ctx.set_precision(lapw1gpu.PREC_FP64)
     kp.free()
-    return p, occ, g64, (gsp, gsp4)
+    return p, occ, g64, (gsp, gsp4, gproj)
 
 
 @pytest.mark.gpu
@@ -142,7 +147,7 @@ def c3_forces(ctx):
 def test_c3_forces_match_central_differences(ctx, c3_forces, ac):
     """dE/dR of the adjoint against (E(R + h) - E(R - h)) / 2h, h = 1e-4
     bohr, through the FP64 setup and the device eigen-solve."""
-    p, occ, g64, (gsp, gsp4) = c3_forces
+    p, occ, g64, (gsp, gsp4, gproj) = c3_forces
     a, c = ac
     bk = np.asarray(p.bkzz, dtype=np.float64).reshape(3, 3)
     h = 1.0e-4 * bk[c, c] / (2.0 * np.pi)  # lattice step of the orthorhombic cell
@@ -151,3 +156,4 @@ def test_c3_forces_match_central_differences(ctx, c3_forces, ac):
     assert abs(fd - g64[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, g64[a, c] * to_cart)
     assert abs(fd - gsp[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gsp[a, c] * to_cart)
     assert abs(fd - gsp4[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gsp4[a, c] * to_cart)
+    assert abs(fd - gproj[a, c]) * to_cart <= TOL_FD_RY_BOHR, (fd * to_cart, gproj[a, c] * to_cart)
