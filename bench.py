@@ -22,7 +22,9 @@ of the same crystal (k-point sharding, no collective on the data path).
 time of K steps, CUDA events on the library's stream, max over ranks, over
 16 N k-points per step).  `fp64_path` times the plain FP64 GPU path (FP64
 spherical kernel, FP64 HNS with library ZGEMM panels, FP64 density
-matrices) on the same k-points and eigenvectors; `setup` and `forces` split
+matrices, every adjoint pair on the FP64 pair kernel) on the same k-points
+and eigenvectors, against the split arm (int8 slice products on tcgen05,
+the adjoint's cross-block spherical pairs as int8 projections); `setup` and `forces` split
 both arms into their parts, with forces/s (3 NDF force components per
 k-point per second).  `e2e` runs k-point 0 through the host C ABI: inputs
 from host memory, HS/HSDIAG copied back into a caller HS page-locked once

@@ -180,7 +180,9 @@ int lapw1gpu_set_precision(lapw1gpu_context* ctx, int prec, int slices);
 int lapw1gpu_set_slices(lapw1gpu_context* ctx, int slices_sph, int slices_hns);
 /* int8 slices (4..8 each, default 6 and 6) of the adjoint's products in
  * split precision (lapw1gpu_forces): the density matrices rho, rhoE and
- * the HNS projections Y = R^H (G c); the force pair sums stay FP64 */
+ * the HNS projections Y = R^H (G c); the spherical pair sums are FP64
+ * (lapw1gpu_set_force_projection moves the cross-block ones to int8
+ * projections) */
 int lapw1gpu_set_force_slices(lapw1gpu_context* ctx, int slices_density,
                               int slices_projection);
 /* Spherical pair sums of the adjoint in split precision as projections:
