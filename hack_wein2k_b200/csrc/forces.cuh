@@ -20,6 +20,10 @@
 //                 step-function term 3 V BESR of each atom (k_table) depends
 //                 on the pair only through dK, so the pairs are binned by dK
 //                 and k_force_step sums the bins per atom
+//   k_force_rsph, k_force_pre, k_force_bins  (split precision) the PW x PW
+//                 pairs of two different row blocks as int8 projections by
+//                 the addition theorem, against a running prefix; the pairs
+//                 inside a block stay on k_force_sph (see below k_force_step)
 //   k_force_lo    local-orbital columns, per equivalent atom (k_lo's terms)
 //   k_force_hns_reduce  the HNS update through its factors.  HNS adds
 //                 A(I,J) = X_J^T T conj(X_I) with X = (ALM, BLM, CLM) per atom
